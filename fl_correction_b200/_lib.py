@@ -1,0 +1,124 @@
+"""ctypes binding of the native library ``libflc.so`` (C ABI in include/flc.h).
+
+The library is loaded once; if it is missing or cannot be loaded every entry
+point raises immediately -- there is no Python or CPU fallback.  Tensors are
+passed as raw device pointers with 64-bit sizes and torch's current stream.
+"""
+import ctypes
+import os
+
+import torch
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libflc.so")
+
+_i64 = ctypes.c_int64
+_vp = ctypes.c_void_p
+_f32 = ctypes.c_float
+_f64 = ctypes.c_double
+_int = ctypes.c_int
+_sz = ctypes.c_size_t
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "flc_status_string": (ctypes.c_char_p, [_int]),
+    "flc_last_error": (ctypes.c_char_p, []),
+    "flc_version": (ctypes.c_char_p, []),
+    "flc_cone_atten": (_int, [_vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _i64, _i64, _int, _vp]),
+    "flc_cone_atten_separable": (_int, [_vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _i64,
+                                        _i64, _int, _vp]),
+    "flc_fwd_emission": (_int, [_vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _vp]),
+    "flc_bwd_emission": (_int, [_vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _vp]),
+    "flc_huber_grad": (_int, [_vp, _vp, _i64, _i64, _i64, _f32, _vp]),
+    "flc_mlem_workspace_bytes": (_sz, [_i64, _i64, _i64, _i64, _i64]),
+    "flc_mlem": (_int, [_vp, _vp, _vp, _vp, _vp, _i64, _f64, _f64, _i64, _i64, _i64, _i64, _i64,
+                        _vp, _sz, _int, _vp]),
+    "flc_atten_workspace_bytes": (_sz, [_i64, _i64, _i64, _i64, _i64, _i64, _i64]),
+    "flc_atten_maps": (_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64,
+                              _i64, _i64, _i64, _i64, _int, _int, _i64, _vp, _sz, _vp]),
+    "flc_rotate": (_int, [_vp, _vp, _i64, _i64, _i64, _f32, _f32, _vp]),
+    "flc_incident_scan": (_int, [_vp, _vp, _i64, _i64, _i64, _vp]),
+}
+
+_LIB = None
+_LOAD_ERROR = None
+
+
+class FlcError(RuntimeError):
+    """A native entry point returned a non-zero flc_status."""
+
+    def __init__(self, name, status, message):
+        self.status = status
+        super().__init__("%s failed: %s: %s" % (name, status, message))
+
+
+def load():
+    """Load libflc.so (building it first if the sources are newer)."""
+    global _LIB, _LOAD_ERROR
+    if _LIB is not None:
+        return _LIB
+    if _LOAD_ERROR is not None:
+        raise _LOAD_ERROR
+    try:
+        if not os.path.exists(LIB_PATH):
+            from . import build as _build
+            _build.build()
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+    except Exception as e:  # keep the first failure and re-raise it on every call
+        _LOAD_ERROR = RuntimeError("fl_correction_b200: cannot load native library %s: %s"
+                                   % (LIB_PATH, e))
+        raise _LOAD_ERROR
+    _LIB = lib
+    return lib
+
+
+def call(name, *args):
+    """Call an flc_* entry point; raise FlcError on a non-zero status."""
+    lib = load()
+    st = getattr(lib, name)(*args)
+    if st != 0:
+        msg = lib.flc_last_error().decode(errors="replace")
+        raise FlcError(name, lib.flc_status_string(st).decode(), msg)
+    return st
+
+
+def query(name, *args):
+    return getattr(load(), name)(*args)
+
+
+def ptr(t):
+    """Device pointer of a tensor (None -> NULL)."""
+    return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+def stream(device=None):
+    return ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+
+
+def require_cuda(name, *tensors, dtype=torch.float32):
+    """TORCH_CHECK-style argument checks of the reference (atten_cuda.cpp)."""
+    dev = None
+    for t in tensors:
+        if not isinstance(t, torch.Tensor):
+            raise TypeError("%s: expected a torch.Tensor, got %s" % (name, type(t).__name__))
+        if not t.is_cuda:
+            raise RuntimeError("%s: tensors must be CUDA tensors" % name)
+        if dtype is not None and t.dtype != dtype:
+            raise RuntimeError("%s: tensors must be %s (got %s)" % (name, dtype, t.dtype))
+        if dev is None:
+            dev = t.device
+        elif t.device != dev:
+            raise RuntimeError("%s: tensors must be on one device" % name)
+    return dev
+
+
+def workspace(nbytes, device):
+    """A 256-byte aligned uint8 workspace from torch's caching allocator."""
+    n = max(int(nbytes), 1) + 256
+    buf = torch.empty(n, dtype=torch.uint8, device=device)
+    off = (-buf.data_ptr()) % 256
+    return buf[off:off + max(int(nbytes), 1)]

@@ -1,0 +1,176 @@
+"""Per-angle attenuation and re-projection with the signatures of FL/core.py.
+
+The reference loops over angles in Python, rotating, assembling mu, running
+the cone kernel and writing one TIFF per element per angle
+(FL/core.py:19-101).  Here every angle of every element is produced by one
+native call (flc_atten_maps) and kept on the device; ``fsave`` (default
+None) optionally writes one ``.npy`` per element instead of per-angle TIFFs.
+"""
+import os
+
+import numpy as np
+import torch
+
+from . import _lib
+from .atten_util import extract_single_value_param
+from .cuda_lib.atten_cuda import forward_emission_batch
+from .detector_mask import factor_mask
+
+__all__ = ["atten_coefficients", "mask_factors", "atten_maps", "cal_xrf_atten_at_angles",
+           "cal_xray_atten_at_angles", "cal_total_atten_at_angles", "cal_atten_at_angles",
+           "re_projection_cuda"]
+
+INCIDENT_MODES = {"own": 0, "all": 1, "none": 2}
+
+
+def atten_coefficients(param, n_angle, n_ch=None):
+    """coef_x (A, n_ch) and coef_f (A, L, n_ch) as float32 numpy arrays,
+    selecting per-angle cross sections like extract_single_value_param."""
+    comps = param["elem_compound"]
+    elems = param["elem_type"]
+    n_ch = len(comps) if n_ch is None else n_ch
+    cx = np.zeros((n_angle, n_ch), np.float32)
+    cf = np.zeros((n_angle, len(elems), n_ch), np.float32)
+    for a in range(n_angle):
+        p = extract_single_value_param(param, a)
+        cs, rho, pix = p["cs"], p["rho"], p["pix"]
+        for j, c in enumerate(comps[:n_ch]):
+            cx[a, j] = float(np.asarray(cs[f"{c}-x"]).reshape(-1)[0]) * rho[c] * pix
+            for i, e in enumerate(elems):
+                cf[a, i, j] = float(cs[f"{c}-{e}"]) * rho[c] * pix
+    return cx, cf
+
+
+def mask_factors(detector_mask, device):
+    """Device copies (u, v) of the rank-one factors of each depth plane."""
+    fac = factor_mask(detector_mask)
+    if fac is None:
+        raise ValueError("detector mask is not rank one per depth plane")
+    u, v = fac
+    return (torch.from_numpy(u).to(device).contiguous(), torch.from_numpy(v).to(device).contiguous(),
+            tuple(np.shape(detector_mask)))
+
+
+def atten_maps(frac_4D, angle_list, coef_x, coef_f, mask_uv=None, incident="own", xrf=True,
+               out=None, chunk=0, workspace=None):
+    """Attenuation (L, A, S, H, W) for fractions frac_4D (n_ch, S, H, W) on the
+    device: incident term (mode 'own' | 'all' | 'none') times exp(-cone).
+
+    coef_x (A, n_ch), coef_f (A, L, n_ch): per-angle mu coefficients (numpy or
+    device tensors).  mask_uv: (u, v, mask_shape) from mask_factors."""
+    _lib.require_cuda("atten_maps", frac_4D)
+    dev = frac_4D.device
+    frac = frac_4D.contiguous()
+    n_ch, S, H, W = frac.shape
+    theta = torch.as_tensor(np.asarray(angle_list, dtype=np.float64) / 180.0 * np.pi,
+                            dtype=torch.float32, device=dev)
+    A = theta.numel()
+    cx = torch.as_tensor(coef_x, dtype=torch.float32, device=dev).contiguous()
+    cf = torch.as_tensor(coef_f, dtype=torch.float32, device=dev).contiguous()
+    L = cf.shape[1]
+    if out is None:
+        out = torch.empty((L, A, S, H, W), dtype=torch.float32, device=dev)
+    if xrf:
+        u, v, (Mz, Mx, My) = mask_uv
+    else:
+        u = v = None
+        Mz = Mx = My = 1
+    ws_bytes = _lib.query("flc_atten_workspace_bytes", n_ch, S, H, W, A, L, chunk)
+    ws = workspace if workspace is not None and workspace.numel() >= ws_bytes else _lib.workspace(ws_bytes, dev)
+    with torch.cuda.device(dev):
+        _lib.call("flc_atten_maps", _lib.ptr(frac), _lib.ptr(theta), _lib.ptr(cx), _lib.ptr(cf),
+                  _lib.ptr(u), _lib.ptr(v), _lib.ptr(out), n_ch, S, H, W, A, L, Mz, Mx, My,
+                  INCIDENT_MODES[incident], 0 if xrf else 1, chunk, _lib.ptr(ws), ws_bytes,
+                  _lib.stream())
+    return out
+
+
+def _save(fsave, kind, param, maps):
+    if fsave is None:
+        return
+    os.makedirs(fsave, exist_ok=True)
+    for i, elem in enumerate(param["elem_type"]):
+        np.save(os.path.join(fsave, f"atten_{kind}_{elem}.npy"), maps[i].cpu().numpy())
+
+
+def cal_xrf_atten_at_angles(frac_4D, param, angle_list, detector_mask, detector_offset_angle=0,
+                            position_det="r", dict_use_ref={}, fsave=None):
+    """exp(-cone(mu_f)) at every angle for every element (FL/core.py:19-52):
+    returns (L, A, S, H, W) on frac_4D's device."""
+    if abs(detector_offset_angle) > 1e-2 * 180 / np.pi or position_det != "r":
+        raise NotImplementedError("only detector_offset_angle=0, position_det='r' is implemented")
+    if len(dict_use_ref) > 0 and dict_use_ref.get("use_ref", False):
+        raise NotImplementedError("reference-spectrum volumes are not implemented")
+    cx, cf = atten_coefficients(param, len(angle_list), frac_4D.shape[0])
+    maps = atten_maps(frac_4D, angle_list, cx, cf, mask_factors(detector_mask, frac_4D.device),
+                      incident="none", xrf=True)
+    _save(fsave, "fl", param, maps)
+    return maps
+
+
+def cal_xray_atten_at_angles(frac_4D, param, angle_list, dict_use_ref={}, fsave=None):
+    """Incident-beam attenuation at every angle (FL/core.py:55-81): element i
+    uses channel i, as the reference writes atten_xray[i] for element i."""
+    if len(dict_use_ref) > 0 and dict_use_ref.get("use_ref", False):
+        raise NotImplementedError("reference-spectrum volumes are not implemented")
+    cx, cf = atten_coefficients(param, len(angle_list), frac_4D.shape[0])
+    maps = atten_maps(frac_4D, angle_list, cx, cf, None, incident="own", xrf=False)
+    _save(fsave, "xray", param, maps)
+    return maps
+
+
+def cal_total_atten_at_angles(fsave, param):
+    """atten = atten_fl * atten_xray per element (FL/core.py:84-101), from the
+    .npy files that the two functions above write into fsave."""
+    out = {}
+    for elem in param["elem_type"]:
+        fl = np.load(os.path.join(fsave, f"atten_fl_{elem}.npy"))
+        xr = np.load(os.path.join(fsave, f"atten_xray_{elem}.npy"))
+        out[elem] = fl * xr
+        np.save(os.path.join(fsave, f"atten_{elem}.npy"), out[elem])
+    return out
+
+
+def cal_atten_at_angles(frac_4D, param, angle_list, detector_mask, incident="own", out=None):
+    """The total attenuation of FL/core.py:84-101 computed in one pass, without
+    the intermediate files: (L, A, S, H, W)."""
+    cx, cf = atten_coefficients(param, len(angle_list), frac_4D.shape[0])
+    return atten_maps(frac_4D, angle_list, cx, cf, mask_factors(detector_mask, frac_4D.device),
+                      incident=incident, xrf=True, out=out)
+
+
+def re_projection_cuda(img3D, angle_list, param=None, rho_compound=1, atten_coef=None, elem="Ni",
+                       use_ref=False, device="cuda"):
+    """XRF projections of img3D ((S,H,W) or (R,S,H,W)) at angle_list (degrees)
+    through atten_coef (A,S,H,W), emission cs from param (FL/core.py:104-156)."""
+    n_angle = len(angle_list)
+    if param is None:
+        em = np.ones((n_angle, 1))
+    else:
+        pix = param["pix"]
+        em_cs_dict = param["em_cs"]
+        if use_ref:
+            n_ref = img3D.shape[0]
+            em = np.zeros([n_angle, n_ref])
+            for i in range(n_ref):
+                em[:, i] = em_cs_dict[f"{elem}_ref{i + 1}"] * pix
+        else:
+            em = np.asarray(em_cs_dict[elem]) * pix
+            em = em.reshape((len(em), 1))
+    img3D = img3D * rho_compound
+    if isinstance(img3D, torch.Tensor):
+        C = img3D.to(device=device, dtype=torch.float)
+    else:
+        C = torch.tensor(np.asarray(img3D), dtype=torch.float, device=device)
+    if C.dim() == 3:
+        C = C[None]
+    n_ref, n_sli, H, W = C.shape
+    if atten_coef is None:
+        at = torch.ones(n_angle, n_sli, H, W, dtype=torch.float, device=device)
+    else:
+        at = torch.as_tensor(atten_coef, dtype=torch.float, device=device)
+        if at.dim() == 3:
+            at = at[:, None]
+    theta = torch.tensor(np.asarray(angle_list) / 180.0 * np.pi, dtype=torch.float, device=device)
+    em_t = torch.tensor(np.asarray(em), dtype=torch.float, device=device)
+    return forward_emission_batch(at.contiguous(), C.contiguous(), em_t, theta).cpu().numpy()

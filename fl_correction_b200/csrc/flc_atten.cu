@@ -1,0 +1,678 @@
+// Per-angle attenuation maps for sm_100a: rotation (grid_sample semantics),
+// mu assembly, incident-beam exclusive product scan, and the fluorescence
+// cone-mask path sum (general and separable forms).
+//
+// Reference path (per angle, FL/core.py:19-101):
+//   frac_rot = torch_rotate_image_nd(frac, theta)           FL/torch_image_util.py:13-114
+//   mu_x[j]  = frac_rot[j] * cs[comp_j-x] * rho_j * pix     FL/torch_functions.py:39-51
+//   atten_x  = exclusive reverse cumprod of (1 - mu_x) on H FL/torch_functions.py:95-102
+//   mu_f[i]  = sum_j frac_rot[j] * cs[comp_j-elem_i]*rho_j*pix   :71-80
+//   res      = rot90^-1(atten_kernel(rot90(mu_f), mask))    :142-171, atten_cuda_kernel.cu:10-57
+//   atten[i] = atten_x[i] * exp(-res[i])                    :174, FL/core.py:99
+// Here one kernel rotates every channel, assembles both mu's, runs the scan
+// along the beam in registers and writes the incident term straight into the
+// output, plus mu_f in the layout the cone kernel streams (the reference's
+// rot90 frame, where a detector-depth plane is a set of contiguous rows).  The
+// cone kernel then multiplies exp(-res) into the same output.
+
+#include <math.h>
+#include <string.h>
+
+#include <vector>
+
+#include "flc_common.cuh"
+
+namespace flc {
+namespace {
+
+// ---------------------------------------------------------------------------
+// grid_sample rotation: out(h,w) samples the input at
+//   ix = c*(w-cx) - s*(h-cy)*(W/H) + cx,  iy = s*(w-cx)*(H/W) + c*(h-cy) + cy
+// (affine_grid with [[c,-s,0],[s,c,0]], align_corners=False, unnormalised),
+// bilinear, zero padding outside the image.
+// ---------------------------------------------------------------------------
+struct RotGeom {
+    float c, s, cx, cy, sxw, syh;  // sxw = W/H, syh = H/W
+};
+
+__device__ __forceinline__ float rot_sample(const float* __restrict__ img, int H, int W,
+                                            const RotGeom& g, int h, int w) {
+    float dw = (float)w - g.cx, dh = (float)h - g.cy;
+    float ix = g.c * dw - g.s * dh * g.sxw + g.cx;
+    float iy = g.s * dw * g.syh + g.c * dh + g.cy;
+    float fx = floorf(ix), fy = floorf(iy);
+    int x0 = (int)fx, y0 = (int)fy;
+    float tx = ix - fx, ty = iy - fy;
+    bool xin0 = x0 >= 0 && x0 < W, xin1 = x0 + 1 >= 0 && x0 + 1 < W;
+    bool yin0 = y0 >= 0 && y0 < H, yin1 = y0 + 1 >= 0 && y0 + 1 < H;
+    float v00 = (yin0 && xin0) ? __ldg(img + y0 * W + x0) : 0.f;
+    float v01 = (yin0 && xin1) ? __ldg(img + y0 * W + x0 + 1) : 0.f;
+    float v10 = (yin1 && xin0) ? __ldg(img + (y0 + 1) * W + x0) : 0.f;
+    float v11 = (yin1 && xin1) ? __ldg(img + (y0 + 1) * W + x0 + 1) : 0.f;
+    float top = fmaf(tx, v01 - v00, v00);
+    float bot = fmaf(tx, v11 - v10, v10);
+    return fmaf(ty, bot - top, top);
+}
+
+__host__ __device__ inline RotGeom rot_geom(float c, float s, int H, int W) {
+    RotGeom g;
+    g.c = c;
+    g.s = s;
+    g.cx = (W - 1) * 0.5f;
+    g.cy = (H - 1) * 0.5f;
+    g.sxw = (float)W / (float)H;
+    g.syh = (float)H / (float)W;
+    return g;
+}
+
+__global__ void rotate_kernel(const float* __restrict__ x, float* __restrict__ out, int64_t N,
+                              int H, int W, RotGeom g) {
+    int w = blockIdx.x * blockDim.x + threadIdx.x;
+    int h = blockIdx.y;
+    if (w >= W) return;
+    for (int64_t n = blockIdx.z; n < N; n += gridDim.z) {
+        const float* img = x + n * H * W;
+        out[(n * H + h) * W + w] = rot_sample(img, H, W, g, h, w);
+    }
+}
+
+__global__ void incident_scan_kernel(const float* __restrict__ mu, float* __restrict__ out,
+                                     int64_t N, int H, int W) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N * W) return;
+    int64_t n = i / W;
+    int w = (int)(i - n * W);
+    const float* m = mu + n * H * W + w;
+    float* o = out + n * H * W + w;
+    float p = 1.f;
+    for (int h = H - 1; h >= 0; --h) {
+        o[(int64_t)h * W] = p;
+        p *= 1.f - m[(int64_t)h * W];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Fused per-angle stage: grid (S, A_chunk), block W threads (one per detector
+// column).  Walks the beam from h = H-1 to 0:
+//   out[i][a][s][h][w] = incident term (exclusive product, mode-dependent)
+//   mu_ref[a][i][s][x=w][y=H-1-h] = mu_f[i] (staged 32 rows at a time in smem
+//   so that the transposed store is a run of 32 contiguous floats)
+// ---------------------------------------------------------------------------
+constexpr int kMaxCh = 8;
+constexpr int kMaxL = 8;
+constexpr int kStageRows = 32;
+
+struct AngleCoef {
+    float cos_t, sin_t;
+    float cx[kMaxCh];
+    float cf[kMaxL][kMaxCh];
+};
+
+__global__ void atten_stage_kernel(const float* __restrict__ frac, const AngleCoef* __restrict__ coefs,
+                                   float* __restrict__ out, float* __restrict__ mu_ref, int n_ch,
+                                   int S, int H, int W, int L, int64_t out_a_stride,
+                                   int64_t out_l_stride, int a_base, int incident_mode,
+                                   int write_mu) {
+    extern __shared__ float stage[];  // [L][kStageRows][W]
+    const int s = blockIdx.x;
+    const int al = blockIdx.y;
+    const int a = a_base + al;
+    const int w = threadIdx.x;
+    const AngleCoef& cf = coefs[a];
+    const RotGeom g = rot_geom(cf.cos_t, cf.sin_t, H, W);
+    float prod[kMaxL];
+#pragma unroll
+    for (int i = 0; i < kMaxL; ++i) prod[i] = 1.f;
+    const int64_t HW = (int64_t)H * W;
+    for (int h = H - 1; h >= 0; --h) {
+        float fr[kMaxCh];
+#pragma unroll
+        for (int j = 0; j < kMaxCh; ++j)
+            fr[j] = (j < n_ch && w < W) ? rot_sample(frac + ((int64_t)j * S + s) * HW, H, W, g, h, w) : 0.f;
+        // incident term: write the exclusive product, then fold in this voxel
+        if (w < W && incident_mode != 2) {
+#pragma unroll
+            for (int i = 0; i < kMaxL; ++i)
+                if (i < L) out[i * out_l_stride + a * out_a_stride + s * HW + (int64_t)h * W + w] = prod[i];
+            if (incident_mode == 0) {
+#pragma unroll
+                for (int i = 0; i < kMaxL; ++i)
+                    if (i < L) prod[i] *= 1.f - fr[i] * cf.cx[i];
+            } else {
+                float f = 1.f;
+#pragma unroll
+                for (int j = 0; j < kMaxCh; ++j)
+                    if (j < n_ch) f *= 1.f - fr[j] * cf.cx[j];
+#pragma unroll
+                for (int i = 0; i < kMaxL; ++i) prod[i] *= f;
+            }
+        } else if (w < W) {
+#pragma unroll
+            for (int i = 0; i < kMaxL; ++i)
+                if (i < L) out[i * out_l_stride + a * out_a_stride + s * HW + (int64_t)h * W + w] = 1.f;
+        }
+        if (!write_mu) continue;
+        const int row = (H - 1 - h) % kStageRows;  // y = H-1-h within the staged block
+#pragma unroll
+        for (int i = 0; i < kMaxL; ++i) {
+            if (i >= L) break;
+            float m = 0.f;
+#pragma unroll
+            for (int j = 0; j < kMaxCh; ++j)
+                if (j < n_ch) m += fr[j] * cf.cf[i][j];
+            if (w < W) stage[(i * kStageRows + row) * W + w] = m;
+        }
+        const int y = H - 1 - h;
+        if (row == kStageRows - 1 || h == 0) {
+            __syncthreads();
+            const int y0 = y - row, nrows = row + 1;
+            // transposed store: mu_ref[al][i][s][x][y0 + r], r contiguous
+            for (int idx = threadIdx.x; idx < L * W * nrows; idx += blockDim.x) {
+                int r = idx % nrows;
+                int rest = idx / nrows;
+                int x = rest % W, i = rest / W;
+                mu_ref[(((int64_t)al * L + i) * S + s) * HW + (int64_t)x * H + y0 + r] =
+                    stage[(i * kStageRows + r) * W + x];
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Cone path sum, general mask: thread per output, loop over the non-zero taps
+// (dz, dx, dy, weight) listed by the host.  Reference layout (K,Z,X,Y).
+// ---------------------------------------------------------------------------
+struct ConeTap {
+    int dz, dx, dy;
+    float w;
+};
+
+__global__ void cone_general_kernel(const float* __restrict__ mu, const ConeTap* __restrict__ taps,
+                                    int ntaps, float* __restrict__ out, int64_t KZ, int Z, int X, int Y) {
+    int y = blockIdx.x * blockDim.x + threadIdx.x;
+    int x = blockIdx.y;
+    if (y >= Y) return;
+    for (int64_t kz = blockIdx.z; kz < KZ; kz += gridDim.z) {
+        int z = (int)(kz % Z);
+        const float* base = mu + (kz - z) * X * Y;
+        float acc = 0.f;
+        for (int t = 0; t < ntaps; ++t) {
+            ConeTap tp = taps[t];
+            int zz = z + tp.dz, xx = x + tp.dx, yy = y + tp.dy;
+            if (zz < 0 || zz >= Z || xx >= X || yy < 0 || yy >= Y) continue;
+            acc = fmaf(__ldg(base + ((int64_t)zz * X + xx) * Y + yy), tp.w, acc);
+        }
+        out[(kz * X + x) * Y + y] = acc;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Cone path sum, separable mask (mask[dz,dx,dy] = u[dx][dz] * v[dx][dy]).
+// Reference layout (V, Z, X, Y): depth axis X (towards the detector), window
+// axes Z (centred) and Y (centred).  For target depth x and source plane
+// p = x + d:   res[z,x,y] += sum_dz u_d[dz] sum_dy v_d[dy] mu[z+dz-hz, p, y+dy-hy].
+// CTA tile: every z, TY window columns y0.., XB consecutive targets x0...
+// For each source plane p the CTA loads mu[:, p, y0-hy : y0+TY+hy) once and,
+// for each of the XB targets it feeds (d = p - x), runs the y filter then the
+// z filter, accumulating in registers.  Thread t owns window column
+// (t % TY) and 8 consecutive z for all XB targets.
+// ---------------------------------------------------------------------------
+constexpr int kTY = 16;
+constexpr int kXB = 8;
+constexpr int kZB = 8;
+
+struct SepDims {
+    int Z, X, Y, Mz, Mx, My;
+    int hz, hy;
+    int PS;   // smem pitch of a plane row (window axis), floats
+    int PZ;   // smem pitch of an X-filtered column (z axis, zero padded), floats
+    int MzP, MyP;  // tap counts padded to a multiple of 4
+};
+
+__host__ __device__ inline int pad4(int n) { return (n + 3) & ~3; }
+__host__ __device__ inline int pitch4mod32(int n) {
+    while ((n & 31) != 4) ++n;
+    return n;
+}
+
+// mode 0: out = res (reference layout); 1: out = exp(-res) (reference layout);
+// 2: beam layout multiply: out_beam[l][a][z][h=Y-1-y][w=x] *= exp(-res),
+//    volume v = a_local * L + l.
+__global__ void __launch_bounds__(512)
+cone_sep_kernel(const float* __restrict__ mu, const float* __restrict__ U,
+                const float* __restrict__ Vw, float* __restrict__ out, SepDims d, int mode,
+                int L, int a_base, int64_t out_a_stride, int64_t out_l_stride) {
+    extern __shared__ __align__(16) float sm[];
+    const int Z = d.Z, X = d.X, Y = d.Y;
+    float* sS = sm;                                  // [Z][PS]
+    float* sX = sS + Z * d.PS;                       // [kXB][kTY][PZ]
+    float* sU = sX + kXB * kTY * d.PZ;               // [kXB][MzP]
+    float* sV = sU + kXB * d.MzP;                    // [kXB][MyP]
+    __shared__ int s_lo_y[kXB], s_hi_y[kXB], s_lo_z[kXB], s_hi_z[kXB], s_act[kXB];
+
+    const int v = blockIdx.z;
+    const int y0 = blockIdx.x * kTY;
+    const int x0 = blockIdx.y * kXB;
+    const float* mu_v = mu + (int64_t)v * Z * X * Y;
+    const int tid = threadIdx.x;
+    const int nthr = blockDim.x;
+    const int t = tid % kTY;          // window column owned in the z filter
+    const int zb = tid / kTY;         // z block owned in the z filter
+    const int zs = zb * kZB;
+
+    float acc[kXB][kZB];
+#pragma unroll
+    for (int j = 0; j < kXB; ++j)
+#pragma unroll
+        for (int q = 0; q < kZB; ++q) acc[j][q] = 0.f;
+
+    // zero the z padding of the X buffer once (rows outside [hz, hz+Z) stay 0)
+    for (int i = tid; i < kXB * kTY * d.PZ; i += nthr) sX[i] = 0.f;
+
+    const int p_end = min(X, x0 + kXB - 1 + d.Mx);
+    for (int p = x0; p < p_end; ++p) {
+        __syncthreads();
+        // ---- load plane p window rows: sS[z][c] = mu[z][p][y0 - hy + c] ----
+        const int W_in = kTY + d.MyP + 4;
+        for (int i = tid; i < Z * W_in; i += nthr) {
+            int z = i / W_in, c = i - z * W_in;
+            int y = y0 - d.hy + c;
+            float val = 0.f;
+            if (y >= 0 && y < Y && c < kTY + d.My - 1) val = __ldg(mu_v + ((int64_t)z * X + p) * Y + y);
+            sS[z * d.PS + c] = val;
+        }
+        // ---- filters of the targets this plane feeds ----
+        if (tid < kXB) {
+            int dd = p - (x0 + tid);
+            int act = (dd >= 0 && dd < d.Mx && x0 + tid < X) ? 1 : 0;
+            s_act[tid] = act;
+            int lo_y = d.My, hi_y = 0, lo_z = d.Mz, hi_z = 0;
+            for (int k = 0; k < d.MyP; ++k) {
+                float wv = (act && k < d.My) ? Vw[dd * d.My + k] : 0.f;
+                sV[tid * d.MyP + k] = wv;
+                if (wv != 0.f) { lo_y = min(lo_y, k); hi_y = max(hi_y, k + 1); }
+            }
+            for (int k = 0; k < d.MzP; ++k) {
+                float wu = (act && k < d.Mz) ? U[dd * d.Mz + k] : 0.f;
+                sU[tid * d.MzP + k] = wu;
+                if (wu != 0.f) { lo_z = min(lo_z, k); hi_z = max(hi_z, k + 1); }
+            }
+            if (hi_y <= lo_y || hi_z <= lo_z) s_act[tid] = 0;
+            s_lo_y[tid] = lo_y & ~3;
+            s_hi_y[tid] = hi_y;
+            s_lo_z[tid] = lo_z & ~3;
+            s_hi_z[tid] = hi_z;
+        }
+        __syncthreads();
+        // ---- y filter: X[j][t][hz+z] = sum_k v_j[k] * S[z][t+k] ----
+        for (int pair = tid; pair < kXB * Z; pair += nthr) {
+            int j = pair / Z, z = pair - j * Z;
+            if (!s_act[j]) continue;
+            float xa[kTY];
+#pragma unroll
+            for (int q = 0; q < kTY; ++q) xa[q] = 0.f;
+            const float* row = sS + z * d.PS;
+            const float* vw = sV + j * d.MyP;
+            for (int k0 = s_lo_y[j]; k0 < s_hi_y[j]; k0 += 4) {
+                float4 wv = *reinterpret_cast<const float4*>(vw + k0);
+                float win[kTY + 4];
+#pragma unroll
+                for (int q = 0; q < (kTY + 4) / 4; ++q) {
+                    float4 f = *reinterpret_cast<const float4*>(row + k0 + 4 * q);
+                    win[4 * q] = f.x; win[4 * q + 1] = f.y; win[4 * q + 2] = f.z; win[4 * q + 3] = f.w;
+                }
+#pragma unroll
+                for (int q = 0; q < kTY; ++q) {
+                    xa[q] = fmaf(wv.x, win[q], xa[q]);
+                    xa[q] = fmaf(wv.y, win[q + 1], xa[q]);
+                    xa[q] = fmaf(wv.z, win[q + 2], xa[q]);
+                    xa[q] = fmaf(wv.w, win[q + 3], xa[q]);
+                }
+            }
+            float* xo = sX + (j * kTY) * d.PZ + d.hz + z;
+#pragma unroll
+            for (int q = 0; q < kTY; ++q) xo[q * d.PZ] = xa[q];
+        }
+        __syncthreads();
+        // ---- z filter: acc[j][q] += sum_k u_j[k] * X[j][t][zs+q+k] ----
+        if (zs < Z) {
+#pragma unroll
+            for (int j = 0; j < kXB; ++j) {
+                if (!s_act[j]) continue;
+                const float* col = sX + (j * kTY + t) * d.PZ + zs;
+                const float* uw = sU + j * d.MzP;
+                for (int k0 = s_lo_z[j]; k0 < s_hi_z[j]; k0 += 4) {
+                    float4 wu = *reinterpret_cast<const float4*>(uw + k0);
+                    float win[kZB + 4];
+#pragma unroll
+                    for (int q = 0; q < (kZB + 4) / 4; ++q) {
+                        float4 f = *reinterpret_cast<const float4*>(col + k0 + 4 * q);
+                        win[4 * q] = f.x; win[4 * q + 1] = f.y; win[4 * q + 2] = f.z; win[4 * q + 3] = f.w;
+                    }
+#pragma unroll
+                    for (int q = 0; q < kZB; ++q) {
+                        acc[j][q] = fmaf(wu.x, win[q], acc[j][q]);
+                        acc[j][q] = fmaf(wu.y, win[q + 1], acc[j][q]);
+                        acc[j][q] = fmaf(wu.z, win[q + 2], acc[j][q]);
+                        acc[j][q] = fmaf(wu.w, win[q + 3], acc[j][q]);
+                    }
+                }
+            }
+        }
+    }
+    // ---- epilogue ----
+    const int y = y0 + t;
+    if (zs >= Z || y >= Y) return;
+    if (mode == 2) {
+        const int al = v / L, l = v - al * L;
+        float* ob = out + l * out_l_stride + (int64_t)(a_base + al) * out_a_stride;
+        const int h = Y - 1 - y;
+#pragma unroll
+        for (int q = 0; q < kZB; ++q) {
+            int z = zs + q;
+            if (z >= Z) break;
+            float* o = ob + ((int64_t)z * Y + h) * X + x0;
+#pragma unroll
+            for (int j = 0; j < kXB; ++j)
+                if (x0 + j < X) o[j] *= expf(-acc[j][q]);
+        }
+    } else {
+        float* ov = out + (int64_t)v * Z * X * Y;
+#pragma unroll
+        for (int q = 0; q < kZB; ++q) {
+            int z = zs + q;
+            if (z >= Z) break;
+#pragma unroll
+            for (int j = 0; j < kXB; ++j) {
+                if (x0 + j >= X) continue;
+                float r = acc[j][q];
+                ov[((int64_t)z * X + x0 + j) * Y + y] = mode == 1 ? expf(-r) : r;
+            }
+        }
+    }
+}
+
+SepDims sep_dims(int64_t Z, int64_t X, int64_t Y, int64_t Mz, int64_t Mx, int64_t My) {
+    SepDims d;
+    d.Z = (int)Z; d.X = (int)X; d.Y = (int)Y;
+    d.Mz = (int)Mz; d.Mx = (int)Mx; d.My = (int)My;
+    d.hz = (int)Mz / 2; d.hy = (int)My / 2;
+    d.MzP = pad4((int)Mz);
+    d.MyP = pad4((int)My);
+    d.PS = pitch4mod32(kTY + d.MyP + 4);
+    d.PZ = pitch4mod32((int)Z + 2 * d.hz + d.MzP + 12);
+    return d;
+}
+
+size_t sep_smem(const SepDims& d) {
+    return sizeof(float) * ((size_t)d.Z * d.PS + (size_t)kXB * kTY * d.PZ + kXB * (d.MzP + d.MyP));
+}
+
+int sep_threads(int Z) { return kTY * ((Z + kZB - 1) / kZB); }
+constexpr int kSepMaxThreads = 512;
+
+}  // namespace
+
+int cone_sep_launch(const float* mu, const float* U, const float* Vw, float* out, int64_t Vn,
+                    int64_t Z, int64_t X, int64_t Y, int64_t Mz, int64_t Mx, int64_t My, int mode,
+                    int L, int a_base, int64_t out_a_stride, int64_t out_l_stride,
+                    cudaStream_t st) {
+    SepDims d = sep_dims(Z, X, Y, Mz, Mx, My);
+    size_t smem = sep_smem(d);
+    int threads = sep_threads((int)Z);
+    if (threads > kSepMaxThreads || smem > (size_t)max_smem_optin()) {
+        set_error("separable cone: Z=%lld Mz=%lld My=%lld needs %d threads / %zu B shared memory",
+                  (long long)Z, (long long)Mz, (long long)My, threads, smem);
+        return FLC_ERR_UNSUPPORTED;
+    }
+    FLC_TRY_CUDA(cudaFuncSetAttribute((const void*)cone_sep_kernel,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    dim3 grid((unsigned)ceil_div(Y, kTY), (unsigned)ceil_div(X, kXB), (unsigned)Vn);
+    cone_sep_kernel<<<grid, threads, smem, st>>>(mu, U, Vw, out, d, mode, L, a_base, out_a_stride,
+                                                 out_l_stride);
+    return check_launch("cone_sep_kernel");
+}
+
+namespace {
+
+// Splits each depth plane of a host mask into u (Mz) x v (My) if it is rank
+// one to FP32 precision.  Returns false otherwise.
+bool factor_mask(const std::vector<float>& m, int64_t Mz, int64_t Mx, int64_t My,
+                 std::vector<float>& U, std::vector<float>& V) {
+    U.assign(Mx * Mz, 0.f);
+    V.assign(Mx * My, 0.f);
+    for (int64_t dx = 0; dx < Mx; ++dx) {
+        double best = 0.0;
+        int64_t bi = 0, bj = 0;
+        for (int64_t i = 0; i < Mz; ++i)
+            for (int64_t j = 0; j < My; ++j) {
+                double a = fabs((double)m[(i * Mx + dx) * My + j]);
+                if (a > best) { best = a; bi = i; bj = j; }
+            }
+        if (best == 0.0) continue;
+        double piv = m[(bi * Mx + dx) * My + bj];
+        for (int64_t i = 0; i < Mz; ++i) U[dx * Mz + i] = m[(i * Mx + dx) * My + bj];
+        for (int64_t j = 0; j < My; ++j) V[dx * My + j] = (float)(m[(bi * Mx + dx) * My + j] / piv);
+        for (int64_t i = 0; i < Mz; ++i)
+            for (int64_t j = 0; j < My; ++j) {
+                double e = fabs((double)U[dx * Mz + i] * V[dx * My + j] - m[(i * Mx + dx) * My + j]);
+                if (e > 1e-6 * best) return false;
+            }
+    }
+    return true;
+}
+
+}  // namespace
+
+int rotate_launch(const float* x, float* out, int64_t N, int64_t H, int64_t W, float c, float s,
+                  cudaStream_t st) {
+    RotGeom g = rot_geom(c, s, (int)H, (int)W);
+    dim3 grid((unsigned)ceil_div(W, 128), (unsigned)H, (unsigned)(N < 65535 ? N : 65535));
+    rotate_kernel<<<grid, 128, 0, st>>>(x, out, N, (int)H, (int)W, g);
+    return check_launch("rotate_kernel");
+}
+
+namespace {
+
+__global__ void fill_coef_kernel(const float* __restrict__ theta, const float* __restrict__ coef_x,
+                                 const float* __restrict__ coef_f, AngleCoef* __restrict__ out,
+                                 int A, int n_ch, int L) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= A) return;
+    AngleCoef k;
+    // the reference rounds math.cos/sin of the angle to an FP32 matrix
+    double th = (double)theta[a];
+    k.cos_t = (float)cos(th);
+    k.sin_t = (float)sin(th);
+    for (int j = 0; j < kMaxCh; ++j) k.cx[j] = j < n_ch ? coef_x[a * n_ch + j] : 0.f;
+    for (int i = 0; i < kMaxL; ++i)
+        for (int j = 0; j < kMaxCh; ++j)
+            k.cf[i][j] = (i < L && j < n_ch) ? coef_f[((int64_t)a * L + i) * n_ch + j] : 0.f;
+    out[a] = k;
+}
+
+size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
+
+int64_t pick_chunk(int64_t S, int64_t H, int64_t W, int64_t A, int64_t L, int64_t chunk) {
+    if (chunk <= 0) {
+        int64_t vol = L * S * H * W * (int64_t)sizeof(float);
+        chunk = (64LL << 20) / (vol > 0 ? vol : 1);
+        if (chunk < 1) chunk = 1;
+    }
+    if (chunk > A) chunk = A;
+    if (chunk * L > 65535) chunk = 65535 / L;
+    return chunk < 1 ? 1 : chunk;
+}
+
+size_t atten_ws_bytes(int64_t S, int64_t H, int64_t W, int64_t A, int64_t L, int64_t chunk) {
+    chunk = pick_chunk(S, H, W, A, L, chunk);
+    return align256(sizeof(AngleCoef) * A) + align256(sizeof(float) * chunk * L * S * H * W);
+}
+
+}  // namespace
+
+int atten_maps_launch(const float* frac, const float* theta, const float* coef_x,
+                      const float* coef_f, const float* u, const float* v, float* out,
+                      int64_t n_ch, int64_t S, int64_t H, int64_t W, int64_t A, int64_t L,
+                      int64_t Mz, int64_t Mx, int64_t My, int incident_mode, int xrf_mode,
+                      int64_t chunk, void* workspace, cudaStream_t st) {
+    chunk = pick_chunk(S, H, W, A, L, chunk);
+    AngleCoef* coefs = (AngleCoef*)workspace;
+    float* mu_ref = (float*)((char*)workspace + align256(sizeof(AngleCoef) * A));
+    fill_coef_kernel<<<(unsigned)ceil_div(A, 128), 128, 0, st>>>(theta, coef_x, coef_f, coefs,
+                                                                  (int)A, (int)n_ch, (int)L);
+    FLC_TRY(check_launch("fill_coef_kernel"));
+    const int64_t out_a = S * H * W, out_l = A * S * H * W;
+    const size_t stage_smem = sizeof(float) * (size_t)L * kStageRows * W;
+    FLC_TRY_CUDA(cudaFuncSetAttribute((const void*)atten_stage_kernel,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_smem));
+    const int threads = (int)((W + 31) & ~31);
+    for (int64_t a0 = 0; a0 < A; a0 += chunk) {
+        int n_a = (int)(A - a0 < chunk ? A - a0 : chunk);
+        atten_stage_kernel<<<dim3((unsigned)S, (unsigned)n_a), threads, stage_smem, st>>>(
+            frac, coefs, out, mu_ref, (int)n_ch, (int)S, (int)H, (int)W, (int)L, out_a, out_l,
+            (int)a0, incident_mode, xrf_mode == 0);
+        FLC_TRY(check_launch("atten_stage_kernel"));
+        if (xrf_mode != 0) continue;
+        // reference frame of the cone: (Z=S, X=W, Y=H)
+        FLC_TRY(cone_sep_launch(mu_ref, u, v, out, (int64_t)n_a * L, S, W, H, Mz, Mx, My, 2,
+                                (int)L, (int)a0, out_a, out_l, st));
+    }
+    return FLC_OK;
+}
+
+}  // namespace flc
+
+using namespace flc;
+
+extern "C" int flc_rotate(const float* x, float* out, int64_t N, int64_t H, int64_t W,
+                          float cos_t, float sin_t, void* stream) {
+    clear_error();
+    FLC_REQUIRE(x && out, "flc_rotate: null pointer argument");
+    FLC_REQUIRE(N >= 1 && H >= 1 && W >= 1, "flc_rotate: sizes must be positive");
+    return rotate_launch(x, out, N, H, W, cos_t, sin_t, as_stream(stream));
+}
+
+extern "C" int flc_incident_scan(const float* mu, float* out, int64_t N, int64_t H, int64_t W,
+                                 void* stream) {
+    clear_error();
+    FLC_REQUIRE(mu && out, "flc_incident_scan: null pointer argument");
+    FLC_REQUIRE(N >= 1 && H >= 1 && W >= 1, "flc_incident_scan: sizes must be positive");
+    int64_t n = N * W;
+    incident_scan_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, as_stream(stream)>>>(mu, out, N,
+                                                                                   (int)H, (int)W);
+    return check_launch("incident_scan_kernel");
+}
+
+extern "C" int flc_cone_atten_separable(const float* mu, const float* u, const float* v,
+                                        float* out, int64_t K, int64_t Z, int64_t X, int64_t Y,
+                                        int64_t Mz, int64_t Mx, int64_t My, int mode,
+                                        void* stream) {
+    clear_error();
+    FLC_REQUIRE(mu && u && v && out, "flc_cone_atten_separable: null pointer argument");
+    FLC_REQUIRE(K >= 1 && Z >= 1 && X >= 1 && Y >= 1 && Mz >= 1 && Mx >= 1 && My >= 1,
+                "flc_cone_atten_separable: sizes must be positive");
+    FLC_REQUIRE(mode == 0 || mode == 1, "flc_cone_atten_separable: mode must be 0 or 1");
+    FLC_REQUIRE(K <= 65535, "flc_cone_atten_separable: K must be <= 65535");
+    return cone_sep_launch(mu, u, v, out, K, Z, X, Y, Mz, Mx, My, mode, 1, 0, 0, 0,
+                           as_stream(stream));
+}
+
+extern "C" int flc_cone_atten(const float* mu, const float* mask, float* out, int64_t K,
+                              int64_t Z, int64_t X, int64_t Y, int64_t Mz, int64_t Mx, int64_t My,
+                              int flags, void* stream) {
+    clear_error();
+    FLC_REQUIRE(mu && mask && out, "flc_cone_atten: null pointer argument");
+    FLC_REQUIRE(K >= 1 && Z >= 1 && X >= 1 && Y >= 1 && Mz >= 1 && Mx >= 1 && My >= 1,
+                "flc_cone_atten: sizes must be positive");
+    FLC_REQUIRE(K * Z <= 2147483647LL && X <= 65535, "flc_cone_atten: volume too large");
+    cudaStream_t st = as_stream(stream);
+    std::vector<float> hm((size_t)(Mz * Mx * My));
+    FLC_TRY_CUDA(cudaMemcpyAsync(hm.data(), mask, sizeof(float) * hm.size(), cudaMemcpyDeviceToHost, st));
+    FLC_TRY_CUDA(cudaStreamSynchronize(st));
+    std::vector<float> U, V;
+    bool sep = !(flags & FLC_CONE_FORCE_GENERAL) && factor_mask(hm, Mz, Mx, My, U, V) &&
+               K <= 65535 && sep_threads((int)Z) <= kSepMaxThreads &&
+               sep_smem(sep_dims(Z, X, Y, Mz, Mx, My)) <= (size_t)max_smem_optin();
+    if (sep) {
+        float* dbuf = nullptr;
+        size_t bytes = sizeof(float) * (U.size() + V.size());
+        FLC_TRY_CUDA(cudaMallocAsync((void**)&dbuf, bytes, st));
+        int s = FLC_OK;
+        cudaError_t e = cudaMemcpyAsync(dbuf, U.data(), sizeof(float) * U.size(), cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(dbuf + U.size(), V.data(), sizeof(float) * V.size(), cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) s = cuda_fail(e, "cudaMemcpyAsync");
+        if (s == FLC_OK)
+            s = cone_sep_launch(mu, dbuf, dbuf + U.size(), out, K, Z, X, Y, Mz, Mx, My, 0, 1, 0, 0, 0, st);
+        cudaFreeAsync(dbuf, st);
+        // the host vectors are read by the copies above before they return
+        cudaStreamSynchronize(st);
+        return s;
+    }
+    std::vector<ConeTap> taps;
+    for (int64_t dz = 0; dz < Mz; ++dz)
+        for (int64_t dx = 0; dx < Mx; ++dx)
+            for (int64_t dy = 0; dy < My; ++dy) {
+                float w = hm[(dz * Mx + dx) * My + dy];
+                if (w != 0.f) taps.push_back({(int)(dz - Mz / 2), (int)dx, (int)(dy - My / 2), w});
+            }
+    if (taps.empty()) {
+        FLC_TRY_CUDA(cudaMemsetAsync(out, 0, sizeof(float) * K * Z * X * Y, st));
+        return FLC_OK;
+    }
+    ConeTap* dt = nullptr;
+    FLC_TRY_CUDA(cudaMallocAsync((void**)&dt, sizeof(ConeTap) * taps.size(), st));
+    int s = FLC_OK;
+    cudaError_t e = cudaMemcpyAsync(dt, taps.data(), sizeof(ConeTap) * taps.size(), cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) s = cuda_fail(e, "cudaMemcpyAsync");
+    if (s == FLC_OK) {
+        dim3 grid((unsigned)ceil_div(Y, 128), (unsigned)X, (unsigned)(K * Z < 65535 ? K * Z : 65535));
+        cone_general_kernel<<<grid, 128, 0, st>>>(mu, dt, (int)taps.size(), out, K * Z, (int)Z,
+                                                  (int)X, (int)Y);
+        s = check_launch("cone_general_kernel");
+    }
+    cudaFreeAsync(dt, st);
+    cudaStreamSynchronize(st);
+    return s;
+}
+
+extern "C" size_t flc_atten_workspace_bytes(int64_t n_ch, int64_t S, int64_t H, int64_t W,
+                                            int64_t A, int64_t L, int64_t chunk) {
+    if (n_ch < 1 || S < 1 || H < 1 || W < 1 || A < 1 || L < 1) return 0;
+    return atten_ws_bytes(S, H, W, A, L, chunk);
+}
+
+extern "C" int flc_atten_maps(const float* frac, const float* theta, const float* coef_x,
+                              const float* coef_f, const float* u, const float* v, float* out,
+                              int64_t n_ch, int64_t S, int64_t H, int64_t W, int64_t A, int64_t L,
+                              int64_t Mz, int64_t Mx, int64_t My, int incident_mode, int xrf_mode,
+                              int64_t chunk, void* workspace, size_t workspace_bytes,
+                              void* stream) {
+    clear_error();
+    FLC_REQUIRE(frac && theta && coef_x && coef_f && out && workspace,
+                "flc_atten_maps: null pointer argument");
+    FLC_REQUIRE(xrf_mode != 0 || (u && v), "flc_atten_maps: mask factors required");
+    FLC_REQUIRE(n_ch >= 1 && n_ch <= kMaxCh, "flc_atten_maps: 1 <= n_ch <= %d", kMaxCh);
+    FLC_REQUIRE(L >= 1 && L <= kMaxL, "flc_atten_maps: 1 <= L <= %d", kMaxL);
+    FLC_REQUIRE(S >= 1 && S <= 65535 && A >= 1 && A <= 65535, "flc_atten_maps: S, A in [1, 65535]");
+    FLC_REQUIRE(H == W && H >= 2 && W <= 1024,
+                "flc_atten_maps: needs square slices H == W in [2, 1024] (the reference's rot90 "
+                "does too)");
+    FLC_REQUIRE(incident_mode >= 0 && incident_mode <= 2 && (xrf_mode == 0 || xrf_mode == 1),
+                "flc_atten_maps: bad mode");
+    FLC_REQUIRE(xrf_mode != 0 || (Mz >= 1 && Mx >= 1 && My >= 1), "flc_atten_maps: bad mask size");
+    if (((uintptr_t)workspace & 255) != 0) {
+        set_error("flc_atten_maps: workspace must be 256-byte aligned");
+        return FLC_ERR_ALIGNMENT;
+    }
+    size_t need = atten_ws_bytes(S, H, W, A, L, chunk);
+    if (workspace_bytes < need) {
+        set_error("flc_atten_maps: workspace of %zu bytes is smaller than the %zu required",
+                  workspace_bytes, need);
+        return FLC_ERR_WORKSPACE;
+    }
+    return atten_maps_launch(frac, theta, coef_x, coef_f, u, v, out, n_ch, S, H, W, A, L, Mz, Mx,
+                             My, incident_mode, xrf_mode, chunk, workspace, as_stream(stream));
+}

@@ -1,0 +1,67 @@
+"""Image rotation helpers with the signatures of FL/torch_image_util.py.
+
+``torch_rotate_image_nd`` runs the native grid_sample-equivalent rotation
+(bilinear, zero padding, align_corners=False, same-size output) for CUDA
+tensors.  The rot90 helpers are pure index permutations (transpose + flip)
+and stay as torch views/copies.
+"""
+import math
+
+import torch
+
+from . import _lib
+
+__all__ = ["torch_rotate_image_nd", "torch_rot90_3D", "torch_rot90_4D"]
+
+
+def _angle(theta):
+    if isinstance(theta, torch.Tensor):
+        return float(theta.detach().cpu().double())
+    return float(theta)
+
+
+def torch_rotate_image_nd(x, theta, enable_crop=True, align_corners=False, mode="bilinear",
+                          padding_mode="zeros"):
+    """Rotate (..., H, W) by theta radians counter-clockwise about the image
+    centre (FL/torch_image_util.py:13-114).  Supports the configuration the
+    hot path uses: enable_crop=True, bilinear, zero padding,
+    align_corners=False; other settings raise NotImplementedError."""
+    if not enable_crop or align_corners or mode != "bilinear" or padding_mode != "zeros":
+        raise NotImplementedError("torch_rotate_image_nd: only enable_crop=True, bilinear, "
+                                  "zeros padding, align_corners=False are implemented")
+    if x.dim() < 2:
+        raise ValueError("Input must have at least 2 dimensions")
+    _lib.require_cuda("torch_rotate_image_nd", x)
+    th = _angle(theta)
+    # the reference builds an FP32 matrix from math.cos / math.sin
+    c = float(torch.tensor(math.cos(th), dtype=torch.float32))
+    s = float(torch.tensor(math.sin(th), dtype=torch.float32))
+    H, W = x.shape[-2:]
+    xc = x.contiguous()
+    out = torch.empty_like(xc)
+    with torch.cuda.device(x.device):
+        _lib.call("flc_rotate", _lib.ptr(xc), _lib.ptr(out), xc.numel() // (H * W), H, W, c, s,
+                  _lib.stream())
+    return out
+
+
+def torch_rot90_3D(img_raw, ax=0, mode="c-clock"):
+    """90-degree rotation of a 3-D array about axis `ax` (FL/torch_image_util.py:117-147).
+    'clock' is -90 degrees, 'c-clock' +90 degrees."""
+    dims = {0: (1, 2), 1: (0, 2), 2: (0, 1)}[ax]
+    img = img_raw.transpose(*dims)
+    if mode == "clock":
+        img = img.flip(dims=({0: 2, 1: 2, 2: 0}[ax],))
+    elif mode == "c-clock":
+        img = img.flip(dims=({0: 1, 1: 0, 2: 1}[ax],))
+    return img.clone() if img.data_ptr() == img_raw.data_ptr() else img.contiguous()
+
+
+def torch_rot90_4D(img4D, ax=0, mode="c-clock"):
+    """torch_rot90_3D applied to every channel of (C, ., ., .) (FL/torch_image_util.py:150-155).
+    Like the reference, the result keeps the input's shape, so the rotated
+    axes must have equal length."""
+    out = torch.stack([torch_rot90_3D(img4D[i], ax, mode) for i in range(img4D.shape[0])])
+    if out.shape != img4D.shape:
+        raise RuntimeError("torch_rot90_4D: rotated axes must have equal length")
+    return out

@@ -1,0 +1,161 @@
+/*
+ * flc.h -- C ABI of the B200 (sm_100a) XRF self-absorption hot path.
+ *
+ * This library replaces the native layer of FL_correction
+ * (FL/cuda_lib/atten_cuda.cpp + FL/cuda_lib/atten_cuda_kernel.cu).  Every
+ * entry point takes plain device pointers, 64-bit sizes and a CUDA stream
+ * (cudaStream_t passed as void*, NULL = legacy default stream), allocates
+ * nothing unless it says so, and returns an flc_status.  It never aborts;
+ * flc_last_error() returns a message describing the last failure on the
+ * calling host thread.
+ *
+ * Layouts are C-contiguous float32 unless stated:
+ *   atten  (A, B, H, W)   attenuation per angle, slice, row, column
+ *   C      (R, B, H, W)   concentration per reference, slice, row, column
+ *   em     (A, R)         emission cross-section per angle and reference
+ *   theta  (A)            angles in radians
+ *   Pf     (A, B, W)      projection per angle, slice, detector column
+ * The single-slice reference functions are the B == 1 case.
+ */
+#ifndef FLC_H
+#define FLC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define FLC_API __attribute__((visibility("default")))
+#else
+#define FLC_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    FLC_OK = 0,
+    FLC_ERR_INVALID_ARG = 1,  /* null pointer, non-positive or inconsistent size */
+    FLC_ERR_UNSUPPORTED = 2,  /* valid request outside what this build supports */
+    FLC_ERR_ALIGNMENT = 3,    /* pointer not aligned as the entry point requires */
+    FLC_ERR_WORKSPACE = 4,    /* caller-provided workspace too small */
+    FLC_ERR_CUDA = 5,         /* CUDA runtime / launch error */
+    FLC_ERR_TIMEOUT = 6,      /* a bounded device-side wait gave up */
+    FLC_ERR_OOM = 7           /* an entry point that allocates could not */
+} flc_status;
+
+/* Human-readable name of a status code. */
+FLC_API const char* flc_status_string(int status);
+/* Message for the last failure on this host thread ("" if none). */
+FLC_API const char* flc_last_error(void);
+/* Library version string. */
+FLC_API const char* flc_version(void);
+
+/* ---------------------------------------------------------------------
+ * Cone-mask (fluorescence) path sum, reference layout.
+ * Replaces cal_atten_cuda / atten_kernel
+ * (FL/cuda_lib/atten_cuda.cpp:12-28, atten_cuda_kernel.cu:10-86):
+ *   out[k,z,x,y] = sum_{dz,dx,dy} mask[dz,dx,dy] * mu[k, z+dz-Mz/2, x+dx, y+dy-My/2]
+ * with taps outside the volume skipped.  mu (K,Z,X,Y), mask (Mz,Mx,My).
+ * When every depth plane mask[:,dx,:] is rank one (true of the masks that
+ * FL.detector_mask builds) the separable kernel runs; otherwise a general
+ * gather over the non-zero taps.  `flags` is a bit set of FLC_CONE_*.
+ * --------------------------------------------------------------------- */
+#define FLC_CONE_FORCE_GENERAL 1  /* skip the rank-one test, use the general kernel */
+FLC_API int flc_cone_atten(const float* mu, const float* mask, float* out,
+                   int64_t K, int64_t Z, int64_t X, int64_t Y,
+                   int64_t Mz, int64_t Mx, int64_t My, int flags, void* stream);
+
+/* Separable cone path sum with a caller-factored mask:
+ *   mask[dz,dx,dy] == u[dx*Mz + dz] * v[dx*My + dy].
+ * mode: 0 writes the sum, 1 writes exp(-sum), 2 multiplies exp(-sum) into out.
+ * No counterpart entry point in the reference (it is the fast path of
+ * cal_atten_cuda, atten_cuda.cpp:12-28). */
+FLC_API int flc_cone_atten_separable(const float* mu, const float* u, const float* v, float* out,
+                             int64_t K, int64_t Z, int64_t X, int64_t Y,
+                             int64_t Mz, int64_t Mx, int64_t My, int mode, void* stream);
+
+/* ---------------------------------------------------------------------
+ * Attenuated emission projector.
+ * forward: Pf[a,b,w] = sum_h atten[a,b,h,w] * sum_r em[a,r] * bilerp(C[r,b], row(a,h,w), col(a,h,w))
+ *   Replaces forward_emission_batch / forward_emission
+ *   (atten_cuda.cpp:142-182 / :82-108; kernels atten_cuda_kernel.cu:298-337 / :91-142).
+ * backward: out[r,b] = exact transpose of the forward applied to ratio (A,B,W).
+ *   Replaces backward_emission_batch / backward_emission
+ *   (atten_cuda.cpp:188-214 / :113-135; kernels :390-446 / :177-231).
+ * The sample point is the reference's: rotation about ((H-1)/2,(W-1)/2),
+ * clamp to [0,H-1.001]x[0,W-1.001], bilinear.  Requires H, W >= 2.
+ * --------------------------------------------------------------------- */
+FLC_API int flc_fwd_emission(const float* atten, const float* C, const float* em, const float* theta,
+                     float* Pf, int64_t A, int64_t B, int64_t R, int64_t H, int64_t W,
+                     void* stream);
+FLC_API int flc_bwd_emission(const float* atten, const float* ratio, const float* em,
+                     const float* theta, float* out, int64_t A, int64_t B, int64_t R,
+                     int64_t H, int64_t W, void* stream);
+
+/* Huber gradient over the four in-plane neighbours of each pixel of
+ * C (RB, H, W).  Replaces huber_grad[_batch]
+ * (atten_cuda.cpp:218-238; atten_cuda_kernel.cu:495-616). */
+FLC_API int flc_huber_grad(const float* C, float* grad, int64_t RB, int64_t H, int64_t W,
+                   float delta, void* stream);
+
+/* ---------------------------------------------------------------------
+ * MLEM with optional Huber regularisation, device resident.
+ * Replaces mlem_cuda_batch / mlem_cuda (atten_cuda.cpp:283-345 / :244-281).
+ * C (R,B,H,W) holds C_init on entry and the result on return (the caller
+ * copies C_init first, as the reference's clone does).  I is (A,B,W).
+ * The caller provides `workspace` of at least flc_mlem_workspace_bytes(...)
+ * bytes (256-byte aligned).  With use_graph != 0 the iteration is captured
+ * once into a CUDA graph and replayed n_iter times.
+ * --------------------------------------------------------------------- */
+FLC_API size_t flc_mlem_workspace_bytes(int64_t A, int64_t B, int64_t R, int64_t H, int64_t W);
+FLC_API int flc_mlem(float* C, const float* atten, const float* em, const float* theta,
+             const float* I, int64_t n_iter, double beta, double delta,
+             int64_t A, int64_t B, int64_t R, int64_t H, int64_t W,
+             void* workspace, size_t workspace_bytes, int use_graph, void* stream);
+
+/* ---------------------------------------------------------------------
+ * Per-angle attenuation maps (rotation + mu assembly + incident scan +
+ * fluorescence cone + product), the path of FL.core.cal_xrf_atten_at_angles,
+ * cal_xray_atten_at_angles and cal_total_atten_at_angles
+ * (FL/core.py:19-101, FL/torch_functions.py:8-176,
+ * FL/torch_image_util.py:13-155) without the TIFF round trips.
+ *
+ *   frac    (n_ch, S, H, W)   unrotated fractions (H == W)
+ *   theta   (A)               rotation angles, radians
+ *   coef_x  (A, n_ch)         cs[comp_j-x] * rho_j * pix per angle
+ *   coef_f  (A, L, n_ch)      cs[comp_j-elem_i] * rho_j * pix per angle
+ *   u, v                      factored cone mask (see flc_cone_atten_separable)
+ *   out     (L, A, S, H, W)   atten[i] = incident(i) * exp(-cone(mu_f[i]))
+ * incident_mode 0: element i uses channel i only (FL/torch_functions.py:39-50,
+ *   FL/core.py:80-81 -- the current package); 1: product over all channels
+ *   (FL/legacy/FL_correction_core.py:1855-1860).  2: no incident term.
+ * xrf_mode 0: fluorescence term on; 1: off (incident only).
+ * workspace: flc_atten_workspace_bytes(...) bytes; `chunk` angles are
+ * processed per pass (0 = choose).
+ * --------------------------------------------------------------------- */
+FLC_API size_t flc_atten_workspace_bytes(int64_t n_ch, int64_t S, int64_t H, int64_t W, int64_t A,
+                                 int64_t L, int64_t chunk);
+FLC_API int flc_atten_maps(const float* frac, const float* theta, const float* coef_x,
+                   const float* coef_f, const float* u, const float* v, float* out,
+                   int64_t n_ch, int64_t S, int64_t H, int64_t W, int64_t A, int64_t L,
+                   int64_t Mz, int64_t Mx, int64_t My, int incident_mode, int xrf_mode,
+                   int64_t chunk, void* workspace, size_t workspace_bytes, void* stream);
+
+/* Rotation with torch grid_sample semantics (bilinear, zero padding,
+ * align_corners=False, same-size output): out (N, H, W) from x (N, H, W).
+ * cos_t/sin_t are the FP32 matrix entries.  Replaces torch_rotate_image_nd
+ * (FL/torch_image_util.py:13-114, enable_crop=True). */
+FLC_API int flc_rotate(const float* x, float* out, int64_t N, int64_t H, int64_t W,
+               float cos_t, float sin_t, void* stream);
+
+/* Incident attenuation: out[n,h,w] = prod_{h'>h} (1 - mu[n,h',w]), out[n,H-1,w] = 1.
+ * Replaces the flip/cumprod/flip of torch_xray_atten_3D (FL/torch_functions.py:95-102). */
+FLC_API int flc_incident_scan(const float* mu, float* out, int64_t N, int64_t H, int64_t W,
+                      void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FLC_H */

@@ -1,0 +1,215 @@
+"""numpy front end of the C oracle (``oracle/flc_oracle.c``).
+
+TEST INFRASTRUCTURE ONLY: used by tests/, ``__graft_entry__.smoke()`` and the
+CPU-baseline legs of ``bench.py``.  Each wrapper names the reference
+file:line that the C function restates.  Inputs are converted to float64;
+angles stay float32 because the reference evaluates cos/sin of FP32 angles.
+"""
+import ctypes
+import math
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+_i64 = ctypes.c_int64
+_dp = ctypes.POINTER(ctypes.c_double)
+_fp = ctypes.POINTER(ctypes.c_float)
+
+
+def build():
+    """Compile liboracle.so (make) if it is missing or stale."""
+    so = os.path.join(_HERE, "liboracle.so")
+    src = os.path.join(_HERE, "flc_oracle.c")
+    if not os.path.exists(so) or os.path.getmtime(so) < os.path.getmtime(src):
+        subprocess.check_call(["make", "-s", "-C", _HERE])
+    return so
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        so = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(so):
+            build()
+        L = ctypes.CDLL(so)
+        L.orc_max_threads.restype = ctypes.c_int
+        _LIB = L
+    return _LIB
+
+
+def set_threads(n):
+    lib().orc_set_threads(ctypes.c_int(int(n)))
+
+
+def max_threads():
+    return int(lib().orc_max_threads())
+
+
+def _d(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _pd(a):
+    return a.ctypes.data_as(_dp)
+
+
+def _pf(a):
+    return a.ctypes.data_as(_fp)
+
+
+def fp32_cos_sin(theta):
+    """cos/sin as the reference builds its FP32 rotation matrix
+    (FL/torch_image_util.py:77-85: math.cos/sin, then a float32 tensor)."""
+    return float(np.float32(math.cos(float(theta)))), float(np.float32(math.sin(float(theta))))
+
+
+def rotate(x, theta):
+    """grid_sample rotation, FL/torch_image_util.py:13-114 (enable_crop=True)."""
+    x = _d(x)
+    H, W = x.shape[-2:]
+    out = np.empty_like(x)
+    c, s = fp32_cos_sin(theta)
+    lib().orc_rotate(_pd(x), _pd(out), _i64(x.size // (H * W)), _i64(H), _i64(W),
+                     ctypes.c_double(c), ctypes.c_double(s))
+    return out
+
+
+def rotate_adjoint(g, theta):
+    g = _d(g)
+    H, W = g.shape[-2:]
+    out = np.empty_like(g)
+    c, s = fp32_cos_sin(theta)
+    lib().orc_rotate_adjoint(_pd(g), _pd(out), _i64(g.size // (H * W)), _i64(H), _i64(W),
+                             ctypes.c_double(c), ctypes.c_double(s))
+    return out
+
+
+def incident_scan(mu):
+    """Exclusive reverse product of (1-mu) along H, FL/torch_functions.py:95-102."""
+    mu = _d(mu)
+    H, W = mu.shape[-2:]
+    out = np.empty_like(mu)
+    lib().orc_incident_scan(_pd(mu), _pd(out), _i64(mu.size // (H * W)), _i64(H), _i64(W))
+    return out
+
+
+def cone_ref(mu, mask):
+    """atten_kernel, FL/cuda_lib/atten_cuda_kernel.cu:10-57 (K,Z,X,Y layout)."""
+    mu = _d(mu)
+    mask = _d(mask)
+    K, Z, X, Y = mu.shape
+    Mz, Mx, My = mask.shape
+    out = np.empty_like(mu)
+    lib().orc_cone_ref(_pd(mu), _pd(mask), _pd(out), _i64(K), _i64(Z), _i64(X), _i64(Y),
+                       _i64(Mz), _i64(Mx), _i64(My))
+    return out
+
+
+def cone_beam(mu, mask):
+    """rot90 -> atten_kernel -> rot90^-1 (FL/torch_functions.py:142-171),
+    evaluated directly in the unrotated frame; mu is (K,Z,H,W)."""
+    mu = _d(mu)
+    mask = _d(mask)
+    K, Z, H, W = mu.shape
+    Mz, Mx, My = mask.shape
+    out = np.empty_like(mu)
+    lib().orc_cone_beam(_pd(mu), _pd(mask), _pd(out), _i64(K), _i64(Z), _i64(H), _i64(W),
+                        _i64(Mz), _i64(Mx), _i64(My))
+    return out
+
+
+def cone_beam_adjoint(g, mask):
+    g = _d(g)
+    mask = _d(mask)
+    K, Z, H, W = g.shape
+    Mz, Mx, My = mask.shape
+    out = np.empty_like(g)
+    lib().orc_cone_beam_adjoint(_pd(g), _pd(mask), _pd(out), _i64(K), _i64(Z), _i64(H), _i64(W),
+                                _i64(Mz), _i64(Mx), _i64(My))
+    return out
+
+
+def _batchify(atten, C):
+    atten = _d(atten)
+    C = _d(C)
+    if atten.ndim == 3:
+        atten = atten[:, None]
+    if C.ndim == 3:
+        C = C[:, None]
+    return atten, C
+
+
+def fwd_emission(atten, C, em, theta):
+    """forward_emission[_batch], atten_cuda_kernel.cu:91-142 / :298-337.
+    atten (A,[B,]H,W), C (R,[B,]H,W), em (A,R), theta (A) radians -> (A,[B,]W)."""
+    single = np.ndim(atten) == 3
+    atten, C = _batchify(atten, C)
+    A, B, H, W = atten.shape
+    R = C.shape[0]
+    em = _d(em).reshape(A, R)
+    th = np.ascontiguousarray(theta, dtype=np.float32)
+    Pf = np.empty((A, B, W))
+    lib().orc_fwd_emission(_pd(atten), _pd(C), _pd(em), _pf(th), _pd(Pf),
+                           _i64(A), _i64(B), _i64(R), _i64(H), _i64(W))
+    return Pf[:, 0] if single else Pf
+
+
+def bwd_emission(atten, ratio, em, theta):
+    """backward_emission[_batch], atten_cuda_kernel.cu:177-231 / :390-446 -> (R,[B,]H,W)."""
+    single = np.ndim(atten) == 3
+    atten = _d(atten)
+    ratio = _d(ratio)
+    if single:
+        atten = atten[:, None]
+        ratio = ratio[:, None]
+    A, B, H, W = atten.shape
+    em = _d(em)
+    R = em.shape[1]
+    th = np.ascontiguousarray(theta, dtype=np.float32)
+    out = np.empty((R, B, H, W))
+    lib().orc_bwd_emission(_pd(atten), _pd(_d(ratio)), _pd(em), _pf(th), _pd(out),
+                           _i64(A), _i64(B), _i64(R), _i64(H), _i64(W))
+    return out[:, 0] if single else out
+
+
+def fwd_emission_datten(gPf, C, em, theta):
+    """d(sum gPf*Pf)/d(atten) for the batched projector."""
+    C = _d(C)
+    gPf = _d(gPf)
+    R, B, H, W = C.shape
+    A = gPf.shape[0]
+    th = np.ascontiguousarray(theta, dtype=np.float32)
+    out = np.empty((A, B, H, W))
+    lib().orc_fwd_emission_datten(_pd(gPf), _pd(C), _pd(_d(em)), _pf(th), _pd(out),
+                                  _i64(A), _i64(B), _i64(R), _i64(H), _i64(W))
+    return out
+
+
+def huber_grad(C, delta):
+    """huber_grad[_batch], atten_cuda_kernel.cu:495-616."""
+    C = _d(C)
+    H, W = C.shape[-2:]
+    g = np.empty_like(C)
+    lib().orc_huber_grad(_pd(C), _pd(g), _i64(C.size // (H * W)), _i64(H), _i64(W),
+                         ctypes.c_double(delta))
+    return g
+
+
+def mlem(C_init, atten, em, theta, I, n_iter, beta=1e-3, delta=0.01):
+    """mlem_cuda[_batch], FL/cuda_lib/atten_cuda.cpp:244-345."""
+    single = np.ndim(atten) == 3
+    atten, C = _batchify(atten, C_init)
+    I = _d(I)
+    if single:
+        I = I[:, None]
+    A, B, H, W = atten.shape
+    R = C.shape[0]
+    C = C.copy()
+    th = np.ascontiguousarray(theta, dtype=np.float32)
+    lib().orc_mlem(_pd(C), _pd(atten), _pd(_d(em)), _pf(th), _pd(np.ascontiguousarray(I)),
+                   _i64(n_iter), ctypes.c_double(beta), ctypes.c_double(delta),
+                   _i64(A), _i64(B), _i64(R), _i64(H), _i64(W))
+    return C[:, 0] if single else C

@@ -1,0 +1,464 @@
+"""Benchmark: self-absorption-corrected XRF MLEM on B200.
+
+Workload (default): 128^3 volume, 3 elements (Fe, Ni, Cu), 120 angles over
+0-180 deg, seeded Voronoi phantom, cone mask of a 7 mm detector at 30 mm; one
+step = the full corrected reconstruction: 50 MLEM iterations with the
+attenuation maps (rotation, incident scan, cone path sum) recomputed on the
+device from the current estimate every 5 iterations.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line.  `value` = MLEM iterations per second of the whole job
+(all ranks), timed with CUDA events on the launching stream after W warm-up
+steps; `e2e` is the same metric through the host-buffer entry point
+(projections copied host->device and the result device->host inside the
+timed region).  Under torchrun every rank reconstructs its own seeded volume
+(replicas, weak scaling); the timing is the max over ranks.
+
+--impl reference times the reference algorithm on the host cores through the
+FP64 C restatement (oracle/), on a bounded sample of the same job that is
+scaled to the full job (the sample is described in the output line).
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "MLEM iters/s & corrected-proj GB/s (% HBM peak), batched/adjoint vs plain GPU"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--config", type=int, default=1, choices=[0, 1])
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--case", default=None, choices=["cone", "mlem", "fwd", "bwd"],
+                   help="run one kernel on a profiling-sized case instead of the benchmark")
+    return p.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# algorithmic work counts
+# ---------------------------------------------------------------------------
+def mlem_bytes_per_iter(A, S, H, W, R=1):
+    """Bytes of one MLEM iteration of one element at the reference API
+    boundary: forward (atten, C, Pf) + backward (atten, ratio, out) + the
+    elementwise update (C, back, sens read; Huber neighbours; C write)."""
+    fwd = 4 * (A * S * H * W + R * S * H * W + A * S * W)
+    bwd = 4 * (A * S * H * W + A * S * W + R * S * H * W)
+    upd = 4 * 4 * R * S * H * W
+    return fwd + bwd + upd
+
+
+def cone_work(mask, Z, H, W):
+    """(nnz-form MACs, separable MACs) of one cone volume (Z, H, W) with mask
+    (Mz, Mx, My), counting only taps that land inside the volume."""
+    m = np.asarray(mask, np.float64)
+    Mz, Mx, My = m.shape
+    hz, hy = Mz // 2, My // 2
+    zc = np.array([max(0, Z - abs(dz - hz)) for dz in range(Mz)], np.float64)
+    yc = np.array([max(0, H - abs(dy - hy)) for dy in range(My)], np.float64)
+    nnz = 0.0
+    sep = 0.0
+    for dx in range(min(Mx, W)):
+        xc = W - dx
+        p = m[:, dx, :] != 0
+        nnz += xc * float((p * zc[:, None] * yc[None, :]).sum())
+        # separable: per output, taps of the y filter + taps of the z filter
+        wz = int(p.any(axis=1).sum())
+        wy = int(p.any(axis=0).sum())
+        if wz and wy:
+            sep += xc * Z * H * (wz + wy)
+    return nnz, sep
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out = ""
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# workload
+# ---------------------------------------------------------------------------
+def build_problem(cfg, rank, device):
+    import torch
+    from fl_correction_b200 import phantoms
+    from fl_correction_b200.detector_mask import generate_detector_mask
+    from fl_correction_b200.recon import CorrectedMLEM
+    wl = phantoms.make_workload(cfg, seed=20240611 + 1000 * rank)
+    N = wl.N
+    mask = generate_detector_mask(wl.mask_angle, wl.mask_angle, N)
+    solver = CorrectedMLEM(wl.param, wl.angles, mask, (N, N, N), device=device)
+    truth = torch.from_numpy(wl.conc).to(device)
+    solver.recompute_attenuation(truth)
+    I = solver.project(truth)                       # (L, A, S, W)
+    if wl.noise_max_counts:
+        g = torch.Generator(device=device).manual_seed(wl.seed)
+        scale = wl.noise_max_counts / float(I.max())
+        I = torch.poisson(I * scale, generator=g) / scale
+    torch.cuda.synchronize()
+    return wl, mask, solver, I.contiguous()
+
+
+def run_ours(args, rank, world, device):
+    import torch
+    import torch.distributed as dist
+    from fl_correction_b200 import _lib
+    hbm, peak_kind = peaks()
+    wl, mask, solver, I = build_problem(args.config, rank, device)
+    N, L, A = wl.N, len(wl.elements), len(wl.angles)
+    n_iter, k = wl.n_iter, wl.recompute_every
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        solver.run(I, n_iter=n_iter, recompute_every=k)
+    torch.cuda.synchronize()
+
+    # ---- timed region: K full jobs, device resident ---------------------
+    cone_ev, mlem_ev = [], []
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    launches0 = _lib.query("flc_launch_count")
+    with Clocks(torch.cuda.current_device()) as clk:
+        start.record()
+        for _ in range(args.steps):
+            C = solver.run(I, n_iter=n_iter, recompute_every=k, cone_events=cone_ev,
+                           mlem_events=mlem_ev)
+        end.record()
+        torch.cuda.synchronize()
+    barrier()
+    launches = _lib.query("flc_launch_count") - launches0
+    ms = start.elapsed_time(end)
+    t_cone = sum(a.elapsed_time(b) for a, b, _ in cone_ev)
+    t_mlem = sum(a.elapsed_time(b) for a, b, _ in mlem_ev)
+    ms_max = ms
+    if world > 1:
+        t = torch.tensor([ms], device=device, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t)
+
+    # ---- end to end through the host-buffer entry point ----------------
+    I_host = I.cpu().pin_memory()
+    for _ in range(1):
+        solver.run_host(I_host, n_iter=n_iter, recompute_every=k)
+    torch.cuda.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        out_host = solver.run_host(I_host, n_iter=n_iter, recompute_every=k)
+    e1.record()
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=device, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t)
+
+    # ---- derived figures ----------------------------------------------
+    n_cone = sum(v for _, _, v in cone_ev)
+    nnz, sep = cone_work(mask.astype(np.float32), N, N, N)
+    cone_launches = len(cone_ev)
+    cone_avg_ms = t_cone / max(cone_launches, 1)
+    vols_per_launch = n_cone / max(cone_launches, 1)
+    fp32_peak = 148 * 128 * 2 * 1965e6 / 1e12
+    mlem_iters = sum(v for _, _, v in mlem_ev)      # element-iterations timed
+    bytes_it = mlem_bytes_per_iter(A, N, N, N)
+    proj_gbs = bytes_it * mlem_iters / (t_mlem * 1e-3) / 1e9 if t_mlem else None
+    value = world * n_iter * args.steps / (ms_max * 1e-3)
+    e2e_value = world * n_iter * args.steps / (e2e_ms * 1e-3)
+    cone_share = t_cone / ms if ms else 0.0
+    line = {
+        "metric": METRIC,
+        "value": round(value, 3),
+        "unit": "MLEM iters/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms_max / args.steps, 3),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded phantom; no dataset ships with the reference)",
+        "config": {"workload": wl.name, "volume": [N, N, N], "elements": wl.elements,
+                   "angles": A, "mlem_iters": n_iter, "recompute_every": k,
+                   "incident": "own-compound (FL/core.py:80-81)",
+                   "mask": list(mask.shape), "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "inputs larger than L2 (attenuation %.1f GB per step)" % (L * A * N ** 3 * 4 / 1e9)},
+        "corrected_proj_gbs": round(proj_gbs, 1) if proj_gbs else None,
+        "corrected_proj_pct_hbm": round(100 * proj_gbs / hbm, 1) if proj_gbs else None,
+        "time_share": {"cone_sep_kernel": round(cone_share, 3),
+                       "mlem (sens + fused iterations)": round(t_mlem / ms, 3) if ms else None},
+        "roofline": {
+            "kernel": "cone_sep_kernel (fluorescence cone path sum)",
+            "bound": "fp32",
+            "achieved": round(2 * sep * vols_per_launch / (cone_avg_ms * 1e-3) / 1e12, 2),
+            "peak": round(fp32_peak, 1),
+            "unit": "TFLOP/s",
+            "frac": round(2 * sep * vols_per_launch / (cone_avg_ms * 1e-3) / 1e12 / fp32_peak, 3),
+            "traffic": None,
+            "peak_kind": "nominal FP32 (148 SM x 128 lanes x 2 x 1965 MHz); no measured FP32 peak",
+            "algorithmic_unit": "separable FLOPs 2*sum(wz+wy) per output and depth = %.3g per volume" % (2 * sep),
+            "launches": cone_launches, "avg_ms": round(cone_avg_ms, 4),
+            "nnz_form_tflops": round(2 * nnz * vols_per_launch / (cone_avg_ms * 1e-3) / 1e12, 1),
+        },
+        "roofline_mlem": {
+            "kernel": "mlem_iter_kernel (+ sensitivity backward)", "bound": "hbm",
+            "achieved": round(proj_gbs, 1) if proj_gbs else None, "peak": hbm, "unit": "GB/s",
+            "frac": round(proj_gbs / hbm, 3) if proj_gbs else None, "traffic": None,
+            "peak_kind": peak_kind,
+            "algorithmic_unit": "%.4g B per element-iteration (fwd + bwd + update at the reference API boundary)" % bytes_it,
+        },
+        "e2e": {"value": round(e2e_value, 3), "unit": "MLEM iters/s",
+                "h2d_bytes_per_step": int(I_host.numel() * 4),
+                "d2h_bytes_per_step": int(out_host.numel() * 4)},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    return line
+
+
+# ---------------------------------------------------------------------------
+# CPU reference (oracle port on the host cores)
+# ---------------------------------------------------------------------------
+def cpu_sample(cfg):
+    """Time a bounded sample of the full job with the FP64 C restatement and
+    scale it to the full job.  Returns (iters_per_s, description, cores)."""
+    from oracle import oracle as O
+    from fl_correction_b200 import phantoms
+    from fl_correction_b200.core import atten_coefficients
+    from fl_correction_b200.detector_mask import generate_detector_mask
+    wl = phantoms.make_workload(cfg)
+    N, L, A = wl.N, len(wl.elements), len(wl.angles)
+    frac = wl.frac()
+    n_ch = frac.shape[0]
+    cx, cf = atten_coefficients(wl.param, A, n_ch)
+    mask = generate_detector_mask(wl.mask_angle, wl.mask_angle, N)
+    rng = np.random.default_rng(0)
+    cores = O.max_threads()
+    n_rec = math.ceil(wl.n_iter / wl.recompute_every)
+    # (1) rotation + mu assembly + incident scan for n_st angles, all slices
+    n_st = 4
+    t0 = time.perf_counter()
+    for a in range(n_st):
+        th = wl.angles[7 + a] / 180 * math.pi
+        fr = O.rotate(frac, th)
+        mux = fr * cx[7 + a][:, None, None, None]
+        O.incident_scan(mux[:L])
+        muf = np.einsum("ij,jshw->ishw", cf[7 + a].astype(np.float64), fr)
+    t_stage = (time.perf_counter() - t0) / n_st
+    # (2) cone path sum for zs of N output slices of one line at one angle
+    zs = max(1, N // 8)
+    t0 = time.perf_counter()
+    O.cone_beam_slab(muf[:1], mask, N // 2, N // 2 + zs)
+    t_cone = time.perf_counter() - t0
+    # (3) one MLEM iteration of one element on Bs of N slices
+    Bs = max(1, N // 4)
+    atten = rng.random((A, Bs, N, N))
+    C = rng.random((1, Bs, N, N))
+    em = np.full((A, 1), 0.02)
+    thetas = (wl.angles / 180 * math.pi).astype(np.float32)
+    t0 = time.perf_counter()
+    Pf = O.fwd_emission(atten, C, em, thetas)
+    ratio = 1.0 / np.maximum(Pf, 1e-6)
+    back = O.bwd_emission(atten, ratio, em, thetas)
+    O.huber_grad(C, 0.01)
+    _ = C * back
+    t_mlem = time.perf_counter() - t0
+    job = (n_rec * (A * t_stage + L * A * (N / zs) * t_cone)
+           + wl.n_iter * L * (N / Bs) * t_mlem)
+    desc = ("oracle port (FP64 C, OpenMP %d threads) timed on: rotation+mu+incident scan of all "
+            "%d channels (%.3f s per angle), cone path sum of %d/%d slices of 1 line at 1 angle "
+            "(%.3f s), 1 MLEM iteration of 1 element on %d/%d slices (%.3f s); scaled linearly to "
+            "the full job (%d recomputes x %d angles x %d lines, %d iterations x %d elements): "
+            "%.1f s" % (cores, n_ch, t_stage, zs, N, t_cone, Bs, N, t_mlem, n_rec, A, L, wl.n_iter, L, job))
+    return wl.n_iter / job, desc, cores, wl
+
+
+def run_reference(args):
+    steps = []
+    desc = cores = wl = None
+    for _ in range(max(1, args.steps)):
+        v, desc, cores, wl = cpu_sample(args.config)
+        steps.append(v)
+    value = statistics.median(steps)
+    return {
+        "impl": "reference",
+        "metric": METRIC, "value": round(value, 6), "unit": "MLEM iters/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(wl.n_iter / value * 1e3, 1), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": wl.name, "volume": [wl.N] * 3, "elements": wl.elements,
+                   "angles": len(wl.angles), "mlem_iters": wl.n_iter,
+                   "recompute_every": wl.recompute_every},
+        "cpu_baseline": {"value": round(value, 6), "unit": "MLEM iters/s", "cores": cores,
+                         "kind": "port", "sample": desc},
+        "e2e": {"value": round(value, 6), "unit": "MLEM iters/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
+def run_case(args):
+    """One kernel on a profiling-sized case (for ncu): W warm-up launches, then
+    one more.  cone: the fluorescence cone of one pipeline chunk at the
+    benchmark size (2 angles x 3 lines of 128^3); mlem: one fused MLEM
+    iteration (plus the sensitivity pass) at 24 angles x 16 slices of 128^2;
+    fwd / bwd: the projector at 120 angles x 16 slices of 128^2."""
+    import torch
+    from fl_correction_b200 import _lib
+    from fl_correction_b200.cuda_lib import atten_cuda as AC
+    from fl_correction_b200.detector_mask import factor_mask, generate_detector_mask
+    dev = torch.device("cuda", 0)
+    g = torch.Generator(device=dev).manual_seed(0)
+    N = 128
+    if args.case == "cone":
+        n_a, L, A = 2, 3, 120
+        mask = generate_detector_mask(13.309, 13.309, N)
+        u, v = (torch.from_numpy(x).to(dev) for x in factor_mask(mask))
+        mu = torch.rand((n_a, L, N, N, N), device=dev, generator=g) * 0.01
+        atten = torch.ones((L, A, N, N, N), device=dev)
+        def once():
+            _lib.call("flc_cone_atten_apply", _lib.ptr(mu), _lib.ptr(u), _lib.ptr(v),
+                      _lib.ptr(atten), n_a, L, N, N, N, A, 0, *mask.shape, _lib.stream())
+    elif args.case == "mlem":
+        A, B = 24, 16
+        atten = torch.rand((A, B, N, N), device=dev, generator=g)
+        em = torch.full((A, 1), 0.02, device=dev)
+        th = torch.linspace(0, math.pi, A + 1, device=dev)[:-1].contiguous()
+        C0 = torch.ones((1, B, N, N), device=dev)
+        I = AC.forward_emission_batch(atten, C0 * 0.7, em, th)
+        def once():
+            AC.mlem_cuda_batch(C0, atten, em, th, I, 1)
+    elif args.case in ("fwd", "bwd"):
+        A, B = 120, 16
+        atten = torch.rand((A, B, N, N), device=dev, generator=g)
+        em = torch.full((A, 1), 0.02, device=dev)
+        th = torch.linspace(0, math.pi, A + 1, device=dev)[:-1].contiguous()
+        C = torch.rand((1, B, N, N), device=dev, generator=g)
+        r = torch.rand((A, B, N), device=dev, generator=g)
+        if args.case == "fwd":
+            def once():
+                AC.forward_emission_batch(atten, C, em, th)
+        else:
+            def once():
+                AC.backward_emission_batch(atten, r, em, th)
+    else:
+        raise ValueError(args.case)
+    for _ in range(args.warmup):
+        once()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    once()
+    e1.record()
+    torch.cuda.synchronize()
+    print(json.dumps({"case": args.case, "ms": round(e0.elapsed_time(e1), 4)}))
+
+
+def main():
+    args = parse()
+    if args.case:
+        run_case(args)
+        return
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    device = torch.device("cuda", torch.cuda.current_device())
+    line = run_ours(args, rank, world, device)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, desc, cores, _ = cpu_sample(args.config)
+        line["cpu_baseline"] = {"value": round(v, 6), "unit": "MLEM iters/s", "cores": cores,
+                                "kind": "port", "sample": desc}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -24,6 +24,7 @@ SIGNATURES = {
     "flc_status_string": (ctypes.c_char_p, [_int]),
     "flc_last_error": (ctypes.c_char_p, []),
     "flc_version": (ctypes.c_char_p, []),
+    "flc_launch_count": (ctypes.c_uint64, []),
     "flc_cone_atten": (_int, [_vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _i64, _i64, _int, _vp]),
     "flc_cone_atten_separable": (_int, [_vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _i64,
                                         _i64, _int, _vp]),
@@ -36,6 +37,10 @@ SIGNATURES = {
     "flc_atten_workspace_bytes": (_sz, [_i64, _i64, _i64, _i64, _i64, _i64, _i64]),
     "flc_atten_maps": (_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64,
                               _i64, _i64, _i64, _i64, _int, _int, _i64, _vp, _sz, _vp]),
+    "flc_atten_stage": (_int, [_vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _i64,
+                               _i64, _i64, _int, _int, _vp]),
+    "flc_cone_atten_apply": (_int, [_vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _i64, _i64,
+                                    _i64, _i64, _i64, _vp]),
     "flc_rotate": (_int, [_vp, _vp, _i64, _i64, _i64, _f32, _f32, _vp]),
     "flc_incident_scan": (_int, [_vp, _vp, _i64, _i64, _i64, _vp]),
 }

@@ -16,7 +16,7 @@ from .atten_util import extract_single_value_param
 from .cuda_lib.atten_cuda import forward_emission_batch
 from .detector_mask import factor_mask
 
-__all__ = ["atten_coefficients", "mask_factors", "atten_maps", "cal_xrf_atten_at_angles",
+__all__ = ["atten_coefficients", "mask_factors", "atten_maps", "pick_chunk", "cal_xrf_atten_at_angles",
            "cal_xray_atten_at_angles", "cal_total_atten_at_angles", "cal_atten_at_angles",
            "re_projection_cuda"]
 
@@ -52,12 +52,15 @@ def mask_factors(detector_mask, device):
 
 
 def atten_maps(frac_4D, angle_list, coef_x, coef_f, mask_uv=None, incident="own", xrf=True,
-               out=None, chunk=0, workspace=None):
+               out=None, chunk=0, workspace=None, cone_events=None):
     """Attenuation (L, A, S, H, W) for fractions frac_4D (n_ch, S, H, W) on the
     device: incident term (mode 'own' | 'all' | 'none') times exp(-cone).
 
     coef_x (A, n_ch), coef_f (A, L, n_ch): per-angle mu coefficients (numpy or
-    device tensors).  mask_uv: (u, v, mask_shape) from mask_factors."""
+    device tensors).  mask_uv: (u, v, mask_shape) from mask_factors.
+    cone_events: optional list; when given, the two pipeline stages are issued
+    per angle chunk and (start, end, volumes) CUDA events of every cone launch
+    are appended to it."""
     _lib.require_cuda("atten_maps", frac_4D)
     dev = frac_4D.device
     frac = frac_4D.contiguous()
@@ -75,14 +78,41 @@ def atten_maps(frac_4D, angle_list, coef_x, coef_f, mask_uv=None, incident="own"
     else:
         u = v = None
         Mz = Mx = My = 1
+    chunk = pick_chunk(S, H, W, A, L, chunk)
     ws_bytes = _lib.query("flc_atten_workspace_bytes", n_ch, S, H, W, A, L, chunk)
     ws = workspace if workspace is not None and workspace.numel() >= ws_bytes else _lib.workspace(ws_bytes, dev)
+    mode = INCIDENT_MODES[incident]
     with torch.cuda.device(dev):
-        _lib.call("flc_atten_maps", _lib.ptr(frac), _lib.ptr(theta), _lib.ptr(cx), _lib.ptr(cf),
-                  _lib.ptr(u), _lib.ptr(v), _lib.ptr(out), n_ch, S, H, W, A, L, Mz, Mx, My,
-                  INCIDENT_MODES[incident], 0 if xrf else 1, chunk, _lib.ptr(ws), ws_bytes,
-                  _lib.stream())
+        st = _lib.stream()
+        if cone_events is None:
+            _lib.call("flc_atten_maps", _lib.ptr(frac), _lib.ptr(theta), _lib.ptr(cx),
+                      _lib.ptr(cf), _lib.ptr(u), _lib.ptr(v), _lib.ptr(out), n_ch, S, H, W, A, L,
+                      Mz, Mx, My, mode, 0 if xrf else 1, chunk, _lib.ptr(ws), ws_bytes, st)
+            return out
+        # same two stages per angle chunk, with CUDA events around each cone launch
+        for a0 in range(0, A, chunk):
+            n_a = min(chunk, A - a0)
+            _lib.call("flc_atten_stage", _lib.ptr(frac), _lib.ptr(theta), _lib.ptr(cx),
+                      _lib.ptr(cf), _lib.ptr(out), _lib.ptr(ws), n_ch, S, H, W, A, L, a0, n_a,
+                      mode, 1 if xrf else 0, st)
+            if not xrf:
+                continue
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            _lib.call("flc_cone_atten_apply", _lib.ptr(ws), _lib.ptr(u), _lib.ptr(v),
+                      _lib.ptr(out), n_a, L, S, H, W, A, a0, Mz, Mx, My, st)
+            e1.record()
+            cone_events.append((e0, e1, n_a * L))
     return out
+
+
+def pick_chunk(S, H, W, A, L, chunk=0):
+    """Angles per pass of the attenuation pipeline (the native default when 0):
+    about 64 MB of staged fluorescence mu, so a chunk stays L2-resident."""
+    if chunk <= 0:
+        chunk = max(1, (64 << 20) // (L * S * H * W * 4))
+    chunk = min(chunk, A)
+    return max(1, min(chunk, 65535 // L))
 
 
 def _save(fsave, kind, param, maps):

@@ -102,24 +102,34 @@ constexpr int kMaxCh = 8;
 constexpr int kMaxL = 8;
 constexpr int kStageRows = 32;
 
-struct AngleCoef {
-    float cos_t, sin_t;
+struct StageCoef {
     float cx[kMaxCh];
     float cf[kMaxL][kMaxCh];
 };
 
-__global__ void atten_stage_kernel(const float* __restrict__ frac, const AngleCoef* __restrict__ coefs,
-                                   float* __restrict__ out, float* __restrict__ mu_ref, int n_ch,
-                                   int S, int H, int W, int L, int64_t out_a_stride,
-                                   int64_t out_l_stride, int a_base, int incident_mode,
-                                   int write_mu) {
+__global__ void atten_stage_kernel(const float* __restrict__ frac, const float* __restrict__ theta,
+                                   const float* __restrict__ coef_x,
+                                   const float* __restrict__ coef_f, float* __restrict__ out,
+                                   float* __restrict__ mu_ref, int n_ch, int S, int H, int W,
+                                   int L, int64_t out_a_stride, int64_t out_l_stride, int a_base,
+                                   int incident_mode, int write_mu) {
     extern __shared__ float stage[];  // [L][kStageRows][W]
+    __shared__ StageCoef cf;
     const int s = blockIdx.x;
     const int al = blockIdx.y;
     const int a = a_base + al;
     const int w = threadIdx.x;
-    const AngleCoef& cf = coefs[a];
-    const RotGeom g = rot_geom(cf.cos_t, cf.sin_t, H, W);
+    for (int t = threadIdx.x; t < kMaxCh * (kMaxL + 1); t += blockDim.x) {
+        int j = t % kMaxCh, i = t / kMaxCh;
+        if (i == kMaxL)
+            cf.cx[j] = j < n_ch ? coef_x[(int64_t)a * n_ch + j] : 0.f;
+        else
+            cf.cf[i][j] = (i < L && j < n_ch) ? coef_f[((int64_t)a * L + i) * n_ch + j] : 0.f;
+    }
+    __syncthreads();
+    // the reference rounds math.cos / math.sin of the angle to an FP32 matrix
+    const double th = (double)theta[a];
+    const RotGeom g = rot_geom((float)cos(th), (float)sin(th), H, W);
     float prod[kMaxL];
 #pragma unroll
     for (int i = 0; i < kMaxL; ++i) prod[i] = 1.f;
@@ -475,23 +485,6 @@ int rotate_launch(const float* x, float* out, int64_t N, int64_t H, int64_t W, f
 
 namespace {
 
-__global__ void fill_coef_kernel(const float* __restrict__ theta, const float* __restrict__ coef_x,
-                                 const float* __restrict__ coef_f, AngleCoef* __restrict__ out,
-                                 int A, int n_ch, int L) {
-    int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a >= A) return;
-    AngleCoef k;
-    // the reference rounds math.cos/sin of the angle to an FP32 matrix
-    double th = (double)theta[a];
-    k.cos_t = (float)cos(th);
-    k.sin_t = (float)sin(th);
-    for (int j = 0; j < kMaxCh; ++j) k.cx[j] = j < n_ch ? coef_x[a * n_ch + j] : 0.f;
-    for (int i = 0; i < kMaxL; ++i)
-        for (int j = 0; j < kMaxCh; ++j)
-            k.cf[i][j] = (i < L && j < n_ch) ? coef_f[((int64_t)a * L + i) * n_ch + j] : 0.f;
-    out[a] = k;
-}
-
 size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
 
 int64_t pick_chunk(int64_t S, int64_t H, int64_t W, int64_t A, int64_t L, int64_t chunk) {
@@ -507,10 +500,24 @@ int64_t pick_chunk(int64_t S, int64_t H, int64_t W, int64_t A, int64_t L, int64_
 
 size_t atten_ws_bytes(int64_t S, int64_t H, int64_t W, int64_t A, int64_t L, int64_t chunk) {
     chunk = pick_chunk(S, H, W, A, L, chunk);
-    return align256(sizeof(AngleCoef) * A) + align256(sizeof(float) * chunk * L * S * H * W);
+    return align256(sizeof(float) * chunk * L * S * H * W);
 }
 
 }  // namespace
+
+int atten_stage_launch(const float* frac, const float* theta, const float* coef_x,
+                       const float* coef_f, float* out, float* mu_ref, int n_ch, int S, int H,
+                       int W, int L, int64_t out_a_stride, int64_t out_l_stride, int a_base,
+                       int n_a, int incident_mode, int write_mu, cudaStream_t st) {
+    size_t smem = sizeof(float) * (size_t)L * kStageRows * W;
+    int threads = (W + 31) & ~31;
+    FLC_TRY_CUDA(cudaFuncSetAttribute((const void*)atten_stage_kernel,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    atten_stage_kernel<<<dim3((unsigned)S, (unsigned)n_a), threads, smem, st>>>(
+        frac, theta, coef_x, coef_f, out, mu_ref, n_ch, S, H, W, L, out_a_stride, out_l_stride,
+        a_base, incident_mode, write_mu);
+    return check_launch("atten_stage_kernel");
+}
 
 int atten_maps_launch(const float* frac, const float* theta, const float* coef_x,
                       const float* coef_f, const float* u, const float* v, float* out,
@@ -518,22 +525,13 @@ int atten_maps_launch(const float* frac, const float* theta, const float* coef_x
                       int64_t Mz, int64_t Mx, int64_t My, int incident_mode, int xrf_mode,
                       int64_t chunk, void* workspace, cudaStream_t st) {
     chunk = pick_chunk(S, H, W, A, L, chunk);
-    AngleCoef* coefs = (AngleCoef*)workspace;
-    float* mu_ref = (float*)((char*)workspace + align256(sizeof(AngleCoef) * A));
-    fill_coef_kernel<<<(unsigned)ceil_div(A, 128), 128, 0, st>>>(theta, coef_x, coef_f, coefs,
-                                                                  (int)A, (int)n_ch, (int)L);
-    FLC_TRY(check_launch("fill_coef_kernel"));
+    float* mu_ref = (float*)workspace;
     const int64_t out_a = S * H * W, out_l = A * S * H * W;
-    const size_t stage_smem = sizeof(float) * (size_t)L * kStageRows * W;
-    FLC_TRY_CUDA(cudaFuncSetAttribute((const void*)atten_stage_kernel,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_smem));
-    const int threads = (int)((W + 31) & ~31);
     for (int64_t a0 = 0; a0 < A; a0 += chunk) {
         int n_a = (int)(A - a0 < chunk ? A - a0 : chunk);
-        atten_stage_kernel<<<dim3((unsigned)S, (unsigned)n_a), threads, stage_smem, st>>>(
-            frac, coefs, out, mu_ref, (int)n_ch, (int)S, (int)H, (int)W, (int)L, out_a, out_l,
-            (int)a0, incident_mode, xrf_mode == 0);
-        FLC_TRY(check_launch("atten_stage_kernel"));
+        FLC_TRY(atten_stage_launch(frac, theta, coef_x, coef_f, out, mu_ref, (int)n_ch, (int)S,
+                                   (int)H, (int)W, (int)L, out_a, out_l, (int)a0, n_a,
+                                   incident_mode, xrf_mode == 0, st));
         if (xrf_mode != 0) continue;
         // reference frame of the cone: (Z=S, X=W, Y=H)
         FLC_TRY(cone_sep_launch(mu_ref, u, v, out, (int64_t)n_a * L, S, W, H, Mz, Mx, My, 2,
@@ -675,4 +673,38 @@ extern "C" int flc_atten_maps(const float* frac, const float* theta, const float
     }
     return atten_maps_launch(frac, theta, coef_x, coef_f, u, v, out, n_ch, S, H, W, A, L, Mz, Mx,
                              My, incident_mode, xrf_mode, chunk, workspace, as_stream(stream));
+}
+
+extern "C" int flc_atten_stage(const float* frac, const float* theta, const float* coef_x,
+                               const float* coef_f, float* out, float* mu_ref, int64_t n_ch,
+                               int64_t S, int64_t H, int64_t W, int64_t A, int64_t L,
+                               int64_t a0, int64_t n_a, int incident_mode, int write_mu,
+                               void* stream) {
+    clear_error();
+    FLC_REQUIRE(frac && theta && coef_x && coef_f && out && (mu_ref || !write_mu),
+                "flc_atten_stage: null pointer argument");
+    FLC_REQUIRE(n_ch >= 1 && n_ch <= kMaxCh && L >= 1 && L <= kMaxL,
+                "flc_atten_stage: 1 <= n_ch <= %d, 1 <= L <= %d", kMaxCh, kMaxL);
+    FLC_REQUIRE(H == W && H >= 2 && W <= 1024 && S >= 1 && S <= 65535,
+                "flc_atten_stage: needs square slices, 2 <= H == W <= 1024");
+    FLC_REQUIRE(a0 >= 0 && n_a >= 1 && a0 + n_a <= A && n_a <= 65535,
+                "flc_atten_stage: angle range [a0, a0+n_a) outside [0, A)");
+    FLC_REQUIRE(incident_mode >= 0 && incident_mode <= 2, "flc_atten_stage: bad incident_mode");
+    return atten_stage_launch(frac, theta, coef_x, coef_f, out, mu_ref, (int)n_ch, (int)S, (int)H,
+                              (int)W, (int)L, S * H * W, A * S * H * W, (int)a0, (int)n_a,
+                              incident_mode, write_mu, as_stream(stream));
+}
+
+extern "C" int flc_cone_atten_apply(const float* mu_ref, const float* u, const float* v,
+                                    float* atten, int64_t n_a, int64_t L, int64_t S, int64_t H,
+                                    int64_t W, int64_t A, int64_t a0, int64_t Mz, int64_t Mx,
+                                    int64_t My, void* stream) {
+    clear_error();
+    FLC_REQUIRE(mu_ref && u && v && atten, "flc_cone_atten_apply: null pointer argument");
+    FLC_REQUIRE(H == W && H >= 2 && S >= 1 && L >= 1 && n_a >= 1 && a0 >= 0 && a0 + n_a <= A,
+                "flc_cone_atten_apply: bad sizes");
+    FLC_REQUIRE(n_a * L <= 65535 && Mz >= 1 && Mx >= 1 && My >= 1,
+                "flc_cone_atten_apply: bad sizes");
+    return cone_sep_launch(mu_ref, u, v, atten, n_a * L, S, W, H, Mz, Mx, My, 2, (int)L, (int)a0,
+                           S * H * W, A * S * H * W, as_stream(stream));
 }

@@ -15,10 +15,17 @@ void clear_error();
 // Maps a CUDA error to FLC_ERR_CUDA with a message naming `what`.
 int cuda_fail(cudaError_t e, const char* what);
 
-// Checks the launch just issued (configuration errors are synchronous).
+// Kernel-launch counter behind flc_launch_count().
+void count_launches(int64_t n);
+uint64_t launches();
+
+// Checks the launch just issued (configuration errors are synchronous) and
+// counts it.
 inline int check_launch(const char* what) {
     cudaError_t e = cudaGetLastError();
-    return e == cudaSuccess ? FLC_OK : cuda_fail(e, what);
+    if (e != cudaSuccess) return cuda_fail(e, what);
+    count_launches(1);
+    return FLC_OK;
 }
 
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }

@@ -363,6 +363,7 @@ int launch_cluster(const void* fn, dim3 grid, int G, size_t smem, cudaStream_t s
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     FLC_TRY_CUDA(cudaLaunchKernelExC(&cfg, fn, args));
+    count_launches(1);
     return FLC_OK;
 }
 

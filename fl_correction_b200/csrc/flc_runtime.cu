@@ -11,6 +11,7 @@
 #include <stdarg.h>
 #include <stdio.h>
 
+#include <atomic>
 #include <mutex>
 
 #include "flc_common.cuh"
@@ -18,6 +19,7 @@
 namespace flc {
 
 namespace {
+std::atomic<uint64_t> g_launches{0};
 thread_local char g_err[1024] = {0};
 int g_sms[64] = {0};
 int g_smem[64] = {0};
@@ -32,6 +34,9 @@ void set_error(const char* fmt, ...) {
 }
 
 void clear_error() { g_err[0] = 0; }
+
+void count_launches(int64_t n) { g_launches.fetch_add((uint64_t)n); }
+uint64_t launches() { return g_launches.load(); }
 
 int cuda_fail(cudaError_t e, const char* what) {
     set_error("%s: %s (%s)", what, cudaGetErrorString(e), cudaGetErrorName(e));
@@ -165,6 +170,8 @@ extern "C" const char* flc_last_error(void) { return g_err; }
 
 extern "C" const char* flc_version(void) { return "flc-b200 0.1.0 (sm_100a)"; }
 
+extern "C" uint64_t flc_launch_count(void) { return launches(); }
+
 extern "C" size_t flc_mlem_workspace_bytes(int64_t A, int64_t B, int64_t R, int64_t H, int64_t W) {
     if (A < 1 || B < 1 || R < 1 || H < 1 || W < 1) return 0;
     return mlem_layout(A, B, R, H, W, nullptr, nullptr);
@@ -215,9 +222,9 @@ extern "C" int flc_mlem(float* C, const float* atten, const float* em, const flo
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int status = FLC_OK;
-    cudaEvent_t ev = nullptr;
     FLC_TRY_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
     do {
+        const uint64_t before = launches();
         if (cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
             status = cuda_fail(cudaGetLastError(), "cudaStreamBeginCapture");
             break;
@@ -226,6 +233,9 @@ extern "C" int flc_mlem(float* C, const float* atten, const float* em, const flo
         int s2 = s1 == FLC_OK ? mlem_step(atten, em, theta, I, m, m.alt, C, A, B, R, H, W, fb, fd, cap)
                               : s1;
         cudaError_t e = cudaStreamEndCapture(cap, &graph);
+        // captured launches run only when the graph is replayed
+        const int64_t body = (int64_t)(launches() - before);
+        count_launches(-body);
         if (s2 != FLC_OK) { status = s2; break; }
         if (e != cudaSuccess) { status = cuda_fail(e, "cudaStreamEndCapture"); break; }
         e = cudaGraphInstantiate(&exec, graph, 0);
@@ -233,6 +243,7 @@ extern "C" int flc_mlem(float* C, const float* atten, const float* em, const flo
         for (int64_t it = 0; it + 1 < n_iter; it += 2) {
             e = cudaGraphLaunch(exec, st);
             if (e != cudaSuccess) { status = cuda_fail(e, "cudaGraphLaunch"); break; }
+            count_launches(body);
         }
         if (status != FLC_OK) break;
         if (n_iter & 1) {
@@ -242,15 +253,8 @@ extern "C" int flc_mlem(float* C, const float* atten, const float* em, const flo
             if (e != cudaSuccess) { status = cuda_fail(e, "cudaMemcpyAsync"); break; }
         }
     } while (0);
-    // Graph resources may only be released once the replays have run.
-    if (exec) {
-        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess) {
-            cudaEventRecord(ev, st);
-            cudaEventSynchronize(ev);
-            cudaEventDestroy(ev);
-        }
-        cudaGraphExecDestroy(exec);
-    }
+    // An executable graph destroyed while in flight is released on completion.
+    if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
     cudaStreamDestroy(cap);
     return status;

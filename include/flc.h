@@ -50,6 +50,9 @@ FLC_API const char* flc_status_string(int status);
 FLC_API const char* flc_last_error(void);
 /* Library version string. */
 FLC_API const char* flc_version(void);
+/* Number of kernels this library has launched in this process (graph
+ * replays count every kernel node they run).  For instrumentation. */
+FLC_API uint64_t flc_launch_count(void);
 
 /* ---------------------------------------------------------------------
  * Cone-mask (fluorescence) path sum, reference layout.
@@ -68,7 +71,7 @@ FLC_API int flc_cone_atten(const float* mu, const float* mask, float* out,
 
 /* Separable cone path sum with a caller-factored mask:
  *   mask[dz,dx,dy] == u[dx*Mz + dz] * v[dx*My + dy].
- * mode: 0 writes the sum, 1 writes exp(-sum), 2 multiplies exp(-sum) into out.
+ * mode: 0 writes the sum, 1 writes exp(-sum).
  * No counterpart entry point in the reference (it is the fast path of
  * cal_atten_cuda, atten_cuda.cpp:12-28). */
 FLC_API int flc_cone_atten_separable(const float* mu, const float* u, const float* v, float* out,
@@ -141,6 +144,23 @@ FLC_API int flc_atten_maps(const float* frac, const float* theta, const float* c
                    int64_t n_ch, int64_t S, int64_t H, int64_t W, int64_t A, int64_t L,
                    int64_t Mz, int64_t Mx, int64_t My, int incident_mode, int xrf_mode,
                    int64_t chunk, void* workspace, size_t workspace_bytes, void* stream);
+
+/* The two stages of flc_atten_maps, for callers that schedule angle chunks
+ * themselves.  flc_atten_stage writes the incident term of angles
+ * [a0, a0+n_a) into out (L, A, S, H, W) and, if write_mu, the fluorescence mu
+ * of those angles into mu_ref (n_a, L, S, W, H) -- the detector-depth-major
+ * layout of the reference's rot90 frame (FL/torch_functions.py:142-143).
+ * flc_cone_atten_apply multiplies exp(-cone(mu_ref)) into the same angles of
+ * out.  No counterpart entry points in the reference (FL/core.py:19-101 runs
+ * these steps per angle in Python). */
+FLC_API int flc_atten_stage(const float* frac, const float* theta, const float* coef_x,
+                            const float* coef_f, float* out, float* mu_ref, int64_t n_ch,
+                            int64_t S, int64_t H, int64_t W, int64_t A, int64_t L, int64_t a0,
+                            int64_t n_a, int incident_mode, int write_mu, void* stream);
+FLC_API int flc_cone_atten_apply(const float* mu_ref, const float* u, const float* v,
+                                 float* atten, int64_t n_a, int64_t L, int64_t S, int64_t H,
+                                 int64_t W, int64_t A, int64_t a0, int64_t Mz, int64_t Mx,
+                                 int64_t My, void* stream);
 
 /* Rotation with torch grid_sample semantics (bilinear, zero padding,
  * align_corners=False, same-size output): out (N, H, W) from x (N, H, W).

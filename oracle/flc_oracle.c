@@ -212,6 +212,37 @@ void orc_cone_beam(const double* mu, const double* mask, double* out,
                 }
 }
 
+/* orc_cone_beam restricted to output slices [z0, z1) of every volume
+ * (out has the full (K,Z,H,W) shape; other slices are left untouched).
+ * Used to time a bounded sample of the full computation. */
+void orc_cone_beam_slab(const double* mu, const double* mask, double* out,
+                        i64 K, i64 Z, i64 H, i64 W, i64 Mz, i64 Mx, i64 My, i64 z0, i64 z1) {
+    i64 hz = Mz / 2, hy = My / 2;
+#pragma omp parallel for collapse(3) schedule(dynamic, 1)
+    for (i64 k = 0; k < K; ++k)
+        for (i64 z = z0; z < z1; ++z)
+            for (i64 h = 0; h < H; ++h)
+                for (i64 w = 0; w < W; ++w) {
+                    double acc = 0.0;
+                    for (i64 dz = 0; dz < Mz; ++dz) {
+                        i64 zz = z + dz - hz;
+                        if (zz < 0 || zz >= Z) continue;
+                        for (i64 dx = 0; dx < Mx; ++dx) {
+                            i64 ww = w + dx;
+                            if (ww >= W) break;
+                            const double* mrow = mask + (dz * Mx + dx) * My;
+                            for (i64 dy = 0; dy < My; ++dy) {
+                                i64 hh = h - (dy - hy);
+                                if (hh < 0 || hh >= H) continue;
+                                double m = mrow[dy];
+                                if (m != 0.0) acc += mu[((k * Z + zz) * H + hh) * W + ww] * m;
+                            }
+                        }
+                    }
+                    out[((k * Z + z) * H + h) * W + w] = acc;
+                }
+}
+
 /* Adjoint of orc_cone_beam: g_mu[k,z',h',w'] = sum over outputs that read it. */
 void orc_cone_beam_adjoint(const double* g, const double* mask, double* gmu,
                            i64 K, i64 Z, i64 H, i64 W, i64 Mz, i64 Mx, i64 My) {

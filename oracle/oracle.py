@@ -213,3 +213,15 @@ def mlem(C_init, atten, em, theta, I, n_iter, beta=1e-3, delta=0.01):
                    _i64(n_iter), ctypes.c_double(beta), ctypes.c_double(delta),
                    _i64(A), _i64(B), _i64(R), _i64(H), _i64(W))
     return C[:, 0] if single else C
+
+
+def cone_beam_slab(mu, mask, z0, z1):
+    """cone_beam for output slices [z0, z1) only (others are zero)."""
+    mu = _d(mu)
+    mask = _d(mask)
+    K, Z, H, W = mu.shape
+    Mz, Mx, My = mask.shape
+    out = np.zeros_like(mu)
+    lib().orc_cone_beam_slab(_pd(mu), _pd(mask), _pd(out), _i64(K), _i64(Z), _i64(H), _i64(W),
+                             _i64(Mz), _i64(Mx), _i64(My), _i64(z0), _i64(z1))
+    return out

@@ -1,0 +1,88 @@
+"""The C ABI: every entry point declared in include/flc.h is exported by
+libflc.so, and argument validation answers with a status code (these calls
+never reach the GPU)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from fl_correction_b200 import _lib
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "flc.h")
+
+
+def declared():
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"FLC_API\s+[\w\s\*]+?\b(flc_\w+)\s*\(", text)))
+
+
+def test_header_declares_entry_points():
+    names = declared()
+    assert len(names) >= 15
+    for n in ("flc_cone_atten", "flc_fwd_emission", "flc_bwd_emission", "flc_mlem",
+              "flc_atten_maps", "flc_huber_grad"):
+        assert n in names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(_lib.LIB_PATH)
+    missing = [n for n in declared() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_python_binding_covers_every_symbol():
+    assert set(declared()) <= set(_lib.SIGNATURES)
+
+
+def test_status_strings_and_version():
+    lib = _lib.load()
+    assert lib.flc_status_string(0) == b"FLC_OK"
+    assert lib.flc_status_string(4) == b"FLC_ERR_WORKSPACE"
+    assert lib.flc_status_string(99) == b"FLC_ERR_UNKNOWN"
+    assert b"sm_100a" in lib.flc_version()
+
+
+@pytest.mark.parametrize("name,args", [
+    ("flc_fwd_emission", (None, None, None, None, None, 1, 1, 1, 4, 4, None)),
+    ("flc_bwd_emission", (None, None, None, None, None, 1, 1, 1, 4, 4, None)),
+    ("flc_cone_atten", (None, None, None, 1, 1, 1, 1, 1, 1, 1, 0, None)),
+    ("flc_huber_grad", (None, None, 1, 4, 4, 0.01, None)),
+    ("flc_rotate", (None, None, 1, 4, 4, 1.0, 0.0, None)),
+    ("flc_incident_scan", (None, None, 1, 4, 4, None)),
+])
+def test_null_pointers_are_rejected(name, args):
+    lib = _lib.load()
+    assert getattr(lib, name)(*args) == 1          # FLC_ERR_INVALID_ARG
+    assert b"null pointer" in lib.flc_last_error()
+
+
+def test_bad_sizes_are_rejected():
+    lib = _lib.load()
+    p = ctypes.c_void_p(16)   # never dereferenced: validation fails first
+    assert lib.flc_fwd_emission(p, p, p, p, p, 4, 2, 1, 1, 8, None) == 1      # H < 2
+    assert lib.flc_fwd_emission(p, p, p, p, p, 4, 2, 9, 8, 8, None) == 1      # R > 8
+    assert lib.flc_mlem(p, p, p, p, p, 5, 1e-3, 0.01, 4, 2, 1, 8, 8, None, 0, 0, None) == 1
+    ws = ctypes.c_void_p(256 * 7)
+    assert lib.flc_mlem(p, p, p, p, p, 5, 1e-3, 0.01, 4, 2, 1, 8, 8, ws, 16, 0, None) == 4
+    assert lib.flc_mlem(p, p, p, p, p, 5, 1e-3, 0.01, 4, 2, 1, 8, 8, ctypes.c_void_p(300),
+                        1 << 30, 0, None) == 3
+    assert lib.flc_atten_maps(p, p, p, p, p, p, p, 3, 4, 8, 6, 5, 2, 3, 8, 3, 0, 0, 0, p,
+                              1 << 30, None) == 1                         # H != W
+
+
+def test_workspace_queries():
+    lib = _lib.load()
+    assert lib.flc_mlem_workspace_bytes(120, 128, 1, 128, 128) >= 3 * 4 * 128 ** 3
+    assert lib.flc_mlem_workspace_bytes(0, 1, 1, 1, 1) == 0
+    assert lib.flc_atten_workspace_bytes(4, 128, 128, 128, 120, 3, 2) >= 2 * 3 * 4 * 128 ** 3
+
+
+def test_cpu_tensors_fail_loudly():
+    import torch
+    from fl_correction_b200.cuda_lib import atten_cuda
+    x = torch.zeros(2, 3, 4, 4)
+    with pytest.raises(RuntimeError, match="CUDA"):
+        atten_cuda.cal_atten_cuda(x, torch.zeros(3, 3, 3))
+    with pytest.raises(RuntimeError, match="CUDA"):
+        atten_cuda.forward_emission_batch(x, x, torch.ones(2, 2), torch.zeros(2))

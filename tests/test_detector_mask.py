@@ -1,0 +1,38 @@
+"""generate_detector_mask against the reference's masks, and the rank-one
+factorisation the separable cone kernel relies on."""
+import numpy as np
+import pytest
+
+from fl_correction_b200.detector_mask import factor_mask, generate_detector_mask
+from tests.helpers import golden_cpu, golden_meta
+
+
+@pytest.mark.parametrize("idx", range(6))
+def test_mask_matches_reference(idx):
+    a, b, L = golden_meta()["mask_cases"][idx]
+    ref = golden_cpu()[f"mask{idx}"]
+    m = generate_detector_mask(a, b, L)
+    assert m.shape == ref.shape
+    # float64 masks; the kernels consume them as float32 (7 significant digits)
+    assert np.abs(m - ref).max() <= 1e-6 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("L", [16, 64, 128, 256])
+def test_config_mask_shapes_and_planes(L):
+    m = generate_detector_mask(13.309, 13.309, L)
+    expect = {16: (3, 16, 3), 64: (15, 64, 15), 128: (29, 128, 29), 256: (59, 256, 59)}[L]
+    assert m.shape == expect
+    assert np.all(m[:, 0, :] == 0)           # the voxel itself is excluded
+    assert np.all(m >= 0)
+
+
+def test_factorisation_is_exact():
+    m = generate_detector_mask(13.309, 13.309, 64)
+    u, v = factor_mask(m)
+    rec = np.einsum("dz,dy->zdy", u.astype(np.float64), v.astype(np.float64))
+    assert np.abs(rec - m).max() <= 1e-6 * m.max()
+
+
+def test_factorisation_rejects_general_mask():
+    rng = np.random.default_rng(0)
+    assert factor_mask(rng.random((5, 7, 3))) is None

@@ -1,0 +1,90 @@
+"""Cone path sum parity: cal_atten_cuda (atten_cuda_kernel.cu:10-86) through
+the C ABI against the FP64 oracle, separable and general paths."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+from fl_correction_b200 import _lib
+from fl_correction_b200.cuda_lib import atten_cuda as AC
+from fl_correction_b200.detector_mask import factor_mask, generate_detector_mask
+from tests.helpers import TOL_MAP, T, golden_cpu, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("K,Z,X,Y,L", [(2, 9, 20, 20, 20), (1, 16, 32, 32, 32), (3, 5, 16, 12, 16),
+                                       (1, 40, 24, 30, 24), (1, 64, 64, 64, 64)])
+def test_separable_matches_oracle(K, Z, X, Y, L):
+    rng = np.random.default_rng(K * 100 + Z)
+    mask = generate_detector_mask(13.309, 13.309, L).astype(np.float32)
+    mu = (rng.random((K, Z, X, Y)) * 0.05).astype(np.float32)
+    out = AC.cal_atten_cuda(T(mu), T(mask)).cpu().numpy()
+    assert rel_err(out, O.cone_ref(mu, mask)) < TOL_MAP
+
+
+def test_wide_mask_and_uneven_angles():
+    rng = np.random.default_rng(3)
+    mask = generate_detector_mask(15.0, 60.0, 12).astype(np.float32)   # (13, 12, 3)
+    mu = rng.random((2, 11, 14, 18)).astype(np.float32)
+    out = AC.cal_atten_cuda(T(mu), T(mask)).cpu().numpy()
+    assert rel_err(out, O.cone_ref(mu, mask)) < TOL_MAP
+
+
+def test_general_mask_matches_oracle():
+    rng = np.random.default_rng(4)
+    mask = rng.random((5, 7, 3)).astype(np.float32)
+    mask[mask < 0.3] = 0
+    mu = rng.random((2, 9, 20, 21)).astype(np.float32)
+    out = AC.cal_atten_cuda(T(mu), T(mask)).cpu().numpy()
+    assert rel_err(out, O.cone_ref(mu, mask)) < TOL_MAP
+
+
+def test_forced_general_equals_separable():
+    rng = np.random.default_rng(5)
+    mask = generate_detector_mask(13.309, 13.309, 16).astype(np.float32)
+    mu = rng.random((1, 12, 16, 16)).astype(np.float32)
+    sep = AC.cal_atten_cuda(T(mu), T(mask))
+    gen = torch.empty_like(sep)
+    m, x = T(mask), T(mu)
+    _lib.call("flc_cone_atten", _lib.ptr(x), _lib.ptr(m), _lib.ptr(gen), 1, 12, 16, 16, 3, 16, 3,
+              1, _lib.stream())
+    assert rel_err(gen.cpu().numpy(), sep.cpu().numpy()) < 1e-6
+
+
+def test_window_wider_than_a_block():
+    # the reference kernel launches one thread per column, so Y > 1024 fails there
+    rng = np.random.default_rng(6)
+    mask = generate_detector_mask(13.309, 13.309, 8).astype(np.float32)
+    mu = rng.random((1, 3, 8, 1100)).astype(np.float32)
+    out = AC.cal_atten_cuda(T(mu), T(mask)).cpu().numpy()
+    assert rel_err(out, O.cone_ref(mu, mask)) < TOL_MAP
+
+
+def test_golden_correlation():
+    g = golden_cpu()
+    out = AC.cal_atten_cuda(T(g["cone_mu"]), T(g["xrf_mask"])).cpu().numpy()
+    assert rel_err(out, g["cone_out"]) < TOL_MAP
+
+
+def test_separable_entry_point_modes():
+    rng = np.random.default_rng(7)
+    mask = generate_detector_mask(13.309, 13.309, 20)
+    u, v = factor_mask(mask)
+    mu = (rng.random((2, 7, 20, 20)) * 0.1).astype(np.float32)
+    ref = O.cone_ref(mu, mask.astype(np.float32))
+    x, U, V = T(mu), T(u), T(v)
+    for mode, expect in ((0, ref), (1, np.exp(-ref))):
+        out = torch.empty_like(x)
+        _lib.call("flc_cone_atten_separable", _lib.ptr(x), _lib.ptr(U), _lib.ptr(V), _lib.ptr(out),
+                  2, 7, 20, 20, mask.shape[0], mask.shape[1], mask.shape[2], mode, _lib.stream())
+        assert rel_err(out.cpu().numpy(), expect) < TOL_MAP
+
+
+def test_benchmark_size_slab():
+    # 128-wide slices with the 128-deep mask, 12 of the 128 slices
+    rng = np.random.default_rng(8)
+    mask = generate_detector_mask(13.309, 13.309, 128).astype(np.float32)
+    mu = (rng.random((1, 12, 128, 128)) * 0.01).astype(np.float32)
+    out = AC.cal_atten_cuda(T(mu), T(mask)).cpu().numpy()
+    assert rel_err(out, O.cone_ref(mu, mask)) < TOL_MAP

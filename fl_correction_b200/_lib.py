@@ -25,6 +25,7 @@ SIGNATURES = {
     "flc_last_error": (ctypes.c_char_p, []),
     "flc_version": (ctypes.c_char_p, []),
     "flc_launch_count": (ctypes.c_uint64, []),
+    "flc_device_status": (_int, [_int]),
     "flc_cone_atten": (_int, [_vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _i64, _i64, _int, _vp]),
     "flc_cone_atten_separable": (_int, [_vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _i64,
                                         _i64, _int, _vp]),

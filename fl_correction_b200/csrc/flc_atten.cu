@@ -424,10 +424,25 @@ constexpr int kSepMaxThreads = 512;
 
 }  // namespace
 
+// TMA-pipelined separable kernel (flc_cone.cu); FLC_ERR_UNSUPPORTED when the
+// shape does not fit it.
+int cone_tma_launch(const float* mu, const float* U, const float* Vw, float* out, int64_t Vn,
+                    int64_t Z, int64_t X, int64_t Y, int64_t Mz, int64_t Mx, int64_t My, int mode,
+                    int L, int a_base, int64_t out_a_stride, int64_t out_l_stride, cudaStream_t st);
+
+// Separable cone path sum.  `mode` (0/1/2, see cone_sep_kernel) may carry
+// kConePlain to select the plain kernel below even where the pipelined one fits.
 int cone_sep_launch(const float* mu, const float* U, const float* Vw, float* out, int64_t Vn,
                     int64_t Z, int64_t X, int64_t Y, int64_t Mz, int64_t Mx, int64_t My, int mode,
                     int L, int a_base, int64_t out_a_stride, int64_t out_l_stride,
                     cudaStream_t st) {
+    if (!(mode & kConePlain)) {
+        int r = cone_tma_launch(mu, U, Vw, out, Vn, Z, X, Y, Mz, Mx, My, mode, L, a_base,
+                                out_a_stride, out_l_stride, st);
+        if (r != FLC_ERR_UNSUPPORTED) return r;
+        clear_error();
+    }
+    mode &= ~kConePlain;
     SepDims d = sep_dims(Z, X, Y, Mz, Mx, My);
     size_t smem = sep_smem(d);
     int threads = sep_threads((int)Z);
@@ -571,7 +586,9 @@ extern "C" int flc_cone_atten_separable(const float* mu, const float* u, const f
     FLC_REQUIRE(mu && u && v && out, "flc_cone_atten_separable: null pointer argument");
     FLC_REQUIRE(K >= 1 && Z >= 1 && X >= 1 && Y >= 1 && Mz >= 1 && Mx >= 1 && My >= 1,
                 "flc_cone_atten_separable: sizes must be positive");
-    FLC_REQUIRE(mode == 0 || mode == 1, "flc_cone_atten_separable: mode must be 0 or 1");
+    FLC_REQUIRE((mode & ~FLC_CONE_PLAIN_KERNEL) == 0 || (mode & ~FLC_CONE_PLAIN_KERNEL) == 1,
+                "flc_cone_atten_separable: mode must be 0 or 1 (optionally | FLC_CONE_PLAIN_KERNEL)");
+    if (mode & FLC_CONE_PLAIN_KERNEL) mode = (mode & ~FLC_CONE_PLAIN_KERNEL) | kConePlain;
     FLC_REQUIRE(K <= 65535, "flc_cone_atten_separable: K must be <= 65535");
     return cone_sep_launch(mu, u, v, out, K, Z, X, Y, Mz, Mx, My, mode, 1, 0, 0, 0,
                            as_stream(stream));
@@ -707,4 +724,9 @@ extern "C" int flc_cone_atten_apply(const float* mu_ref, const float* u, const f
                 "flc_cone_atten_apply: bad sizes");
     return cone_sep_launch(mu_ref, u, v, atten, n_a * L, S, W, H, Mz, Mx, My, 2, (int)L, (int)a0,
                            S * H * W, A * S * H * W, as_stream(stream));
+}
+
+extern "C" int flc_device_status(int reset) {
+    clear_error();
+    return cone_device_status(reset);
 }

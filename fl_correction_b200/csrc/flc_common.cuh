@@ -37,6 +37,13 @@ int max_smem_optin();
 
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
+// Bit of the cone `mode` argument that selects the plain separable kernel
+// over the TMA-pipelined one (for parity tests of both).
+constexpr int kConePlain = 0x100;
+
+// Device-side status left by bounded waits that gave up (flc_cone.cu).
+int cone_device_status(int reset);
+
 }  // namespace flc
 
 #define FLC_REQUIRE(cond, ...)                      \

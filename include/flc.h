@@ -50,6 +50,9 @@ FLC_API const char* flc_status_string(int status);
 FLC_API const char* flc_last_error(void);
 /* Library version string. */
 FLC_API const char* flc_version(void);
+/* Status left on the device by kernels whose bounded waits gave up
+ * (FLC_ERR_TIMEOUT) or FLC_OK; synchronizes the device.  reset != 0 clears it. */
+FLC_API int flc_device_status(int reset);
 /* Number of kernels this library has launched in this process (graph
  * replays count every kernel node they run).  For instrumentation. */
 FLC_API uint64_t flc_launch_count(void);
@@ -65,13 +68,15 @@ FLC_API uint64_t flc_launch_count(void);
  * gather over the non-zero taps.  `flags` is a bit set of FLC_CONE_*.
  * --------------------------------------------------------------------- */
 #define FLC_CONE_FORCE_GENERAL 1  /* skip the rank-one test, use the general kernel */
+#define FLC_CONE_PLAIN_KERNEL 16  /* separable: plain kernel, not the TMA pipeline */
 FLC_API int flc_cone_atten(const float* mu, const float* mask, float* out,
                    int64_t K, int64_t Z, int64_t X, int64_t Y,
                    int64_t Mz, int64_t Mx, int64_t My, int flags, void* stream);
 
 /* Separable cone path sum with a caller-factored mask:
  *   mask[dz,dx,dy] == u[dx*Mz + dz] * v[dx*My + dy].
- * mode: 0 writes the sum, 1 writes exp(-sum).
+ * mode: 0 writes the sum, 1 writes exp(-sum); OR FLC_CONE_PLAIN_KERNEL to use
+ * the plain separable kernel instead of the TMA-pipelined one.
  * No counterpart entry point in the reference (it is the fast path of
  * cal_atten_cuda, atten_cuda.cpp:12-28). */
 FLC_API int flc_cone_atten_separable(const float* mu, const float* u, const float* v, float* out,

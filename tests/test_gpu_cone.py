@@ -88,3 +88,23 @@ def test_benchmark_size_slab():
     mu = (rng.random((1, 12, 128, 128)) * 0.01).astype(np.float32)
     out = AC.cal_atten_cuda(T(mu), T(mask)).cpu().numpy()
     assert rel_err(out, O.cone_ref(mu, mask)) < TOL_MAP
+
+
+@pytest.mark.parametrize("K,Z,X,Y,L", [(2, 9, 20, 20, 20), (3, 64, 64, 64, 64), (1, 128, 128, 128, 128),
+                                       (2, 40, 36, 44, 36), (1, 160, 24, 32, 24)])
+def test_pipelined_and_plain_kernels_agree(K, Z, X, Y, L):
+    rng = np.random.default_rng(Z + X)
+    mask = generate_detector_mask(13.309, 13.309, L)
+    u, v = factor_mask(mask)
+    mu = (rng.random((K, Z, X, Y)) * 0.02).astype(np.float32)
+    x, U, V = T(mu), T(u), T(v)
+    outs = []
+    for flag in (0, 16):                       # 16 = FLC_CONE_PLAIN_KERNEL
+        out = torch.empty_like(x)
+        _lib.call("flc_cone_atten_separable", _lib.ptr(x), _lib.ptr(U), _lib.ptr(V), _lib.ptr(out),
+                  K, Z, X, Y, mask.shape[0], mask.shape[1], mask.shape[2], flag, _lib.stream())
+        outs.append(out.cpu().numpy())
+    assert _lib.query("flc_device_status", 1) == 0
+    assert rel_err(outs[0], outs[1]) < 1e-6
+    if Z * X * Y <= 64 ** 3:
+        assert rel_err(outs[0], O.cone_ref(mu, mask.astype(np.float32))) < TOL_MAP

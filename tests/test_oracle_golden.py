@@ -62,3 +62,26 @@ def test_rotated_pipeline(g):
             muf[i] += fr[j] * float(np.float32(cs[f"{c}-{e}"] * rho[c] * pix))
     res = O.cone_beam(muf, g["xrf_mask"].astype(np.float32))
     assert rel_err(np.exp(-res), g["pipe_atten_xrf"]) < 2e-6
+
+
+def test_oracle_matches_reference_cuda_kernels():
+    """Pin the oracle against outputs of the reference's own CUDA extension
+    (tests/golden/ref_gpu.npz, recorded by make_golden_refgpu.py)."""
+    import os
+    from tests.helpers import GOLDEN
+    p = os.path.join(GOLDEN, "ref_gpu.npz")
+    if not os.path.exists(p):
+        pytest.skip("reference GPU fixtures not recorded")
+    r = np.load(p)
+    assert rel_err(O.cone_ref(r["cone_mu"], r["cone_mask"]), r["cone_out"]) < 1e-6
+    assert rel_err(O.cone_ref(r["cone_mu"], r["cone_gmask"]), r["cone_gout"]) < 1e-6
+    a, C, em, th, ratio = r["p_atten"], r["p_C"], r["p_em"], r["p_theta"], r["p_ratio"]
+    assert rel_err(O.fwd_emission(a, C, em, th), r["p_fwd_batch"]) < 1e-6
+    assert rel_err(O.bwd_emission(a, ratio, em, th), r["p_bwd_batch"]) < 1e-6
+    assert rel_err(O.fwd_emission(a[:, 0], C[:, 0], em, th), r["p_fwd"]) < 1e-6
+    assert rel_err(O.bwd_emission(a[:, 0], ratio[:, 0], em, th), r["p_bwd"]) < 1e-6
+    C0 = np.ones_like(C)
+    assert rel_err(O.mlem(C0, a, em, th, r["m_I"], 20, 1e-3, 0.01), r["m_beta"]) < 1e-5
+    assert rel_err(O.mlem(C0, a, em, th, r["m_I"], 20, 0.0, 0.01), r["m_nobeta"]) < 1e-5
+    assert rel_err(O.mlem(C0[:, 0], a[:, 0], em, th, r["m_I"][:, 0], 20, 1e-3, 0.01),
+                   r["m_single"]) < 1e-5

@@ -26,6 +26,8 @@ SIGNATURES = {
     "flc_version": (ctypes.c_char_p, []),
     "flc_launch_count": (ctypes.c_uint64, []),
     "flc_device_status": (_int, [_int]),
+    "flc_tune_set": (_int, [ctypes.c_char_p, _i64]),
+    "flc_tune_get": (_i64, [ctypes.c_char_p]),
     "flc_cone_atten": (_int, [_vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _i64, _i64, _int, _vp]),
     "flc_cone_atten_separable": (_int, [_vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _i64,
                                         _i64, _int, _vp]),
@@ -42,6 +44,9 @@ SIGNATURES = {
                                _i64, _i64, _int, _int, _vp]),
     "flc_cone_atten_apply": (_int, [_vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _i64, _i64,
                                     _i64, _i64, _i64, _vp]),
+    "flc_xrf_workspace_bytes": (_sz, [_i64, _i64, _i64, _i64, _i64, _i64, _i64]),
+    "flc_xrf_project": (_int, [_vp] * 8 + [_i64] * 9 + [_int, _i64, _vp, _sz, _vp]),
+    "flc_xrf_project_adjoint": (_int, [_vp] * 11 + [_i64] * 9 + [_int, _i64, _vp, _sz, _vp]),
     "flc_rotate": (_int, [_vp, _vp, _i64, _i64, _i64, _f32, _f32, _vp]),
     "flc_incident_scan": (_int, [_vp, _vp, _i64, _i64, _i64, _vp]),
 }

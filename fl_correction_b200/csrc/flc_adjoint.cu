@@ -1,0 +1,348 @@
+// Self-absorption-corrected XRF projection with the attenuation recomputed
+// per angle chunk, and its hand-written adjoint (sm_100a).
+//
+// Forward model, per element l and angle a (the composition of
+// FL/core.py:19-101, FL/torch_functions.py:8-176 and the projector of
+// FL/cuda_lib/atten_cuda_kernel.cu:298-337):
+//   fr_j   = rotate(frac_j, theta_a)                      (grid_sample, zero pad)
+//   inc_l  = prod_{h'>h} (1 - cx_l fr_l)                  (own compound; or all)
+//   E_l    = exp(-cone(sum_j cf_lj fr_j))
+//   Pf_l,a = sum_h inc_l E_l em_l,a bilerp(C_l, theta_a)  with C_l = frac_l
+// The reference holds the attenuation fixed and differentiates the projector
+// in C only (FL/cuda_lib/autograd.py:5-77).  The adjoint here also carries
+// the gradient through the attenuation, i.e. through mu, back to C:
+//   G        = dL/dPf * em * bilerp(C)                     (d Pf / d atten)
+//   dres     = -G * atten,  dinc = G * E
+//   dmu_f    = cone^T(dres)          (the cone with flipped taps, depth reversed)
+//   dmu_x    = reverse-mode of the exclusive product scan
+//   dfr_j    = cx_j dmu_x_j + sum_l cf_lj dmu_f_l
+//   dC_l    += rotate^T(dfr_l) + P_a^T[atten](dL/dPf)     (direct term)
+// Nothing of size A x volume is stored: each chunk of angles is recomputed in
+// the backward pass (so 256^3 x 180-angle problems fit in HBM).
+
+#include "flc_common.cuh"
+#include "flc_geom.cuh"
+
+namespace flc {
+
+int atten_stage_launch(const float* frac, const float* theta, const float* coef_x,
+                       const float* coef_f, float* out, float* mu_ref, int n_ch, int S, int H,
+                       int W, int L, int64_t out_a_stride, int64_t out_l_stride, int a_base,
+                       int n_a, int incident_mode, int write_mu, cudaStream_t st, int out_a0);
+int cone_sep_launch(const float* mu, const float* U, const float* Vw, float* out, int64_t Vn,
+                    int64_t Z, int64_t X, int64_t Y, int64_t Mz, int64_t Mx, int64_t My, int mode,
+                    int L, int a_base, int64_t out_a_stride, int64_t out_l_stride, cudaStream_t st);
+int fwd_emission_launch(const float* atten, const float* C, const float* em, const float* theta,
+                        float* Pf, const float* I, int64_t A, int64_t B, int64_t R, int64_t H,
+                        int64_t W, cudaStream_t st);
+int bwd_emission_launch(const float* atten, const float* ratio, const float* em,
+                        const float* theta, float* out, int64_t A, int64_t B, int64_t R,
+                        int64_t H, int64_t W, float clamp_min, cudaStream_t st);
+
+namespace {
+
+constexpr int kMaxCh = 8;
+constexpr int kMaxL = 8;
+
+__global__ void mul_kernel(const float* __restrict__ a, const float* __restrict__ b,
+                           float* __restrict__ o, int64_t n) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) o[i] = a[i] * b[i];
+}
+
+__global__ void add_kernel(float* __restrict__ y, const float* __restrict__ x, int64_t n) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) y[i] += x[i];
+}
+
+// G = dL/dPf * em * bilerp(C) per sample; writes dinc = G*E (beam layout) and
+// dres = -G*atten in the depth-reversed reference layout that the cone
+// adjoint streams: dres_rev[al*L + l][s][W-1-w][H-1-h].
+// grid (ceil(W/32)*ceil(H/32), S, n_a*L), block (32, 8).
+__global__ void xrf_g_kernel(const float* __restrict__ C, const float* __restrict__ theta,
+                             const float* __restrict__ em, const float* __restrict__ gPf,
+                             const float* __restrict__ ATT, const float* __restrict__ E,
+                             float* __restrict__ dinc, float* __restrict__ dres_rev, int L, int A,
+                             int a0, int n_a, int S, int H, int W) {
+    __shared__ float T[32][33];
+    const int nbw = (W + 31) >> 5;
+    const int w0 = (blockIdx.x % nbw) * 32, h0 = (blockIdx.x / nbw) * 32;
+    const int s = blockIdx.y;
+    const int l = blockIdx.z % L;
+    const int al = blockIdx.z / L;
+    const int a = a0 + al;
+    const Geo g = make_geo(theta[a], H, W);
+    const float* Cl = C + ((int64_t)l * S + s) * H * W;
+    const float gem = em[(int64_t)l * A + a];
+    const float* gp = gPf + (((int64_t)l * A + a) * S + s) * W;
+    const int64_t base = (((int64_t)l * n_a + al) * S + s) * H * W;
+    for (int k = 0; k < 32; k += 8) {
+        const int hl = threadIdx.y + k, h = h0 + hl, w = w0 + threadIdx.x;
+        float dr = 0.f;
+        if (h < H && w < W) {
+            const Smp sm = sample(g, h, w);
+            const float Gv = gp[w] * gem * bilerp(Cl, W, sm);
+            const int64_t o = base + (int64_t)h * W + w;
+            dinc[o] = Gv * E[o];
+            dr = -Gv * ATT[o];
+        }
+        T[hl][threadIdx.x] = dr;
+    }
+    __syncthreads();
+    const int64_t vbase = (((int64_t)al * L + l) * S + s) * W;
+    for (int k = 0; k < 32; k += 8) {
+        const int wl = threadIdx.y + k, hl = threadIdx.x;
+        const int w = w0 + wl, h = h0 + hl;
+        if (h < H && w < W) dres_rev[(vbase + (W - 1 - w)) * H + (H - 1 - h)] = T[hl][wl];
+    }
+}
+
+// Reverse mode of the per-angle stage (rotation, mu assembly, incident scan),
+// one thread per detector column walking the beam from h = 0 upward:
+//   gbar[h] = dinc[h] + gbar[h-1] * f[h],  df[h] = gbar[h-1] * inc[h]
+// (the adjoint of inc[h-1] = f[h] * inc[h]), then
+//   dfr_j = cx_j * dmu_x_j + sum_l cf_lj * dmu_f_l
+// spread back onto the unrotated grid with the rotation's own taps (global
+// atomics into dC, channels j < L).  grid (S, n_a), block = W rounded to 32.
+__global__ void xrf_stage_adjoint_kernel(const float* __restrict__ frac,
+                                         const float* __restrict__ theta,
+                                         const float* __restrict__ coef_x,
+                                         const float* __restrict__ coef_f,
+                                         const float* __restrict__ INC,
+                                         const float* __restrict__ dinc,
+                                         const float* __restrict__ dmu_rev, float* __restrict__ dC,
+                                         int n_ch, int S, int H, int W, int L, int a0, int n_a,
+                                         int incident_mode) {
+    __shared__ float cx[kMaxCh];
+    __shared__ float cf[kMaxL][kMaxCh];
+    const int s = blockIdx.x, al = blockIdx.y, a = a0 + al, w = threadIdx.x;
+    for (int t = threadIdx.x; t < kMaxCh * (kMaxL + 1); t += blockDim.x) {
+        int j = t % kMaxCh, i = t / kMaxCh;
+        if (i == kMaxL)
+            cx[j] = j < n_ch ? coef_x[(int64_t)a * n_ch + j] : 0.f;
+        else
+            cf[i][j] = (i < L && j < n_ch) ? coef_f[((int64_t)a * L + i) * n_ch + j] : 0.f;
+    }
+    __syncthreads();
+    if (w >= W) return;
+    const double th = (double)theta[a];
+    const RotGeom g = rot_geom((float)cos(th), (float)sin(th), H, W);
+    const int64_t HW = (int64_t)H * W;
+    float gbar[kMaxL];
+#pragma unroll
+    for (int l = 0; l < kMaxL; ++l) gbar[l] = 0.f;
+    for (int h = 0; h < H; ++h) {
+        const RotTap tp = rot_tap(g, h, w);
+        float fr[kMaxCh];
+#pragma unroll
+        for (int j = 0; j < kMaxCh; ++j)
+            fr[j] = j < n_ch ? rot_sample_tap(frac + ((int64_t)j * S + s) * HW, H, W, tp) : 0.f;
+        float dmux[kMaxCh];
+#pragma unroll
+        for (int j = 0; j < kMaxCh; ++j) dmux[j] = 0.f;
+        if (incident_mode == 0) {
+#pragma unroll
+            for (int l = 0; l < kMaxL; ++l) {
+                if (l >= L) break;
+                const int64_t o = (((int64_t)l * n_a + al) * S + s) * HW + (int64_t)h * W + w;
+                const float f = 1.f - fr[l] * cx[l];
+                const float df = h > 0 ? gbar[l] * INC[o] : 0.f;
+                gbar[l] = h > 0 ? fmaf(gbar[l], f, dinc[o]) : dinc[o];
+                dmux[l] = -df;
+            }
+        } else if (incident_mode == 1) {
+            // one recursion on the summed adjoint: every element sees the same f
+            float ftot = 1.f, dsum = 0.f;
+#pragma unroll
+            for (int j = 0; j < kMaxCh; ++j)
+                if (j < n_ch) ftot *= 1.f - fr[j] * cx[j];
+            for (int l = 0; l < L; ++l)
+                dsum += dinc[(((int64_t)l * n_a + al) * S + s) * HW + (int64_t)h * W + w];
+            const float inc = INC[(((int64_t)0 * n_a + al) * S + s) * HW + (int64_t)h * W + w];
+            const float df = h > 0 ? gbar[0] * inc : 0.f;
+            gbar[0] = h > 0 ? fmaf(gbar[0], ftot, dsum) : dsum;
+#pragma unroll
+            for (int j = 0; j < kMaxCh; ++j) {
+                if (j >= n_ch) break;
+                float others = 1.f;
+#pragma unroll
+                for (int k = 0; k < kMaxCh; ++k)
+                    if (k < n_ch && k != j) others *= 1.f - fr[k] * cx[k];
+                dmux[j] = -df * others;
+            }
+        }
+        // fluorescence mu gradient of every line at this sample
+        float dmuf[kMaxL];
+#pragma unroll
+        for (int l = 0; l < kMaxL; ++l) {
+            dmuf[l] = 0.f;
+            if (l < L)
+                dmuf[l] = __ldg(dmu_rev + ((((int64_t)al * L + l) * S + s) * W + (W - 1 - w)) * H +
+                                (H - 1 - h));
+        }
+        // only the concentration channels (j < L) carry a gradient
+#pragma unroll
+        for (int j = 0; j < kMaxL; ++j) {
+            if (j >= L) break;
+            float d = cx[j] * dmux[j];
+#pragma unroll
+            for (int l = 0; l < kMaxL; ++l)
+                if (l < L) d = fmaf(cf[l][j], dmuf[l], d);
+            if (d != 0.f) rot_splat_tap(dC + ((int64_t)j * S + s) * HW, H, W, tp, d);
+        }
+    }
+}
+
+size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
+
+struct XrfBufs {
+    float *INC, *E, *ATT, *DINC, *MU, *DRES, *DMU, *TMP;
+};
+
+size_t xrf_layout(int64_t S, int64_t H, int64_t W, int64_t L, int64_t chunk, char* base,
+                  XrfBufs* b) {
+    const size_t vol = align256(sizeof(float) * (size_t)L * chunk * S * H * W);
+    const size_t one = align256(sizeof(float) * (size_t)S * H * W);
+    if (b) {
+        float** p[7] = {&b->INC, &b->E, &b->ATT, &b->DINC, &b->MU, &b->DRES, &b->DMU};
+        for (int i = 0; i < 7; ++i) *p[i] = (float*)(base + i * vol);
+        b->TMP = (float*)(base + 7 * vol);
+    }
+    return 7 * vol + one;
+}
+
+int64_t xrf_chunk(int64_t S, int64_t H, int64_t W, int64_t A, int64_t L, int64_t chunk) {
+    if (chunk <= 0) {
+        // about 1 GB of per-chunk scratch
+        int64_t per_angle = 7 * L * S * H * W * (int64_t)sizeof(float);
+        chunk = (1LL << 30) / (per_angle > 0 ? per_angle : 1);
+        if (chunk < 1) chunk = 1;
+    }
+    if (chunk > A) chunk = A;
+    if (chunk * L > 65535) chunk = 65535 / L;
+    return chunk < 1 ? 1 : chunk;
+}
+
+int check_xrf_args(int64_t n_ch, int64_t S, int64_t H, int64_t W, int64_t A, int64_t L,
+                   int64_t Mz, int64_t Mx, int64_t My, int incident_mode) {
+    FLC_REQUIRE(n_ch >= 1 && n_ch <= kMaxCh && L >= 1 && L <= kMaxL && L <= n_ch,
+                "xrf: need 1 <= L <= n_ch <= %d", kMaxCh);
+    FLC_REQUIRE(H == W && H >= 2 && W <= 1024 && S >= 1 && S <= 65535 && A >= 1,
+                "xrf: needs square slices 2 <= H == W <= 1024");
+    FLC_REQUIRE(Mz >= 1 && Mx >= 1 && My >= 1 && (Mz & 1) && (My & 1),
+                "xrf: the cone mask needs odd slice/column extents (got %lld x %lld)",
+                (long long)Mz, (long long)My);
+    FLC_REQUIRE(incident_mode >= 0 && incident_mode <= 2, "xrf: bad incident_mode");
+    return FLC_OK;
+}
+
+}  // namespace
+
+size_t xrf_ws_bytes(int64_t S, int64_t H, int64_t W, int64_t A, int64_t L, int64_t chunk) {
+    return xrf_layout(S, H, W, L, xrf_chunk(S, H, W, A, L, chunk), nullptr, nullptr);
+}
+
+}  // namespace flc
+
+using namespace flc;
+
+extern "C" size_t flc_xrf_workspace_bytes(int64_t n_ch, int64_t S, int64_t H, int64_t W, int64_t A,
+                                          int64_t L, int64_t chunk) {
+    if (n_ch < 1 || S < 1 || H < 1 || W < 1 || A < 1 || L < 1) return 0;
+    return xrf_ws_bytes(S, H, W, A, L, chunk);
+}
+
+extern "C" int flc_xrf_project(const float* frac, const float* theta, const float* coef_x,
+                               const float* coef_f, const float* u, const float* v,
+                               const float* em, float* Pf, int64_t n_ch, int64_t S, int64_t H,
+                               int64_t W, int64_t A, int64_t L, int64_t Mz, int64_t Mx,
+                               int64_t My, int incident_mode, int64_t chunk, void* workspace,
+                               size_t workspace_bytes, void* stream) {
+    clear_error();
+    FLC_REQUIRE(frac && theta && coef_x && coef_f && u && v && em && Pf && workspace,
+                "flc_xrf_project: null pointer argument");
+    FLC_TRY(check_xrf_args(n_ch, S, H, W, A, L, Mz, Mx, My, incident_mode));
+    chunk = xrf_chunk(S, H, W, A, L, chunk);
+    size_t need = xrf_layout(S, H, W, L, chunk, nullptr, nullptr);
+    if (workspace_bytes < need || ((uintptr_t)workspace & 255)) {
+        set_error("flc_xrf_project: need a 256-byte aligned workspace of %zu bytes", need);
+        return workspace_bytes < need ? FLC_ERR_WORKSPACE : FLC_ERR_ALIGNMENT;
+    }
+    cudaStream_t st = as_stream(stream);
+    XrfBufs b;
+    xrf_layout(S, H, W, L, chunk, (char*)workspace, &b);
+    const int64_t vol = S * H * W;
+    for (int64_t a0 = 0; a0 < A; a0 += chunk) {
+        const int n_a = (int)(A - a0 < chunk ? A - a0 : chunk);
+        // incident term straight into ATT, fluorescence mu into MU
+        FLC_TRY(atten_stage_launch(frac, theta, coef_x, coef_f, b.ATT, b.MU, (int)n_ch, (int)S,
+                                   (int)H, (int)W, (int)L, vol, (int64_t)n_a * vol, (int)a0, n_a,
+                                   incident_mode, 1, st, 0));
+        FLC_TRY(cone_sep_launch(b.MU, u, v, b.ATT, (int64_t)n_a * L, S, W, H, Mz, Mx, My, 2,
+                                (int)L, 0, vol, (int64_t)n_a * vol, st));
+        for (int64_t l = 0; l < L; ++l)
+            FLC_TRY(fwd_emission_launch(b.ATT + l * n_a * vol, frac + l * vol, em + l * A + a0,
+                                        theta + a0, Pf + (l * A + a0) * S * W, nullptr, n_a, S, 1,
+                                        H, W, st));
+    }
+    return FLC_OK;
+}
+
+extern "C" int flc_xrf_project_adjoint(const float* frac, const float* theta, const float* coef_x,
+                                       const float* coef_f, const float* u, const float* v,
+                                       const float* uf, const float* vf, const float* em,
+                                       const float* gPf, float* dC, int64_t n_ch, int64_t S,
+                                       int64_t H, int64_t W, int64_t A, int64_t L, int64_t Mz,
+                                       int64_t Mx, int64_t My, int incident_mode, int64_t chunk,
+                                       void* workspace, size_t workspace_bytes, void* stream) {
+    clear_error();
+    FLC_REQUIRE(frac && theta && coef_x && coef_f && u && v && uf && vf && em && gPf && dC &&
+                    workspace,
+                "flc_xrf_project_adjoint: null pointer argument");
+    FLC_TRY(check_xrf_args(n_ch, S, H, W, A, L, Mz, Mx, My, incident_mode));
+    chunk = xrf_chunk(S, H, W, A, L, chunk);
+    size_t need = xrf_layout(S, H, W, L, chunk, nullptr, nullptr);
+    if (workspace_bytes < need || ((uintptr_t)workspace & 255)) {
+        set_error("flc_xrf_project_adjoint: need a 256-byte aligned workspace of %zu bytes", need);
+        return workspace_bytes < need ? FLC_ERR_WORKSPACE : FLC_ERR_ALIGNMENT;
+    }
+    cudaStream_t st = as_stream(stream);
+    XrfBufs b;
+    xrf_layout(S, H, W, L, chunk, (char*)workspace, &b);
+    const int64_t vol = S * H * W;
+    FLC_TRY_CUDA(cudaMemsetAsync(dC, 0, sizeof(float) * L * vol, st));
+    for (int64_t a0 = 0; a0 < A; a0 += chunk) {
+        const int n_a = (int)(A - a0 < chunk ? A - a0 : chunk);
+        const int64_t nv = (int64_t)n_a * L * vol;
+        // recompute the chunk: INC, E = exp(-cone), ATT = INC * E
+        FLC_TRY(atten_stage_launch(frac, theta, coef_x, coef_f, b.INC, b.MU, (int)n_ch, (int)S,
+                                   (int)H, (int)W, (int)L, vol, (int64_t)n_a * vol, (int)a0, n_a,
+                                   incident_mode, 1, st, 0));
+        FLC_TRY(cone_sep_launch(b.MU, u, v, b.E, (int64_t)n_a * L, S, W, H, Mz, Mx, My, 3, (int)L,
+                                0, vol, (int64_t)n_a * vol, st));
+        mul_kernel<<<(unsigned)ceil_div(nv, 256), 256, 0, st>>>(b.INC, b.E, b.ATT, nv);
+        FLC_TRY(check_launch("mul_kernel"));
+        // direct term: P^T[atten](dL/dPf) per element
+        for (int64_t l = 0; l < L; ++l) {
+            FLC_TRY(bwd_emission_launch(b.ATT + l * n_a * vol, gPf + (l * A + a0) * S * W,
+                                        em + l * A + a0, theta + a0, b.TMP, n_a, S, 1, H, W, 0.f,
+                                        st));
+            add_kernel<<<(unsigned)ceil_div(vol, 256), 256, 0, st>>>(dC + l * vol, b.TMP, vol);
+            FLC_TRY(check_launch("add_kernel"));
+        }
+        // through the attenuation
+        dim3 gg((unsigned)(ceil_div(W, 32) * ceil_div(H, 32)), (unsigned)S, (unsigned)(n_a * L));
+        xrf_g_kernel<<<gg, dim3(32, 8), 0, st>>>(frac, theta, em, gPf, b.ATT, b.E, b.DINC, b.DRES,
+                                                  (int)L, (int)A, (int)a0, n_a, (int)S, (int)H,
+                                                  (int)W);
+        FLC_TRY(check_launch("xrf_g_kernel"));
+        FLC_TRY(cone_sep_launch(b.DRES, uf, vf, b.DMU, (int64_t)n_a * L, S, W, H, Mz, Mx, My, 0,
+                                1, 0, 0, 0, st));
+        const int threads = (int)((W + 31) & ~31);
+        xrf_stage_adjoint_kernel<<<dim3((unsigned)S, (unsigned)n_a), threads, 0, st>>>(
+            frac, theta, coef_x, coef_f, b.INC, b.DINC, b.DMU, dC, (int)n_ch, (int)S, (int)H,
+            (int)W, (int)L, (int)a0, n_a, incident_mode);
+        FLC_TRY(check_launch("xrf_stage_adjoint_kernel"));
+    }
+    return FLC_OK;
+}

@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "flc_common.cuh"
+#include "flc_geom.cuh"
 
 namespace flc {
 namespace {
@@ -31,39 +32,7 @@ namespace {
 // (affine_grid with [[c,-s,0],[s,c,0]], align_corners=False, unnormalised),
 // bilinear, zero padding outside the image.
 // ---------------------------------------------------------------------------
-struct RotGeom {
-    float c, s, cx, cy, sxw, syh;  // sxw = W/H, syh = H/W
-};
-
-__device__ __forceinline__ float rot_sample(const float* __restrict__ img, int H, int W,
-                                            const RotGeom& g, int h, int w) {
-    float dw = (float)w - g.cx, dh = (float)h - g.cy;
-    float ix = g.c * dw - g.s * dh * g.sxw + g.cx;
-    float iy = g.s * dw * g.syh + g.c * dh + g.cy;
-    float fx = floorf(ix), fy = floorf(iy);
-    int x0 = (int)fx, y0 = (int)fy;
-    float tx = ix - fx, ty = iy - fy;
-    bool xin0 = x0 >= 0 && x0 < W, xin1 = x0 + 1 >= 0 && x0 + 1 < W;
-    bool yin0 = y0 >= 0 && y0 < H, yin1 = y0 + 1 >= 0 && y0 + 1 < H;
-    float v00 = (yin0 && xin0) ? __ldg(img + y0 * W + x0) : 0.f;
-    float v01 = (yin0 && xin1) ? __ldg(img + y0 * W + x0 + 1) : 0.f;
-    float v10 = (yin1 && xin0) ? __ldg(img + (y0 + 1) * W + x0) : 0.f;
-    float v11 = (yin1 && xin1) ? __ldg(img + (y0 + 1) * W + x0 + 1) : 0.f;
-    float top = fmaf(tx, v01 - v00, v00);
-    float bot = fmaf(tx, v11 - v10, v10);
-    return fmaf(ty, bot - top, top);
-}
-
-__host__ __device__ inline RotGeom rot_geom(float c, float s, int H, int W) {
-    RotGeom g;
-    g.c = c;
-    g.s = s;
-    g.cx = (W - 1) * 0.5f;
-    g.cy = (H - 1) * 0.5f;
-    g.sxw = (float)W / (float)H;
-    g.syh = (float)H / (float)W;
-    return g;
-}
+// RotGeom / rot_sample live in flc_geom.cuh, shared with the adjoint kernels.
 
 __global__ void rotate_kernel(const float* __restrict__ x, float* __restrict__ out, int64_t N,
                               int H, int W, RotGeom g) {
@@ -112,7 +81,7 @@ __global__ void atten_stage_kernel(const float* __restrict__ frac, const float* 
                                    const float* __restrict__ coef_f, float* __restrict__ out,
                                    float* __restrict__ mu_ref, int n_ch, int S, int H, int W,
                                    int L, int64_t out_a_stride, int64_t out_l_stride, int a_base,
-                                   int incident_mode, int write_mu) {
+                                   int incident_mode, int write_mu, int out_a0) {
     extern __shared__ float stage[];  // [L][kStageRows][W]
     __shared__ StageCoef cf;
     const int s = blockIdx.x;
@@ -143,7 +112,7 @@ __global__ void atten_stage_kernel(const float* __restrict__ frac, const float* 
         if (w < W && incident_mode != 2) {
 #pragma unroll
             for (int i = 0; i < kMaxL; ++i)
-                if (i < L) out[i * out_l_stride + a * out_a_stride + s * HW + (int64_t)h * W + w] = prod[i];
+                if (i < L) out[i * out_l_stride + (int64_t)(out_a0 + al) * out_a_stride + s * HW + (int64_t)h * W + w] = prod[i];
             if (incident_mode == 0) {
 #pragma unroll
                 for (int i = 0; i < kMaxL; ++i)
@@ -159,7 +128,7 @@ __global__ void atten_stage_kernel(const float* __restrict__ frac, const float* 
         } else if (w < W) {
 #pragma unroll
             for (int i = 0; i < kMaxL; ++i)
-                if (i < L) out[i * out_l_stride + a * out_a_stride + s * HW + (int64_t)h * W + w] = 1.f;
+                if (i < L) out[i * out_l_stride + (int64_t)(out_a0 + al) * out_a_stride + s * HW + (int64_t)h * W + w] = 1.f;
         }
         if (!write_mu) continue;
         const int row = (H - 1 - h) % kStageRows;  // y = H-1-h within the staged block
@@ -374,7 +343,8 @@ cone_sep_kernel(const float* __restrict__ mu, const float* __restrict__ U,
     // ---- epilogue ----
     const int y = y0 + t;
     if (zs >= Z || y >= Y) return;
-    if (mode == 2) {
+    if (mode >= 2) {
+        // beam layout: 2 multiplies exp(-res) in, 3 stores exp(-res)
         const int al = v / L, l = v - al * L;
         float* ob = out + l * out_l_stride + (int64_t)(a_base + al) * out_a_stride;
         const int h = Y - 1 - y;
@@ -384,8 +354,11 @@ cone_sep_kernel(const float* __restrict__ mu, const float* __restrict__ U,
             if (z >= Z) break;
             float* o = ob + ((int64_t)z * Y + h) * X + x0;
 #pragma unroll
-            for (int j = 0; j < kXB; ++j)
-                if (x0 + j < X) o[j] *= expf(-acc[j][q]);
+            for (int j = 0; j < kXB; ++j) {
+                if (x0 + j >= X) continue;
+                const float e = expf(-acc[j][q]);
+                if (mode == 2) o[j] *= e; else o[j] = e;
+            }
         }
     } else {
         float* ov = out + (int64_t)v * Z * X * Y;
@@ -503,6 +476,7 @@ namespace {
 size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
 
 int64_t pick_chunk(int64_t S, int64_t H, int64_t W, int64_t A, int64_t L, int64_t chunk) {
+    if (chunk <= 0) chunk = tune(kTuneAttenChunk);
     if (chunk <= 0) {
         int64_t vol = L * S * H * W * (int64_t)sizeof(float);
         chunk = (64LL << 20) / (vol > 0 ? vol : 1);
@@ -523,14 +497,14 @@ size_t atten_ws_bytes(int64_t S, int64_t H, int64_t W, int64_t A, int64_t L, int
 int atten_stage_launch(const float* frac, const float* theta, const float* coef_x,
                        const float* coef_f, float* out, float* mu_ref, int n_ch, int S, int H,
                        int W, int L, int64_t out_a_stride, int64_t out_l_stride, int a_base,
-                       int n_a, int incident_mode, int write_mu, cudaStream_t st) {
+                       int n_a, int incident_mode, int write_mu, cudaStream_t st, int out_a0) {
     size_t smem = sizeof(float) * (size_t)L * kStageRows * W;
     int threads = (W + 31) & ~31;
     FLC_TRY_CUDA(cudaFuncSetAttribute((const void*)atten_stage_kernel,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     atten_stage_kernel<<<dim3((unsigned)S, (unsigned)n_a), threads, smem, st>>>(
         frac, theta, coef_x, coef_f, out, mu_ref, n_ch, S, H, W, L, out_a_stride, out_l_stride,
-        a_base, incident_mode, write_mu);
+        a_base, incident_mode, write_mu, out_a0 < 0 ? a_base : out_a0);
     return check_launch("atten_stage_kernel");
 }
 
@@ -546,7 +520,7 @@ int atten_maps_launch(const float* frac, const float* theta, const float* coef_x
         int n_a = (int)(A - a0 < chunk ? A - a0 : chunk);
         FLC_TRY(atten_stage_launch(frac, theta, coef_x, coef_f, out, mu_ref, (int)n_ch, (int)S,
                                    (int)H, (int)W, (int)L, out_a, out_l, (int)a0, n_a,
-                                   incident_mode, xrf_mode == 0, st));
+                                   incident_mode, xrf_mode == 0, st, -1));
         if (xrf_mode != 0) continue;
         // reference frame of the cone: (Z=S, X=W, Y=H)
         FLC_TRY(cone_sep_launch(mu_ref, u, v, out, (int64_t)n_a * L, S, W, H, Mz, Mx, My, 2,
@@ -709,7 +683,7 @@ extern "C" int flc_atten_stage(const float* frac, const float* theta, const floa
     FLC_REQUIRE(incident_mode >= 0 && incident_mode <= 2, "flc_atten_stage: bad incident_mode");
     return atten_stage_launch(frac, theta, coef_x, coef_f, out, mu_ref, (int)n_ch, (int)S, (int)H,
                               (int)W, (int)L, S * H * W, A * S * H * W, (int)a0, (int)n_a,
-                              incident_mode, write_mu, as_stream(stream));
+                              incident_mode, write_mu, as_stream(stream), -1);
 }
 
 extern "C" int flc_cone_atten_apply(const float* mu_ref, const float* u, const float* v,

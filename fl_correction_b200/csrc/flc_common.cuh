@@ -30,6 +30,16 @@ inline int check_launch(const char* what) {
 
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// Launch-shape knobs (set by the autotuner through flc_tune_set; 0 = auto).
+enum TuneKey {
+    kTuneProjCluster = 0,   // max CTAs per slice cluster for the backward / MLEM kernels
+    kTuneProjApc = 1,       // angles per CTA for the projector kernels
+    kTuneConeVariant = 2,   // 1: TMA 16x8 tile, 2: TMA 8x4 tile, 3: plain kernel
+    kTuneAttenChunk = 3,    // angles per attenuation-pipeline pass
+    kTuneCount = 4
+};
+int64_t tune(int key);
+
 // Number of SMs of the current device (cached per device).
 int sm_count();
 // Opt-in shared memory per block of the current device (cached per device).

@@ -144,14 +144,15 @@ cone_tma_kernel(const __grid_constant__ CUtensorMap tmap, const float* __restric
     const int tid = threadIdx.x;
     const int nthr = blockDim.x;
 
-    // shared layout: S[2][Z][boxW] | X[XB][TY][PZ] | wy[2][XB][WY] | wz[2][XB][WZ] | bars
+    // shared layout: S[2][Z][boxW] | X[XB][TY][PZ] | wy[Mx][WY] | wz[Mx][WZ] |
+    //               meta[Mx][8] | bars[2]
     const int sbuf = (Z * g.boxW + 31) & ~31;  // 128-byte aligned TMA destinations
     float* S = reinterpret_cast<float*>(smem_raw);
     float* Xs = S + 2 * sbuf;
     float* wy = Xs + XB * TY * g.PZ;
-    float* wz = wy + 2 * XB * g.WY;
-    int* meta = reinterpret_cast<int*>(wz + 2 * XB * g.WZ);  // [2][XB][4]: act, mlo_y, mhi_y, mlo_z, (mhi_z)
-    uint64_t* bars = reinterpret_cast<uint64_t*>(meta + 2 * XB * 8);
+    float* wz = wy + g.Mx * g.WY;
+    int* meta = reinterpret_cast<int*>(wz + g.Mx * g.WZ);  // per depth: on, ylo, yhi, zlo, zhi
+    uint64_t* bars = reinterpret_cast<uint64_t*>(meta + g.Mx * 8);
     __shared__ int s_fail;
 
     const int p_begin = x0;
@@ -172,6 +173,42 @@ cone_tma_kernel(const __grid_constant__ CUtensorMap tmap, const float* __restric
             tma_load_3d(S + q * sbuf, &tmap, y0 - g.HYP, p_begin + q, v * Z, &bars[q]);
         }
     }
+    // every depth's filters, zero-padded and shifted so that tap m of a row
+    // lines up with input column t + m (y) / row z + m (z); then each depth's
+    // tap support, found by warp ballots
+    for (int i = tid; i < g.Mx * g.WY; i += nthr) {
+        const int d = i / g.WY, dy = i - d * g.WY - g.offy;
+        wy[i] = (dy >= 0 && dy < g.My) ? __ldg(V + (int64_t)d * g.My + dy) : 0.f;
+    }
+    for (int i = tid; i < g.Mx * g.WZ; i += nthr) {
+        const int d = i / g.WZ, dz = i - d * g.WZ - g.offz;
+        wz[i] = (dz >= 0 && dz < g.Mz) ? __ldg(U + (int64_t)d * g.Mz + dz) : 0.f;
+    }
+    __syncthreads();
+    {
+        const int lane = tid & 31, warp = tid >> 5, nwarps = (nthr + 31) >> 5;
+        for (int d = warp; d < g.Mx; d += nwarps) {
+            int lo = 1 << 30, hi = -1, loz = 1 << 30, hiz = -1;
+            for (int m0 = 0; m0 < g.WY; m0 += 32) {
+                const int m = m0 + lane;
+                unsigned bal = __ballot_sync(0xffffffffu, m < g.WY && wy[d * g.WY + min(m, g.WY - 1)] != 0.f);
+                if (bal) { lo = min(lo, m0 + __ffs(bal) - 1); hi = m0 + 31 - __clz(bal); }
+            }
+            for (int m0 = 0; m0 < g.WZ; m0 += 32) {
+                const int m = m0 + lane;
+                unsigned bal = __ballot_sync(0xffffffffu, m < g.WZ && wz[d * g.WZ + min(m, g.WZ - 1)] != 0.f);
+                if (bal) { loz = min(loz, m0 + __ffs(bal) - 1); hiz = m0 + 31 - __clz(bal); }
+            }
+            if (lane == 0) {
+                const int on = hi >= 0 && hiz >= 0;
+                meta[d * 8 + 0] = on;
+                meta[d * 8 + 1] = on ? (lo & ~3) : 0;
+                meta[d * 8 + 2] = on ? hi + 1 : 0;
+                meta[d * 8 + 3] = on ? (loz & ~3) : 0;
+                meta[d * 8 + 4] = on ? hiz + 1 : 0;
+            }
+        }
+    }
 
     // z-filter ownership: (j, t, zb) with t fastest
     const int zt_t = tid % TY;
@@ -188,41 +225,6 @@ cone_tma_kernel(const __grid_constant__ CUtensorMap tmap, const float* __restric
         const int step = p - p_begin;
         const int buf = step & 1;
         const uint32_t parity = (uint32_t)((step >> 1) & 1);
-        // weights and tap support of the XB targets this plane feeds: warp w
-        // stages target j = w, w + nwarps, ... and finds its support by ballot
-        float* wyb = wy + buf * XB * g.WY;
-        float* wzb = wz + buf * XB * g.WZ;
-        int* mb = meta + buf * XB * 8;
-        {
-            const int lane = tid & 31, warp = tid >> 5, nwarps = (nthr + 31) >> 5;
-            for (int j = warp; j < XB; j += nwarps) {
-                const int d = p - (x0 + j);
-                const bool act = d >= 0 && d < g.Mx && x0 + j < X;
-                int lo = 1 << 30, hi = -1, loz = 1 << 30, hiz = -1;
-                for (int m0 = 0; m0 < g.WY; m0 += 32) {
-                    int m = m0 + lane, dy = m - g.offy;
-                    float w = (act && m < g.WY && dy >= 0 && dy < g.My) ? __ldg(V + (int64_t)d * g.My + dy) : 0.f;
-                    if (m < g.WY) wyb[j * g.WY + m] = w;
-                    unsigned bal = __ballot_sync(0xffffffffu, w != 0.f);
-                    if (bal) { lo = min(lo, m0 + __ffs(bal) - 1); hi = m0 + 31 - __clz(bal); }
-                }
-                for (int m0 = 0; m0 < g.WZ; m0 += 32) {
-                    int m = m0 + lane, dz = m - g.offz;
-                    float w = (act && m < g.WZ && dz >= 0 && dz < g.Mz) ? __ldg(U + (int64_t)d * g.Mz + dz) : 0.f;
-                    if (m < g.WZ) wzb[j * g.WZ + m] = w;
-                    unsigned bal = __ballot_sync(0xffffffffu, w != 0.f);
-                    if (bal) { loz = min(loz, m0 + __ffs(bal) - 1); hiz = m0 + 31 - __clz(bal); }
-                }
-                if (lane == 0) {
-                    int on = hi >= 0 && hiz >= 0;
-                    mb[j * 8 + 0] = on;
-                    mb[j * 8 + 1] = on ? (lo & ~3) : 0;
-                    mb[j * 8 + 2] = on ? hi + 1 : 0;
-                    mb[j * 8 + 3] = on ? (loz & ~3) : 0;
-                    mb[j * 8 + 4] = on ? hiz + 1 : 0;
-                }
-            }
-        }
         if (tid == 0 && !mbar_wait(&bars[buf], parity)) s_fail = 1 + step;
         __syncthreads();
         if (s_fail) break;
@@ -234,11 +236,12 @@ cone_tma_kernel(const __grid_constant__ CUtensorMap tmap, const float* __restric
             int rest = it / Z;
             int half = rest % (TY / 8);
             int j = rest / (TY / 8);
-            if (!mb[j * 8]) continue;
+            const int d = p - (x0 + j);
+            if (d < 0 || d >= g.Mx || x0 + j >= X || !meta[d * 8]) continue;
             float a8[8];
 #pragma unroll
             for (int k = 0; k < 8; ++k) a8[k] = 0.f;
-            corr8(a8, Sb + z * g.boxW + half * 8, wyb + j * g.WY, mb[j * 8 + 1], mb[j * 8 + 2]);
+            corr8(a8, Sb + z * g.boxW + half * 8, wy + d * g.WY, meta[d * 8 + 1], meta[d * 8 + 2]);
             float* xo = Xs + (j * TY + half * 8) * g.PZ + g.HZP + z;
 #pragma unroll
             for (int k = 0; k < 8; ++k) xo[k * g.PZ] = a8[k];
@@ -251,10 +254,11 @@ cone_tma_kernel(const __grid_constant__ CUtensorMap tmap, const float* __restric
             tma_load_3d(S + buf * sbuf, &tmap, y0 - g.HYP, p + 2, v * Z, &bars[buf]);
         }
         // ---- z filter: acc[z] += sum_m wz[j][m] * X[j][t][z + m] ----
-        if (zt_on && mb[zt_j * 8]) {
+        const int dz_ = p - (x0 + zt_j);
+        if (zt_on && dz_ >= 0 && dz_ < g.Mx && x0 + zt_j < X && meta[dz_ * 8]) {
             const float* xr = Xs + (zt_j * TY + zt_t) * g.PZ;
-            const float* wr = wzb + zt_j * g.WZ;
-            const int mlo = mb[zt_j * 8 + 3], mhi = mb[zt_j * 8 + 4];
+            const float* wr = wz + dz_ * g.WZ;
+            const int mlo = meta[dz_ * 8 + 3], mhi = meta[dz_ * 8 + 4];
 #pragma unroll
             for (int q = 0; q < 4; ++q) corr8(acc[q], xr + zt_zb * 32 + q * 8, wr, mlo, mhi);
         }
@@ -277,9 +281,10 @@ cone_tma_kernel(const __grid_constant__ CUtensorMap tmap, const float* __restric
     // ---- epilogue ----
     const int y = y0 + zt_t;
     const int x = x0 + zt_j;
-    if (mode == 2) {
-        // transpose through shared memory so that stores run along x
-        float* T = S;  // [Z][TY][XB]
+    if (mode >= 2) {
+        // beam layout (2: multiply exp(-res) in, 3: store exp(-res)); transpose
+        // through shared memory so that stores run along x
+        float* T = S;  // [Z][TY][XB], spans the S and X buffers (contiguous)
         __syncthreads();
         if (zt_on) {
 #pragma unroll
@@ -299,7 +304,8 @@ cone_tma_kernel(const __grid_constant__ CUtensorMap tmap, const float* __restric
             int yy = y0 + t, xx = x0 + j;
             if (yy >= Y || xx >= X) continue;
             float* o = ob + ((int64_t)z * Y + (Y - 1 - yy)) * X + xx;
-            *o *= expf(-T[i]);
+            const float e = expf(-T[i]);
+            if (mode == 2) *o *= e; else *o = e;
         }
         return;
     }
@@ -347,10 +353,11 @@ bool cone_tma_geom(int64_t Z, int64_t X, int64_t Y, int64_t Mz, int64_t Mx, int6
     if (*threads > 512) return false;
     size_t sb = ((size_t)g->Z * g->boxW + 31) & ~(size_t)31;
     size_t s = sizeof(float) * (2 * sb + (size_t)XB * TY * g->PZ +
-                                2 * (size_t)XB * (g->WY + g->WZ)) +
-               sizeof(int) * 2 * XB * 8 + 2 * sizeof(uint64_t) + 64;
+                                (size_t)g->Mx * (g->WY + g->WZ)) +
+               sizeof(int) * (size_t)g->Mx * 8 + 2 * sizeof(uint64_t) + 64;
     // the mode-2 epilogue reuses S for a [Z][TY][XB] tile
-    if ((size_t)g->Z * TY * XB > 2 * sb) return false;
+    // the mode-2 epilogue stages a [Z][TY][XB] tile over the S and X buffers
+    if ((size_t)g->Z * TY * XB > 2 * sb + (size_t)XB * TY * g->PZ) return false;
     *smem = s;
     return s <= (size_t)max_smem_optin();
 }
@@ -407,7 +414,10 @@ int cone_tma_launch(const float* mu, const float* U, const float* Vw, float* out
     ConeGeom g;
     size_t smem;
     int threads;
-    if (Z <= 128 && cone_tma_geom<16, 8>(Z, X, Y, Mz, Mx, My, &g, &smem, &threads))
+    const int64_t variant = tune(kTuneConeVariant);  // 0 auto, 1 16x8, 2 8x4, 3 plain
+    if (variant == 3) return FLC_ERR_UNSUPPORTED;
+    if ((variant == 1 || (variant == 0 && Z <= 128)) &&
+        cone_tma_geom<16, 8>(Z, X, Y, Mz, Mx, My, &g, &smem, &threads))
         return cone_tma_launch_t<16, 8>(mu, U, Vw, out, Vn, g, smem, threads, mode, L, a_base,
                                         out_a_stride, out_l_stride, st);
     if (cone_tma_geom<8, 4>(Z, X, Y, Mz, Mx, My, &g, &smem, &threads))

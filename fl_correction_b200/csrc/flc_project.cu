@@ -4,36 +4,43 @@
 // Reference semantics: FL/cuda_lib/atten_cuda_kernel.cu:91-446,495-616 and
 // FL/cuda_lib/atten_cuda.cpp:82-345.  The reference scatters with one global
 // atomicAdd per sample (forward) and four per sample per reference
-// (backward).  Here:
-//  * one CTA owns one slice b and a group of angles; the slice of C is staged
-//    once in shared memory (row pitch chosen to spread banks) and every
-//    bilinear tap is a shared-memory load;
+// (backward).  Here one CTA owns one slice b and a group of angles:
+//  * the slice of C is staged once in shared memory (row pitch == 3 mod 32,
+//    which spreads the rotated bilinear taps of a warp over the banks);
+//  * per angle the atten tile (H x W, contiguous) is copied into shared memory
+//    with coalesced 128-bit loads, issued one angle ahead into registers so
+//    the copy overlaps the previous angle's work;
 //  * the forward sums each detector column along the beam in registers and
 //    combines a fixed number of partial sums in a fixed order (no atomics,
 //    deterministic);
-//  * the backward splats into a shared-memory accumulator of the whole slice;
-//    the CTAs of one slice form a thread-block cluster and reduce their
-//    accumulators through distributed shared memory in rank order, so no
-//    partial buffer touches HBM;
+//  * the backward splats the exact transpose into a shared-memory image of the
+//    slice in nine phases: samples whose (h, w) agree modulo 3 sit >= 3 apart
+//    on the rotated lattice, so their 2x2 footprints are disjoint and plain
+//    read-modify-writes cannot race.  Only the border frame (rows 0, H-2, H-1,
+//    columns 0, W-2, W-1), where samples clamped to the edge pile up, takes
+//    shared atomics; samples clamped in both coordinates all land on one of
+//    the four corners and are summed in registers, then flushed once;
+//  * the CTAs of one slice form a thread-block cluster and reduce their images
+//    through distributed shared memory in rank order;
 //  * one MLEM iteration (forward, ratio, backward, Huber, update, clamp) is a
-//    single cluster launch: atten streams from HBM once per iteration in the
-//    forward pass and is re-read from L2 in the backward pass.
+//    single cluster launch that reads each atten tile from HBM once.
 
 #include <cooperative_groups.h>
 
 #include "flc_common.cuh"
+#include "flc_geom.cuh"
 
 namespace cg = cooperative_groups;
 
 namespace flc {
 namespace {
 
-constexpr int kThreads = 256;
+constexpr int kThreads = 512;
 constexpr int kMaxCluster = 8;
 constexpr int kMaxR = 8;
+constexpr int kTileRegs = 8;   // float4 per thread prefetched for the next tile
 
-// Row pitch (floats) of a staged slice: >= W and == 3 (mod 32), which keeps
-// the warp's 32 rotated taps spread over banks for every angle class.
+// Row pitch (floats) of a staged slice: >= W and == 3 (mod 32).
 __host__ __device__ inline int slice_pitch(int W) {
     int p = W;
     while ((p & 31) != 3) ++p;
@@ -43,17 +50,47 @@ __host__ __device__ inline int slice_pitch(int W) {
 // Partial sums per detector column: enough (w, part) items to fill the CTA.
 __host__ __device__ inline int col_parts(int W, int H) {
     int p = (2 * kThreads + W - 1) / W;
-    if (p > 8) p = 8;
+    if (p > 16) p = 16;
     if (p > H) p = H;
     return p < 1 ? 1 : p;
 }
 
-__device__ __forceinline__ float bilerp(const float* img, int pitch, const Tap& t) {
-    const float* p = img + t.i0 * pitch + t.j0;
-    float v00 = p[0], v01 = p[1], v10 = p[pitch], v11 = p[pitch + 1];
-    float top = fmaf(t.fc, v01 - v00, v00);
-    float bot = fmaf(t.fc, v11 - v10, v10);
-    return fmaf(t.fr, bot - top, top);
+// Sample geometry (Geo, sample, ...) lives in flc_geom.cuh, shared with the adjoints.
+
+// ---------------------------------------------------------------------------
+// Tile staging: copy n floats (16-byte aligned when vec) from global into a
+// register set (issue) and later into shared memory (commit).
+// ---------------------------------------------------------------------------
+struct TileRegs {
+    float4 r[kTileRegs];
+};
+
+__device__ __forceinline__ void tile_issue(TileRegs& t, const float* __restrict__ src, int n) {
+    const int n4 = n >> 2;
+#pragma unroll
+    for (int k = 0; k < kTileRegs; ++k) {
+        int i = threadIdx.x + k * blockDim.x;
+        if (i < n4) t.r[k] = __ldg(reinterpret_cast<const float4*>(src) + i);
+    }
+}
+
+__device__ __forceinline__ void tile_commit(const TileRegs& t, const float* __restrict__ src,
+                                            float* dst, int n) {
+    const int n4 = n >> 2;
+#pragma unroll
+    for (int k = 0; k < kTileRegs; ++k) {
+        int i = threadIdx.x + k * blockDim.x;
+        if (i < n4) reinterpret_cast<float4*>(dst)[i] = t.r[k];
+    }
+    // tiles larger than the register set, and the n % 4 tail, are copied directly
+    for (int i = kTileRegs * blockDim.x + threadIdx.x; i < n4; i += blockDim.x)
+        reinterpret_cast<float4*>(dst)[i] = __ldg(reinterpret_cast<const float4*>(src) + i);
+    for (int i = (n4 << 2) + threadIdx.x; i < n; i += blockDim.x) dst[i] = __ldg(src + i);
+}
+
+// Plain staged copy (used when the tile start is not 16-byte aligned).
+__device__ __forceinline__ void tile_copy(const float* __restrict__ src, float* dst, int n) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = __ldg(src + i);
 }
 
 // Loads R slices C[r, b] (H x W, row stride W) into smem with row pitch `pitch`.
@@ -69,52 +106,181 @@ __device__ void stage_slice(float* sC, const float* __restrict__ C, int R, int B
     }
 }
 
-// Forward projection of one (angle, slice) into spart[parts][W]:
-// spart[p][w] = sum over beam steps h of part p of atten * sum_r em_r * bilerp(C_r).
-__device__ void forward_angle(const float* __restrict__ atten_ab, const float* sC,
-                              int img_stride, int pitch, const float* em_a, int R,
-                              const ProjGeom& g, int H, int W, int parts, float* spart) {
-    int hper = (H + parts - 1) / parts;
+// ---------------------------------------------------------------------------
+// Forward of one (angle, slice): spart[p][w] = sum over beam steps h of part
+// p of atten[h][w] * sum_r em_r * bilerp(C_r).
+// ---------------------------------------------------------------------------
+__device__ void forward_angle(const float* sA, const float* sC, int img_stride, int pitch,
+                              const float* em_a, int R, const Geo& g, int H, int W, int parts,
+                              float* spart) {
+    const int hper = (H + parts - 1) / parts;
     for (int item = threadIdx.x; item < parts * W; item += blockDim.x) {
-        int part = item / W, w = item - part * W;
-        int h0 = part * hper, h1 = min(H, h0 + hper);
-        float wf = (float)w, acc = 0.f;
-#pragma unroll 4
-        for (int h = h0; h < h1; ++h) {
-            float a = __ldg(atten_ab + (int64_t)h * W + w);
-            Tap t = proj_tap(g, (float)h, wf);
-            float val = 0.f;
-            for (int r = 0; r < R; ++r) val = fmaf(em_a[r], bilerp(sC + r * img_stride, pitch, t), val);
-            acc = fmaf(a, val, acc);
+        const int part = item / W, w = item - part * W;
+        const int h0 = part * hper, h1 = min(H, h0 + hper);
+        const float bx = col_bx(g, w), by = col_by(g, w);
+        float acc0 = 0.f, acc1 = 0.f;
+        int h = h0;
+        float hf = (float)h0 - g.cy;
+        for (; h + 1 < h1; h += 2, hf += 2.f) {
+            Smp s0 = sample_xy(g, fmaf(g.c, hf, bx), fmaf(g.s, hf, by));
+            Smp s1 = sample_xy(g, fmaf(g.c, hf + 1.f, bx), fmaf(g.s, hf + 1.f, by));
+            float v0 = 0.f, v1 = 0.f;
+            for (int r = 0; r < R; ++r) {
+                const float* p0 = sC + r * img_stride + s0.i0 * pitch + s0.j0;
+                const float* p1 = sC + r * img_stride + s1.i0 * pitch + s1.j0;
+                float t0 = fmaf(s0.fy, p0[1] - p0[0], p0[0]);
+                float b0 = fmaf(s0.fy, p0[pitch + 1] - p0[pitch], p0[pitch]);
+                float t1 = fmaf(s1.fy, p1[1] - p1[0], p1[0]);
+                float b1 = fmaf(s1.fy, p1[pitch + 1] - p1[pitch], p1[pitch]);
+                v0 = fmaf(em_a[r], fmaf(s0.fx, b0 - t0, t0), v0);
+                v1 = fmaf(em_a[r], fmaf(s1.fx, b1 - t1, t1), v1);
+            }
+            acc0 = fmaf(sA[h * W + w], v0, acc0);
+            acc1 = fmaf(sA[(h + 1) * W + w], v1, acc1);
         }
-        spart[part * W + w] = acc;
+        if (h < h1) {
+            Smp s0 = sample_xy(g, fmaf(g.c, hf, bx), fmaf(g.s, hf, by));
+            float v0 = 0.f;
+            for (int r = 0; r < R; ++r) {
+                const float* p0 = sC + r * img_stride + s0.i0 * pitch + s0.j0;
+                float t0 = fmaf(s0.fy, p0[1] - p0[0], p0[0]);
+                float b0 = fmaf(s0.fy, p0[pitch + 1] - p0[pitch], p0[pitch]);
+                v0 = fmaf(em_a[r], fmaf(s0.fx, b0 - t0, t0), v0);
+            }
+            acc0 = fmaf(sA[h * W + w], v0, acc0);
+        }
+        spart[part * W + w] = acc0 + acc1;
     }
 }
 
-// Backward (splat) of one (angle, slice) into the smem accumulator sacc[R][H][pitch]:
-// sacc_r += em_r * atten * ratio[w] * bilinear weights, the transpose of forward_angle.
-__device__ void backward_angle(const float* __restrict__ atten_ab, const float* sratio,
-                               float* sacc, int img_stride, int pitch, const float* em_a, int R,
-                               const ProjGeom& g, int H, int W, int parts) {
-    int hper = (H + parts - 1) / parts;
-    for (int item = threadIdx.x; item < parts * W; item += blockDim.x) {
-        int part = item / W, w = item - part * W;
-        int h0 = part * hper, h1 = min(H, h0 + hper);
-        float wf = (float)w, rq = sratio[w];
-#pragma unroll 2
-        for (int h = h0; h < h1; ++h) {
-            float av = __ldg(atten_ab + (int64_t)h * W + w) * rq;
-            Tap t = proj_tap(g, (float)h, wf);
-            float w00 = (1.f - t.fc) * (1.f - t.fr), w01 = t.fc * (1.f - t.fr);
-            float w10 = (1.f - t.fc) * t.fr, w11 = t.fc * t.fr;
-            for (int r = 0; r < R; ++r) {
-                float v = em_a[r] * av;
-                float* p = sacc + r * img_stride + t.i0 * pitch + t.j0;
-                atomicAdd(p, v * w00);
-                atomicAdd(p + 1, v * w01);
-                atomicAdd(p + pitch, v * w10);
-                atomicAdd(p + pitch + 1, v * w11);
+// Corner sums of samples clamped in both coordinates, in registers for the
+// first kCornerR references: v[r][k], k = 2*xhigh + yhigh.  (Indexed with
+// compile-time constants only, so they stay in registers.)
+constexpr int kCornerR = 2;
+struct Corners {
+    float v[kCornerR][4];
+    __device__ __forceinline__ void zero() {
+#pragma unroll
+        for (int r = 0; r < kCornerR; ++r)
+#pragma unroll
+            for (int k = 0; k < 4; ++k) v[r][k] = 0.f;
+    }
+    __device__ __forceinline__ void add(int r, int k, float x) {
+#pragma unroll
+        for (int rr = 0; rr < kCornerR; ++rr)
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk) v[rr][kk] += (rr == r && kk == k) ? x : 0.f;
+    }
+};
+
+// Adds v, spread over the pixels of corner class k, into img with atomics.
+// Clamped coordinate 0 -> index 0 with weight 1; rmax -> indices ih, ih+1 with
+// weights 1-fxh, fxh (atten_cuda_kernel.cu:116-133).
+__device__ __forceinline__ void corner_add(float* img, int pitch, const Geo& g, int k, float v) {
+    const bool xh = k >= 2, yh = k & 1;
+    const int i0 = xh ? g.ih : 0, j0 = yh ? g.jh : 0;
+    const float fx = xh ? g.fxh : 0.f, fy = yh ? g.fyh : 0.f;
+    const float wr[2] = {1.f - fx, fx}, wc[2] = {1.f - fy, fy};
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            const float wgt = wc[b] * wr[a];
+            if (wgt != 0.f) atomicAdd(img + (i0 + a) * pitch + j0 + b, v * wgt);
+        }
+}
+
+__device__ __forceinline__ bool in_frame(int i, int j, int H, int W) {
+    return i == 0 || i >= H - 2 || j == 0 || j >= W - 2;
+}
+
+__device__ __forceinline__ void splat1(float* img, int pitch, int i, int j, float v, int H, int W) {
+    if (v == 0.f) return;
+    float* p = img + i * pitch + j;
+    if (in_frame(i, j, H, W))
+        atomicAdd(p, v);
+    else
+        *p += v;
+}
+
+// Backward of one (angle, slice): sacc_r += em_r * atten * ratio[w] * bilinear
+// weights, the exact transpose of forward_angle.  Nine phases of disjoint
+// footprints, separated by barriers.
+__device__ void backward_angle(const float* sA, const float* sratio, float* sacc, int img_stride,
+                               int pitch, const float* em_a, int R, const Geo& g, int H, int W,
+                               Corners& cs) {
+    const int nthr = blockDim.x;
+    for (int ph = 0; ph < 3; ++ph) {
+        for (int pw = 0; pw < 3; ++pw) {
+            const int nh = (H - ph + 2) / 3, nw = (W - pw + 2) / 3;
+            // item it = hh * nw + ww walks by nthr: advance (hh, ww) without
+            // division.  A phase can be empty (H or W <= 2): skip to the barrier.
+            const int dh = nw > 0 ? nthr / nw : 0, dw = nthr - dh * nw;
+            int hh = nw > 0 ? threadIdx.x / nw : nh, ww = threadIdx.x - hh * nw;
+            if (nh <= 0 || nw <= 0) hh = nh;
+            for (; hh < nh; hh += dh, ww += dw) {
+                if (ww >= nw) { ww -= nw; ++hh; if (hh >= nh) break; }
+                const int h = ph + 3 * hh, w = pw + 3 * ww;
+                const float av = sA[h * W + w] * sratio[w];
+                const float hf = (float)h - g.cy;
+                const float x = fmaf(g.c, hf, col_bx(g, w)), y = fmaf(g.s, hf, col_by(g, w));
+                if (x >= 1.f && x < (float)(H - 3) && y >= 1.f && y < (float)(W - 3)) {
+                    // interior: unclamped, footprint outside the border frame
+                    float fx, fy;
+                    const int i0 = ffloor(x, fx), j0 = ffloor(y, fy);
+                    const float w00 = (1.f - fy) * (1.f - fx), w01 = fy * (1.f - fx);
+                    const float w10 = (1.f - fy) * fx, w11 = fy * fx;
+                    for (int r = 0; r < R; ++r) {
+                        const float v = em_a[r] * av;
+                        float* p = sacc + r * img_stride + i0 * pitch + j0;
+                        p[0] += v * w00;
+                        p[1] += v * w01;
+                        p[pitch] += v * w10;
+                        p[pitch + 1] += v * w11;
+                    }
+                    continue;
+                }
+                const Smp s = sample_xy(g, x, y);
+                const bool xl = s.x <= 0.f, xh = s.x >= g.rmax;
+                const bool yl = s.y <= 0.f, yh = s.y >= g.cmax;
+                if ((xl || xh) && (yl || yh)) {
+                    const int k = (xh ? 2 : 0) + (yh ? 1 : 0);
+                    for (int r = 0; r < R; ++r) {
+                        if (r < kCornerR) cs.add(r, k, em_a[r] * av);
+                        else corner_add(sacc + r * img_stride, pitch, g, k, em_a[r] * av);
+                    }
+                    continue;
+                }
+                const float w00 = (1.f - s.fy) * (1.f - s.fx), w01 = s.fy * (1.f - s.fx);
+                const float w10 = (1.f - s.fy) * s.fx, w11 = s.fy * s.fx;
+                for (int r = 0; r < R; ++r) {
+                    const float v = em_a[r] * av;
+                    float* img = sacc + r * img_stride;
+                    splat1(img, pitch, s.i0, s.j0, v * w00, H, W);
+                    splat1(img, pitch, s.i0, s.j0 + 1, v * w01, H, W);
+                    splat1(img, pitch, s.i0 + 1, s.j0, v * w10, H, W);
+                    splat1(img, pitch, s.i0 + 1, s.j0 + 1, v * w11, H, W);
+                }
             }
+            __syncthreads();
+        }
+    }
+}
+
+// Adds the register corner sums into the image: warp-reduce, then one atomic
+// per warp and pixel.  The weights are those of the clamped coordinates
+// (0 -> row/col 0 with weight 1; rmax -> rows ih, ih+1 with 1-fxh, fxh).
+__device__ void flush_corners(Corners& cs, float* sacc, int img_stride, int pitch, const Geo& g,
+                              int R, int H, int W) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int r = 0; r < kCornerR; ++r) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            float v = cs.v[r][k];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (r < R && lane == 0 && v != 0.f) corner_add(sacc + r * img_stride, pitch, g, k, v);
         }
     }
 }
@@ -122,28 +288,39 @@ __device__ void backward_angle(const float* __restrict__ atten_ab, const float* 
 // ---------------------------------------------------------------------------
 // Forward projection: grid (angle groups, B); optional MLEM ratio epilogue.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads)
+// stage_tile: atten tiles are copied to shared memory (else read from global);
+// stage_c: the C slice is staged (else read from global with pitch W).
+__global__ void __launch_bounds__(kThreads, 1)
 proj_fwd_kernel(const float* __restrict__ atten, const float* __restrict__ C,
                 const float* __restrict__ em, const float* __restrict__ theta,
                 float* __restrict__ Pf, const float* __restrict__ I, int A, int B, int R,
-                int H, int W, int apc, int staged) {
-    extern __shared__ float smem[];
+                int H, int W, int apc, int stage_tile, int stage_c) {
+    extern __shared__ __align__(16) float smem[];
     const int b = blockIdx.y;
     const int a0 = blockIdx.x * apc, a1 = min(A, a0 + apc);
-    const int pitch = staged ? slice_pitch(W) : W;
+    const int pitch = stage_c ? slice_pitch(W) : W;
     const int parts = col_parts(W, H);
-    const int img_stride = staged ? H * pitch : B * H * W;
-    float* sC = smem;
-    float* spart = smem + (staged ? R * H * pitch : 0);
-    float* sem = spart + parts * W;
-    const float* Cb = staged ? sC : C + (int64_t)b * H * W;
-    if (staged) stage_slice(sC, C, R, B, b, H, W, pitch);
+    const int HW = H * W;
+    const int img_stride = stage_c ? H * pitch : B * HW;
+    float* sA = smem;                                        // [H*W] (16-byte aligned)
+    float* sC = sA + (stage_tile ? ((HW + 3) & ~3) : 0);     // [R][H][pitch]
+    float* spart = sC + (stage_c ? R * img_stride : 0);      // [parts][W]
+    float* sem = spart + parts * W;                          // [R]
+    const float* Cb = stage_c ? sC : C + (int64_t)b * HW;
+    const bool vec = stage_tile && ((HW & 3) == 0) && (((uintptr_t)atten & 15) == 0);
+    if (stage_c) stage_slice(sC, C, R, B, b, H, W, pitch);
+    TileRegs tr;
+    if (a0 < a1 && vec) tile_issue(tr, atten + ((int64_t)a0 * B + b) * HW, HW);
     for (int a = a0; a < a1; ++a) {
+        const float* src = atten + ((int64_t)a * B + b) * HW;
+        __syncthreads();  // previous angle done with sA / spart
+        if (vec) tile_commit(tr, src, sA, HW);
+        else if (stage_tile) tile_copy(src, sA, HW);
         if (threadIdx.x < R) sem[threadIdx.x] = em[a * R + threadIdx.x];
         __syncthreads();
-        ProjGeom g = proj_geom(theta[a], H, W);
-        const float* atten_ab = atten + ((int64_t)a * B + b) * H * W;
-        forward_angle(atten_ab, Cb, img_stride, pitch, sem, R, g, H, W, parts, spart);
+        if (a + 1 < a1 && vec) tile_issue(tr, atten + ((int64_t)(a + 1) * B + b) * HW, HW);
+        const Geo g = make_geo(theta[a], H, W);
+        forward_angle(stage_tile ? sA : src, Cb, img_stride, pitch, sem, R, g, H, W, parts, spart);
         __syncthreads();
         for (int w = threadIdx.x; w < W; w += blockDim.x) {
             float s = 0.f;
@@ -152,59 +329,79 @@ proj_fwd_kernel(const float* __restrict__ atten, const float* __restrict__ C,
             if (I) s = I[o] / fmaxf(s, 1e-6f);
             Pf[o] = s;
         }
-        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Cluster reduction of the G images (rank order) for this CTA's share of the
+// slice; `fn(i, r, h, w, back)` consumes each reduced pixel.
+// ---------------------------------------------------------------------------
+template <class Fn>
+__device__ void cluster_reduce(cg::cluster_group& cluster, float* sacc, int R, int H, int W,
+                               int pitch, Fn fn) {
+    const int G = (int)cluster.num_blocks();
+    const int rank = (int)cluster.block_rank();
+    const int img_stride = H * pitch;
+    const int64_t n = (int64_t)R * H * W;
+    const int64_t share = (n + G - 1) / G;
+    const int64_t i0 = rank * share, i1 = min(n, i0 + share);
+    for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+        const int r = (int)(i / ((int64_t)H * W));
+        const int rem = (int)(i - (int64_t)r * H * W);
+        const int h = rem / W, w = rem - h * W;
+        const int off = r * img_stride + h * pitch + w;
+        float s = 0.f;
+        for (int q = 0; q < G; ++q) s += cluster.map_shared_rank(sacc, q)[off];
+        fn(r, h, w, s);
     }
 }
 
 // ---------------------------------------------------------------------------
 // Backward projection: grid (G, B), cluster (G, 1, 1).  CTA g of slice b
-// splats angles [g*apc, (g+1)*apc) into its smem accumulator; the cluster
-// then reduces the G accumulators in rank order, each CTA finishing a 1/G
-// share of the slice.  ratio == nullptr means ratio = 1 (sensitivity).
-// clamp_min > 0 applies max(out, clamp_min) (the reference's sens clamp).
+// splats angles [g*apc, (g+1)*apc).  ratio == nullptr means ratio = 1
+// (sensitivity); clamp_min > 0 applies max(out, clamp_min).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 1)
 proj_bwd_kernel(const float* __restrict__ atten, const float* __restrict__ ratio,
                 const float* __restrict__ em, const float* __restrict__ theta,
                 float* __restrict__ out, int A, int B, int R, int H, int W, int apc,
-                float clamp_min) {
-    extern __shared__ float smem[];
+                float clamp_min, int stage_tile) {
+    extern __shared__ __align__(16) float smem[];
     cg::cluster_group cluster = cg::this_cluster();
-    const int G = (int)cluster.num_blocks();
-    const int rank = (int)cluster.block_rank();
     const int b = blockIdx.y;
     const int a0 = blockIdx.x * apc, a1 = min(A, a0 + apc);
     const int pitch = slice_pitch(W);
-    const int parts = col_parts(W, H);
+    const int HW = H * W;
     const int img_stride = H * pitch;
-    float* sacc = smem;
-    float* sratio = smem + R * img_stride;
+    float* sA = smem;
+    float* sacc = sA + (stage_tile ? ((HW + 3) & ~3) : 0);
+    float* sratio = sacc + R * img_stride;
     float* sem = sratio + W;
+    const bool vec = stage_tile && ((HW & 3) == 0) && (((uintptr_t)atten & 15) == 0);
     for (int i = threadIdx.x; i < R * img_stride; i += blockDim.x) sacc[i] = 0.f;
+    Corners cs;
+    cs.zero();
+    TileRegs tr;
+    if (a0 < a1 && vec) tile_issue(tr, atten + ((int64_t)a0 * B + b) * HW, HW);
     for (int a = a0; a < a1; ++a) {
+        const float* src = atten + ((int64_t)a * B + b) * HW;
         __syncthreads();
+        if (vec) tile_commit(tr, src, sA, HW);
+        else if (stage_tile) tile_copy(src, sA, HW);
         if (threadIdx.x < R) sem[threadIdx.x] = em[a * R + threadIdx.x];
         for (int w = threadIdx.x; w < W; w += blockDim.x)
             sratio[w] = ratio ? ratio[((int64_t)a * B + b) * W + w] : 1.f;
         __syncthreads();
-        ProjGeom g = proj_geom(theta[a], H, W);
-        backward_angle(atten + ((int64_t)a * B + b) * H * W, sratio, sacc, img_stride, pitch,
-                       sem, R, g, H, W, parts);
+        if (a + 1 < a1 && vec) tile_issue(tr, atten + ((int64_t)(a + 1) * B + b) * HW, HW);
+        backward_angle(stage_tile ? sA : src, sratio, sacc, img_stride, pitch, sem, R,
+                       make_geo(theta[a], H, W), H, W, cs);
     }
+    flush_corners(cs, sacc, img_stride, pitch, make_geo(0.f, H, W), R, H, W);
     cluster.sync();
-    const int64_t n = (int64_t)R * H * W;
-    const int64_t share = (n + G - 1) / G;
-    const int64_t i0 = rank * share, i1 = min(n, i0 + share);
-    for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
-        int r = (int)(i / (H * W));
-        int rem = (int)(i - (int64_t)r * H * W);
-        int h = rem / W, w = rem - h * W;
-        int off = r * img_stride + h * pitch + w;
-        float s = 0.f;
-        for (int q = 0; q < G; ++q) s += cluster.map_shared_rank(sacc, q)[off];
+    cluster_reduce(cluster, sacc, R, H, W, pitch, [&](int r, int h, int w, float s) {
         if (clamp_min > 0.f) s = fmaxf(s, clamp_min);
         out[(((int64_t)r * B + b) * H + h) * W + w] = s;
-    }
+    });
     cluster.sync();
 }
 
@@ -212,38 +409,45 @@ proj_bwd_kernel(const float* __restrict__ atten, const float* __restrict__ ratio
 // One fused MLEM iteration (grid (G, B), cluster (G,1,1)):
 //   Pf = max(P C, 1e-6); ratio = I / Pf; back = P^T ratio;
 //   C' = C*back / (sens + beta*huber(C))  (or C*back/sens), C' = max(C', 0)
-// as atten_cuda.cpp:321-342.  Reads C from Cin, writes Cout (ping-pong:
-// the Huber term needs the old neighbours).
+// as atten_cuda.cpp:321-342.  Reads C from Cin, writes Cout (ping-pong: the
+// Huber term needs the old neighbours).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 1)
 mlem_iter_kernel(const float* __restrict__ atten, const float* __restrict__ em,
                  const float* __restrict__ theta, const float* __restrict__ I,
                  const float* __restrict__ sens, const float* __restrict__ Cin,
                  float* __restrict__ Cout, int A, int B, int R, int H, int W, int apc,
                  float beta, float delta) {
-    extern __shared__ float smem[];
+    extern __shared__ __align__(16) float smem[];
     cg::cluster_group cluster = cg::this_cluster();
-    const int G = (int)cluster.num_blocks();
-    const int rank = (int)cluster.block_rank();
     const int b = blockIdx.y;
     const int a0 = blockIdx.x * apc, a1 = min(A, a0 + apc);
     const int pitch = slice_pitch(W);
     const int parts = col_parts(W, H);
+    const int HW = H * W;
     const int img_stride = H * pitch;
-    float* sC = smem;
+    float* sA = smem;
+    float* sC = sA + ((HW + 3) & ~3);
     float* sacc = sC + R * img_stride;
     float* spart = sacc + R * img_stride;
     float* sratio = spart + parts * W;
     float* sem = sratio + W;
+    const bool vec = ((HW & 3) == 0) && (((uintptr_t)atten & 15) == 0);
     stage_slice(sC, Cin, R, B, b, H, W, pitch);
     for (int i = threadIdx.x; i < R * img_stride; i += blockDim.x) sacc[i] = 0.f;
+    Corners cs;
+    cs.zero();
+    TileRegs tr;
+    if (a0 < a1 && vec) tile_issue(tr, atten + ((int64_t)a0 * B + b) * HW, HW);
     for (int a = a0; a < a1; ++a) {
+        const float* src = atten + ((int64_t)a * B + b) * HW;
         __syncthreads();
+        if (vec) tile_commit(tr, src, sA, HW); else tile_copy(src, sA, HW);
         if (threadIdx.x < R) sem[threadIdx.x] = em[a * R + threadIdx.x];
         __syncthreads();
-        ProjGeom g = proj_geom(theta[a], H, W);
-        const float* atten_ab = atten + ((int64_t)a * B + b) * H * W;
-        forward_angle(atten_ab, sC, img_stride, pitch, sem, R, g, H, W, parts, spart);
+        if (a + 1 < a1 && vec) tile_issue(tr, atten + ((int64_t)(a + 1) * B + b) * HW, HW);
+        const Geo g = make_geo(theta[a], H, W);
+        forward_angle(sA, sC, img_stride, pitch, sem, R, g, H, W, parts, spart);
         __syncthreads();
         for (int w = threadIdx.x; w < W; w += blockDim.x) {
             float s = 0.f;
@@ -251,40 +455,62 @@ mlem_iter_kernel(const float* __restrict__ atten, const float* __restrict__ em,
             sratio[w] = I[((int64_t)a * B + b) * W + w] / fmaxf(s, 1e-6f);
         }
         __syncthreads();
-        backward_angle(atten_ab, sratio, sacc, img_stride, pitch, sem, R, g, H, W, parts);
+        backward_angle(sA, sratio, sacc, img_stride, pitch, sem, R, g, H, W, cs);
     }
+    flush_corners(cs, sacc, img_stride, pitch, make_geo(0.f, H, W), R, H, W);
     cluster.sync();
-    const int64_t n = (int64_t)R * H * W;
-    const int64_t share = (n + G - 1) / G;
-    const int64_t i0 = rank * share, i1 = min(n, i0 + share);
-    for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
-        int r = (int)(i / (H * W));
-        int rem = (int)(i - (int64_t)r * H * W);
-        int h = rem / W, w = rem - h * W;
-        int off = r * img_stride + h * pitch + w;
-        float back = 0.f;
-        for (int q = 0; q < G; ++q) back += cluster.map_shared_rank(sacc, q)[off];
+    cluster_reduce(cluster, sacc, R, H, W, pitch, [&](int r, int h, int w, float back) {
         const float* img = sC + r * img_stride;
-        float cp = img[h * pitch + w];
-        int64_t gi = (((int64_t)r * B + b) * H + h) * W + w;
+        const float cp = img[h * pitch + w];
+        const int64_t gi = (((int64_t)r * B + b) * H + h) * W + w;
         float den = sens[gi];
         if (beta > 0.f) {
             float hg = 0.f;
-            const int dr[4] = {-1, 1, 0, 0};
-            const int dc[4] = {0, 0, -1, 1};
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                int rr = h + dr[k], cc = w + dc[k];
-                if (rr < 0 || rr >= H || cc < 0 || cc >= W) continue;
-                float d = cp - img[rr * pitch + cc];
-                hg += fabsf(d) <= delta ? d : copysignf(delta, d);
-            }
+            if (h > 0) { float d = cp - img[(h - 1) * pitch + w]; hg += fabsf(d) <= delta ? d : copysignf(delta, d); }
+            if (h + 1 < H) { float d = cp - img[(h + 1) * pitch + w]; hg += fabsf(d) <= delta ? d : copysignf(delta, d); }
+            if (w > 0) { float d = cp - img[h * pitch + w - 1]; hg += fabsf(d) <= delta ? d : copysignf(delta, d); }
+            if (w + 1 < W) { float d = cp - img[h * pitch + w + 1]; hg += fabsf(d) <= delta ? d : copysignf(delta, d); }
             den = __fadd_rn(den, __fmul_rn(beta, hg));
         }
-        float c = __fmul_rn(cp, back) / den;
-        Cout[gi] = fmaxf(c, 0.f);
-    }
+        Cout[gi] = fmaxf(__fmul_rn(cp, back) / den, 0.f);
+    });
     cluster.sync();
+}
+
+// Backward for slices whose image does not fit in shared memory: one thread
+// per (angle, slice, column) walks the beam and adds into global memory with
+// atomics (the reference's own scheme, atten_cuda_kernel.cu:390-446); `out`
+// must be zeroed first.
+__global__ void proj_bwd_global_kernel(const float* __restrict__ atten,
+                                       const float* __restrict__ ratio,
+                                       const float* __restrict__ em,
+                                       const float* __restrict__ theta, float* __restrict__ out,
+                                       int A, int B, int R, int H, int W) {
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    const int b = blockIdx.y, a = blockIdx.z;
+    if (w >= W) return;
+    const Geo g = make_geo(theta[a], H, W);
+    const float rq = ratio ? ratio[((int64_t)a * B + b) * W + w] : 1.f;
+    const float* at = atten + ((int64_t)a * B + b) * H * W;
+    for (int h = 0; h < H; ++h) {
+        const float av = at[(int64_t)h * W + w] * rq;
+        const Smp s = sample(g, h, w);
+        const float w00 = (1.f - s.fy) * (1.f - s.fx), w01 = s.fy * (1.f - s.fx);
+        const float w10 = (1.f - s.fy) * s.fx, w11 = s.fy * s.fx;
+        for (int r = 0; r < R; ++r) {
+            const float v = em[a * R + r] * av;
+            float* img = out + ((int64_t)r * B + b) * H * W + (int64_t)s.i0 * W + s.j0;
+            if (v * w00 != 0.f) atomicAdd(img, v * w00);
+            if (v * w01 != 0.f) atomicAdd(img + 1, v * w01);
+            if (v * w10 != 0.f) atomicAdd(img + W, v * w10);
+            if (v * w11 != 0.f) atomicAdd(img + W + 1, v * w11);
+        }
+    }
+}
+
+__global__ void clamp_min_kernel(float* __restrict__ x, int64_t n, float lo) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] = fmaxf(x[i], lo);
 }
 
 __global__ void huber_kernel(const float* __restrict__ C, float* __restrict__ grad, int64_t n,
@@ -296,15 +522,10 @@ __global__ void huber_kernel(const float* __restrict__ C, float* __restrict__ gr
     int r = rem / W, c = rem - r * W;
     const float* p = C + img * H * W;
     float cp = p[rem], g = 0.f;
-    const int dr[4] = {-1, 1, 0, 0};
-    const int dc[4] = {0, 0, -1, 1};
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        int rr = r + dr[k], cc = c + dc[k];
-        if (rr < 0 || rr >= H || cc < 0 || cc >= W) continue;
-        float d = cp - p[rr * W + cc];
-        g += fabsf(d) <= delta ? d : copysignf(delta, d);
-    }
+    if (r > 0) { float d = cp - p[rem - W]; g += fabsf(d) <= delta ? d : copysignf(delta, d); }
+    if (r + 1 < H) { float d = cp - p[rem + W]; g += fabsf(d) <= delta ? d : copysignf(delta, d); }
+    if (c > 0) { float d = cp - p[rem - 1]; g += fabsf(d) <= delta ? d : copysignf(delta, d); }
+    if (c + 1 < W) { float d = cp - p[rem + 1]; g += fabsf(d) <= delta ? d : copysignf(delta, d); }
     grad[i] = g;
 }
 
@@ -337,10 +558,11 @@ Plan plan_cluster(int64_t A, int64_t B, size_t smem_per_cta) {
     if (per_sm < 1) per_sm = 1;
     int64_t want = 2LL * sms * per_sm;
     int G = (int)ceil_div(want, B);
-    if (G > kMaxCluster) G = kMaxCluster;
+    int gmax = kMaxCluster;
+    if (int64_t t = tune(kTuneProjCluster)) gmax = (int)(t < kMaxCluster ? t : kMaxCluster);
+    if (G > gmax) G = gmax;
     if (G > A) G = (int)A;
     if (G < 1) G = 1;
-    p.G = G;
     p.apc = (int)ceil_div(A, G);
     p.G = (int)ceil_div(A, p.apc);
     p.smem = smem_per_cta;
@@ -367,13 +589,23 @@ int launch_cluster(const void* fn, dim3 grid, int G, size_t smem, cudaStream_t s
     return FLC_OK;
 }
 
-size_t bwd_smem(int64_t R, int64_t H, int64_t W) {
-    return sizeof(float) * (R * H * slice_pitch((int)W) + W + kMaxR);
+size_t tile_floats(int64_t H, int64_t W) { return (size_t)((H * W + 3) & ~3LL); }
+
+size_t fwd_smem(int64_t R, int64_t H, int64_t W, bool stage_tile, bool stage_c) {
+    int parts = col_parts((int)W, (int)H);
+    return sizeof(float) * ((stage_tile ? tile_floats(H, W) : 0) +
+                            (stage_c ? R * H * slice_pitch((int)W) : 0) + parts * W + kMaxR);
+}
+
+size_t bwd_smem(int64_t R, int64_t H, int64_t W, bool stage_tile) {
+    return sizeof(float) *
+           ((stage_tile ? tile_floats(H, W) : 0) + R * H * slice_pitch((int)W) + W + kMaxR);
 }
 
 size_t mlem_smem(int64_t R, int64_t H, int64_t W) {
     int parts = col_parts((int)W, (int)H);
-    return sizeof(float) * (2 * R * H * slice_pitch((int)W) + parts * W + W + kMaxR);
+    return sizeof(float) *
+           (tile_floats(H, W) + 2 * R * H * slice_pitch((int)W) + parts * W + W + kMaxR);
 }
 
 }  // namespace
@@ -382,39 +614,53 @@ size_t mlem_smem(int64_t R, int64_t H, int64_t W) {
 int bwd_emission_launch(const float* atten, const float* ratio, const float* em,
                         const float* theta, float* out, int64_t A, int64_t B, int64_t R,
                         int64_t H, int64_t W, float clamp_min, cudaStream_t st) {
-    size_t smem = bwd_smem(R, H, W);
-    if (smem > (size_t)max_smem_optin()) {
-        set_error("backward projector: slice %lldx%lld x R=%lld needs %zu B of shared memory (max %d)",
-                  (long long)H, (long long)W, (long long)R, smem, max_smem_optin());
-        return FLC_ERR_UNSUPPORTED;
+    const size_t cap = (size_t)max_smem_optin();
+    int stage_tile = bwd_smem(R, H, W, true) <= cap;
+    if (!stage_tile && bwd_smem(R, H, W, false) > cap) {
+        // the slice image does not fit on chip: global atomics
+        FLC_TRY_CUDA(cudaMemsetAsync(out, 0, sizeof(float) * R * B * H * W, st));
+        proj_bwd_global_kernel<<<dim3((unsigned)ceil_div(W, 128), (unsigned)B, (unsigned)A), 128, 0,
+                                 st>>>(atten, ratio, em, theta, out, (int)A, (int)B, (int)R,
+                                       (int)H, (int)W);
+        FLC_TRY(check_launch("proj_bwd_global_kernel"));
+        if (clamp_min > 0.f) {
+            int64_t n = R * B * H * W;
+            clamp_min_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, st>>>(out, n, clamp_min);
+            FLC_TRY(check_launch("clamp_min_kernel"));
+        }
+        return FLC_OK;
     }
+    size_t smem = bwd_smem(R, H, W, stage_tile);
     Plan p = plan_cluster(A, B, smem);
     int iA = (int)A, iB = (int)B, iR = (int)R, iH = (int)H, iW = (int)W, apc = p.apc;
     void* args[] = {(void*)&atten, (void*)&ratio, (void*)&em, (void*)&theta, (void*)&out,
-                    &iA, &iB, &iR, &iH, &iW, &apc, &clamp_min};
+                    &iA, &iB, &iR, &iH, &iW, &apc, &clamp_min, &stage_tile};
     return launch_cluster((const void*)proj_bwd_kernel, dim3(p.G, (unsigned)B), p.G, smem, st, args);
 }
 
 int fwd_emission_launch(const float* atten, const float* C, const float* em, const float* theta,
                         float* Pf, const float* I, int64_t A, int64_t B, int64_t R, int64_t H,
                         int64_t W, cudaStream_t st) {
-    int parts = col_parts((int)W, (int)H);
-    size_t staged_bytes = sizeof(float) * (R * H * slice_pitch((int)W) + parts * W + kMaxR);
-    int staged = staged_bytes <= (size_t)max_smem_optin() ? 1 : 0;
-    size_t smem = staged ? staged_bytes : sizeof(float) * (parts * W + kMaxR);
+    const size_t cap = (size_t)max_smem_optin();
+    int stage_tile = 1, stage_c = 1;
+    if (fwd_smem(R, H, W, true, true) > cap) stage_tile = 0;
+    if (!stage_tile && fwd_smem(R, H, W, false, true) > cap) stage_c = 0;
+    size_t smem = fwd_smem(R, H, W, stage_tile, stage_c);
     int per_sm = (int)(max_smem_optin() / (smem + 1024));
     if (per_sm < 1) per_sm = 1;
-    if (per_sm > 8) per_sm = 8;
+    if (per_sm > 4) per_sm = 4;
     int64_t want = 3LL * sm_count() * per_sm;
     int64_t groups = ceil_div(want, B);
     if (groups > A) groups = A;
     if (groups < 1) groups = 1;
     int apc = (int)ceil_div(A, groups);
+    if (int64_t t = tune(kTuneProjApc)) apc = (int)(t < A ? t : A);
     groups = ceil_div(A, apc);
     FLC_TRY_CUDA(cudaFuncSetAttribute((const void*)proj_fwd_kernel,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     proj_fwd_kernel<<<dim3((unsigned)groups, (unsigned)B), kThreads, smem, st>>>(
-        atten, C, em, theta, Pf, I, (int)A, (int)B, (int)R, (int)H, (int)W, apc, staged);
+        atten, C, em, theta, Pf, I, (int)A, (int)B, (int)R, (int)H, (int)W, apc, stage_tile,
+        stage_c);
     return check_launch("proj_fwd_kernel");
 }
 

@@ -10,6 +10,7 @@
 
 #include <stdarg.h>
 #include <stdio.h>
+#include <string.h>
 
 #include <atomic>
 #include <mutex>
@@ -52,6 +53,20 @@ static void query_device(int dev) {
     v = 0;
     cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     g_smem[dev] = v > 0 ? v : 48 * 1024;
+}
+
+namespace {
+std::atomic<int64_t> g_tune[kTuneCount];
+const char* const kTuneNames[kTuneCount] = {"proj.cluster", "proj.apc", "cone.variant",
+                                            "atten.chunk"};
+}  // namespace
+
+int64_t tune(int key) { return (key >= 0 && key < kTuneCount) ? g_tune[key].load() : 0; }
+
+int tune_index(const char* name) {
+    for (int i = 0; i < kTuneCount; ++i)
+        if (name && strcmp(name, kTuneNames[i]) == 0) return i;
+    return -1;
 }
 
 int sm_count() {
@@ -258,4 +273,24 @@ extern "C" int flc_mlem(float* C, const float* atten, const float* em, const flo
     if (graph) cudaGraphDestroy(graph);
     cudaStreamDestroy(cap);
     return status;
+}
+
+extern "C" int flc_tune_set(const char* name, int64_t value) {
+    clear_error();
+    int k = tune_index(name);
+    if (k < 0) {
+        set_error("flc_tune_set: unknown knob '%s'", name ? name : "(null)");
+        return FLC_ERR_INVALID_ARG;
+    }
+    if (value < 0) {
+        set_error("flc_tune_set: value must be >= 0 (0 = automatic)");
+        return FLC_ERR_INVALID_ARG;
+    }
+    g_tune[k].store(value);
+    return FLC_OK;
+}
+
+extern "C" int64_t flc_tune_get(const char* name) {
+    int k = tune_index(name);
+    return k < 0 ? -1 : g_tune[k].load();
 }

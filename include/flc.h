@@ -56,6 +56,16 @@ FLC_API int flc_device_status(int reset);
 /* Number of kernels this library has launched in this process (graph
  * replays count every kernel node they run).  For instrumentation. */
 FLC_API uint64_t flc_launch_count(void);
+/* Launch-shape knobs of this library (no counterpart in the reference; the
+ * autotuner in fl_correction_b200/tune.py sets them).  Names:
+ *   "proj.cluster"  max CTAs per slice cluster, backward/MLEM kernels (1..8)
+ *   "proj.apc"      angles per CTA, projector kernels
+ *   "cone.variant"  1: TMA 16x8 tile, 2: TMA 8x4 tile, 3: plain kernel
+ *   "atten.chunk"   angles per attenuation-pipeline pass
+ * 0 restores the automatic choice.  flc_tune_get returns -1 for an unknown
+ * name.  Process-wide; not synchronized with launches in flight. */
+FLC_API int flc_tune_set(const char* name, int64_t value);
+FLC_API int64_t flc_tune_get(const char* name);
 
 /* ---------------------------------------------------------------------
  * Cone-mask (fluorescence) path sum, reference layout.
@@ -166,6 +176,38 @@ FLC_API int flc_cone_atten_apply(const float* mu_ref, const float* u, const floa
                                  float* atten, int64_t n_a, int64_t L, int64_t S, int64_t H,
                                  int64_t W, int64_t A, int64_t a0, int64_t Mz, int64_t Mx,
                                  int64_t My, void* stream);
+
+/* ---------------------------------------------------------------------
+ * Differentiable corrected projection with per-angle recomputation.
+ *
+ * flc_xrf_project: Pf (L, A, S, W) of the concentrations frac[0:L] through
+ *   their own self-absorption: for each chunk of angles the attenuation
+ *   (incident scan x exp(-cone)) is rebuilt from frac (n_ch, S, H, W, the
+ *   first L channels are the element concentrations C_l) and used at once;
+ *   nothing of size A x volume is kept.  em (L, A) is em_cs * rho * pix.
+ * flc_xrf_project_adjoint: dC (L, S, H, W) = d<gPf, Pf>/dC, including the
+ *   dependence of the attenuation on C (rotation, mu assembly, incident scan
+ *   and cone are differentiated by hand).  uf, vf are u, v with the taps of
+ *   every depth reversed (uf[d][k] = u[d][Mz-1-k]); Mz and My must be odd.
+ * Both take flc_xrf_workspace_bytes(...) of scratch (256-byte aligned).
+ * Counterpart: the reference differentiates only the projector in C
+ * (FL/cuda_lib/autograd.py:5-77) with attenuation held fixed
+ * (FL/example/demo.py:413-475); this is the full-mu extension of that path.
+ * --------------------------------------------------------------------- */
+FLC_API size_t flc_xrf_workspace_bytes(int64_t n_ch, int64_t S, int64_t H, int64_t W, int64_t A,
+                                       int64_t L, int64_t chunk);
+FLC_API int flc_xrf_project(const float* frac, const float* theta, const float* coef_x,
+                            const float* coef_f, const float* u, const float* v, const float* em,
+                            float* Pf, int64_t n_ch, int64_t S, int64_t H, int64_t W, int64_t A,
+                            int64_t L, int64_t Mz, int64_t Mx, int64_t My, int incident_mode,
+                            int64_t chunk, void* workspace, size_t workspace_bytes, void* stream);
+FLC_API int flc_xrf_project_adjoint(const float* frac, const float* theta, const float* coef_x,
+                                    const float* coef_f, const float* u, const float* v,
+                                    const float* uf, const float* vf, const float* em,
+                                    const float* gPf, float* dC, int64_t n_ch, int64_t S,
+                                    int64_t H, int64_t W, int64_t A, int64_t L, int64_t Mz,
+                                    int64_t Mx, int64_t My, int incident_mode, int64_t chunk,
+                                    void* workspace, size_t workspace_bytes, void* stream);
 
 /* Rotation with torch grid_sample semantics (bilinear, zero padding,
  * align_corners=False, same-size output): out (N, H, W) from x (N, H, W).

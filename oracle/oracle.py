@@ -225,3 +225,102 @@ def cone_beam_slab(mu, mask, z0, z1):
     lib().orc_cone_beam_slab(_pd(mu), _pd(mask), _pd(out), _i64(K), _i64(Z), _i64(H), _i64(W),
                              _i64(Mz), _i64(Mx), _i64(My), _i64(z0), _i64(z1))
     return out
+
+
+# ---------------------------------------------------------------------------
+# Differentiable corrected projection (per-angle attenuation recomputed from
+# the concentrations).  Forward: the composition FL/core.py:19-101 (rotate ->
+# mu -> incident scan, cone) followed by the projector
+# (atten_cuda_kernel.cu:298-337).  Adjoint: reverse mode of the same chain,
+# composed from the adjoints above; pinned by finite differences in
+# tests/test_oracle_adjoint.py (the reference has no such adjoint).
+# ---------------------------------------------------------------------------
+INCIDENT = {"own": 0, "all": 1, "none": 2}
+
+
+def _xrf_angle(frac, theta, cx, cf, mask, incident):
+    """Rotated fractions, incident term (L,S,H,W), exp(-cone) (L,S,H,W)."""
+    L = cf.shape[0]
+    fr = rotate(frac, theta)
+    mux = fr * _d(cx)[:, None, None, None]
+    muf = np.einsum("ij,jshw->ishw", _d(cf), fr)
+    E = np.exp(-cone_beam(muf, mask))
+    if incident == "own":
+        inc = incident_scan(mux[:L])
+    elif incident == "all":
+        inc = np.repeat(incident_scan(1 - np.prod(1 - mux, axis=0, keepdims=True)), L, axis=0)
+    else:
+        inc = np.ones_like(E)
+    return fr, mux, inc, E
+
+
+def xrf_project(frac, theta, cx, cf, mask, em, incident="own"):
+    """Pf (L, A, S, W) of C = frac[:L] through the attenuation of every angle.
+
+    frac (n_ch,S,H,W); theta (A,) float32 radians; cx (A,n_ch); cf (A,L,n_ch);
+    mask (Mz,Mx,My); em (L,A)."""
+    frac = _d(frac)
+    th = np.asarray(theta, np.float32)
+    A = th.size
+    L = np.shape(cf)[1]
+    n_ch, S, H, W = frac.shape
+    em = _d(em)
+    Pf = np.zeros((L, A, S, W))
+    for a in range(A):
+        _, _, inc, E = _xrf_angle(frac, th[a], np.asarray(cx)[a], np.asarray(cf)[a], mask, incident)
+        att = inc * E
+        for l in range(L):
+            Pf[l, a] = fwd_emission(att[l:l + 1], frac[l:l + 1], em[l, a].reshape(1, 1),
+                                    th[a:a + 1])[0]
+    return Pf
+
+
+def _scan_adjoint(f, inc, dinc):
+    """Reverse mode of inc[h-1] = f[h] * inc[h] (inc[H-1] = 1) along axis -2:
+    returns d/df."""
+    H = f.shape[-2]
+    df = np.zeros_like(f)
+    gbar = dinc[..., 0, :].copy()
+    for h in range(1, H):
+        df[..., h, :] = gbar * inc[..., h, :]
+        gbar = dinc[..., h, :] + gbar * f[..., h, :]
+    return df
+
+
+def xrf_project_adjoint(frac, theta, cx, cf, mask, em, gPf, incident="own"):
+    """dC (L, S, H, W) = d<gPf, xrf_project(frac)>/d frac[:L] (channels >= L
+    are held fixed), through both the projector and the attenuation."""
+    frac = _d(frac)
+    th = np.asarray(theta, np.float32)
+    A = th.size
+    cx = np.asarray(cx)
+    cf = np.asarray(cf)
+    L = cf.shape[1]
+    n_ch, S, H, W = frac.shape
+    em = _d(em)
+    gPf = _d(gPf)
+    dC = np.zeros((L, S, H, W))
+    for a in range(A):
+        fr, mux, inc, E = _xrf_angle(frac, th[a], cx[a], cf[a], mask, incident)
+        att = inc * E
+        datt = np.zeros_like(att)
+        for l in range(L):
+            ema = em[l, a].reshape(1, 1)
+            dC[l] += bwd_emission(att[l:l + 1], gPf[l, a][None], ema, th[a:a + 1])[0]
+            datt[l] = fwd_emission_datten(gPf[l, a][None], frac[l:l + 1], ema, th[a:a + 1])[0]
+        dinc = datt * E
+        dres = -datt * att
+        dmuf = cone_beam_adjoint(dres, mask)
+        dmux = np.zeros_like(mux)
+        if incident == "own":
+            dmux[:L] = -_scan_adjoint(1 - mux[:L], inc, dinc)
+        elif incident == "all":
+            f = 1 - mux
+            ftot = np.prod(f, axis=0, keepdims=True)
+            dftot = _scan_adjoint(ftot, inc[:1], dinc.sum(axis=0, keepdims=True))
+            for j in range(n_ch):
+                others = np.prod(np.delete(f, j, axis=0), axis=0)
+                dmux[j] = -dftot[0] * others
+        dfr = dmux * cx[a][:, None, None, None] + np.einsum("ij,ishw->jshw", cf[a].astype(np.float64), dmuf)
+        dC += rotate_adjoint(dfr[:L], th[a])
+    return dC

@@ -86,3 +86,32 @@ def test_cpu_tensors_fail_loudly():
         atten_cuda.cal_atten_cuda(x, torch.zeros(3, 3, 3))
     with pytest.raises(RuntimeError, match="CUDA"):
         atten_cuda.forward_emission_batch(x, x, torch.ones(2, 2), torch.zeros(2))
+
+
+def test_tuning_knobs_round_trip():
+    lib = _lib.load()
+    for name in (b"proj.cluster", b"proj.apc", b"cone.variant", b"atten.chunk"):
+        old = lib.flc_tune_get(name)
+        assert old >= 0
+        assert lib.flc_tune_set(name, 3) == 0
+        assert lib.flc_tune_get(name) == 3
+        assert lib.flc_tune_set(name, old) == 0
+    assert lib.flc_tune_get(b"no.such.knob") == -1
+    assert lib.flc_tune_set(b"no.such.knob", 1) == 1
+    assert b"unknown knob" in lib.flc_last_error()
+    assert lib.flc_tune_set(b"proj.cluster", -1) == 1
+
+
+def test_xrf_argument_checks():
+    lib = _lib.load()
+    p = ctypes.c_void_p(256)
+    assert lib.flc_xrf_workspace_bytes(3, 4, 16, 16, 10, 2, 0) > 0
+    assert lib.flc_xrf_workspace_bytes(3, 4, 16, 16, 10, 2, 2) < lib.flc_xrf_workspace_bytes(
+        3, 4, 16, 16, 10, 2, 10)
+    # even cone extent in slices is rejected before anything runs
+    assert lib.flc_xrf_project(p, p, p, p, p, p, p, p, 3, 4, 16, 16, 10, 2, 4, 16, 3, 0, 0, p,
+                               1 << 30, None) == 1
+    assert lib.flc_xrf_project(p, p, p, p, p, p, p, p, 3, 4, 16, 12, 10, 2, 3, 16, 3, 0, 0, p,
+                               1 << 30, None) == 1                      # H != W
+    assert lib.flc_xrf_project_adjoint(p, p, p, p, p, p, p, p, p, None, p, 3, 4, 16, 16, 10, 2,
+                                       3, 16, 3, 0, 0, p, 1 << 30, None) == 1

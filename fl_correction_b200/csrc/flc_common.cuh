@@ -32,7 +32,7 @@ inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s
 
 // Launch-shape knobs (set by the autotuner through flc_tune_set; 0 = auto).
 enum TuneKey {
-    kTuneProjCluster = 0,   // max CTAs per slice cluster for the backward / MLEM kernels
+    kTuneProjCluster = 0,   // CTAs per slice cluster for the backward / MLEM kernels
     kTuneProjApc = 1,       // angles per CTA for the projector kernels
     kTuneConeVariant = 2,   // 1: TMA 16x8 tile, 2: TMA 8x4 tile, 3: plain kernel
     kTuneAttenChunk = 3,    // angles per attenuation-pipeline pass

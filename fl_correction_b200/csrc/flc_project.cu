@@ -16,16 +16,22 @@
 //  * the backward splats the exact transpose into a shared-memory image of the
 //    slice in nine phases: samples whose (h, w) agree modulo 3 sit >= 3 apart
 //    on the rotated lattice, so their 2x2 footprints are disjoint and plain
-//    read-modify-writes cannot race.  Only the border frame (rows 0, H-2, H-1,
-//    columns 0, W-2, W-1), where samples clamped to the edge pile up, takes
-//    shared atomics; samples clamped in both coordinates all land on one of
-//    the four corners and are summed in registers, then flushed once;
+//    read-modify-writes cannot race.  Samples clamped to the edge (they land
+//    only on the border frame: rows 0, H-2, H-1, columns 0, W-2, W-1) go with
+//    shared atomics into separate frame buffers, folded into the image after
+//    the last angle; samples clamped in both coordinates all land on one of
+//    the four corners and are summed in registers.  Every lane of a warp runs
+//    the same code for unclamped samples (no divergent border path), and
+//    each thread issues two footprints' loads before their stores;
 //  * the CTAs of one slice form a thread-block cluster and reduce their images
 //    through distributed shared memory in rank order;
 //  * one MLEM iteration (forward, ratio, backward, Huber, update, clamp) is a
 //    single cluster launch that reads each atten tile from HBM once.
 
 #include <cooperative_groups.h>
+
+#include <mutex>
+#include <vector>
 
 #include "flc_common.cuh"
 #include "flc_geom.cuh"
@@ -173,105 +179,166 @@ struct Corners {
     }
 };
 
-// Adds v, spread over the pixels of corner class k, into img with atomics.
-// Clamped coordinate 0 -> index 0 with weight 1; rmax -> indices ih, ih+1 with
-// weights 1-fxh, fxh (atten_cuda_kernel.cu:116-133).
-__device__ __forceinline__ void corner_add(float* img, int pitch, const Geo& g, int k, float v) {
+// Samples clamped to the image border (atten_cuda_kernel.cu:116-133) land
+// only on the border frame: a row clamp on row 0 (x < 0, weight 1) or rows
+// ih = H-2, ih+1 (x > rmax, weights 1-fxh, fxh); a column clamp likewise on
+// columns 0 or W-2, W-1.  They are collected, with shared atomics, in frame
+// buffers kept apart from the slice image so that the unclamped samples can
+// update the image with plain read-modify-writes:
+//   srow[r][slot][j], slot 0: row 0, 1: row H-2, 2: row H-1   (R x 3 x W)
+//   scol[r][slot][i], slot 0: col 0, 1: col W-2, 2: col W-1   (R x 3 x H)
+// and added into the image once, after the last angle (fold_frame).
+
+// Adds v, spread over the pixels of corner class k (2*xhigh + yhigh), into
+// the row buffer of one reference.
+__device__ __forceinline__ void corner_add(float* srow, int W, const Geo& g, int k, float v) {
     const bool xh = k >= 2, yh = k & 1;
-    const int i0 = xh ? g.ih : 0, j0 = yh ? g.jh : 0;
-    const float fx = xh ? g.fxh : 0.f, fy = yh ? g.fyh : 0.f;
-    const float wr[2] = {1.f - fx, fx}, wc[2] = {1.f - fy, fy};
-#pragma unroll
-    for (int a = 0; a < 2; ++a)
-#pragma unroll
-        for (int b = 0; b < 2; ++b) {
-            const float wgt = wc[b] * wr[a];
-            if (wgt != 0.f) atomicAdd(img + (i0 + a) * pitch + j0 + b, v * wgt);
-        }
+    const int j0 = yh ? g.jh : 0;
+    const float fy = yh ? g.fyh : 0.f;
+    const float c0 = v * (1.f - fy), c1 = v * fy;
+    if (!xh) {
+        atomicAdd(srow + j0, c0);
+        if (c1 != 0.f) atomicAdd(srow + j0 + 1, c1);
+        return;
+    }
+    const float r0 = 1.f - g.fxh, r1 = g.fxh;
+    atomicAdd(srow + W + j0, c0 * r0);
+    atomicAdd(srow + 2 * W + j0, c0 * r1);
+    if (c1 != 0.f) {
+        atomicAdd(srow + W + j0 + 1, c1 * r0);
+        atomicAdd(srow + 2 * W + j0 + 1, c1 * r1);
+    }
 }
 
-__device__ __forceinline__ bool in_frame(int i, int j, int H, int W) {
-    return i == 0 || i >= H - 2 || j == 0 || j >= W - 2;
+// Bilinear footprint of one sample on the clamped grid.
+struct Foot {
+    int off;                 // i0 * pitch + j0
+    int i0, j0;
+    float w00, w01, w10, w11;
+    float av;                // atten * ratio
+    int kind;                // bits: 1 x < 0, 2 x > rmax, 4 y < 0, 8 y > cmax
+};
+
+__device__ __forceinline__ Foot footprint(const Geo& g, const float* sA, const float* sratio,
+                                          int W, int pitch, int h, int w) {
+    Foot f;
+    f.av = sA[h * W + w] * sratio[w];
+    const float hf = (float)h - g.cy;
+    const float x = fmaf(g.c, hf, col_bx(g, w)), y = fmaf(g.s, hf, col_by(g, w));
+    const float xc = fminf(fmaxf(x, 0.f), g.rmax), yc = fminf(fmaxf(y, 0.f), g.cmax);
+    float fx, fy;
+    f.i0 = ffloor(xc, fx);
+    f.j0 = ffloor(yc, fy);
+    f.off = f.i0 * pitch + f.j0;
+    f.w00 = (1.f - fy) * (1.f - fx);
+    f.w01 = fy * (1.f - fx);
+    f.w10 = (1.f - fy) * fx;
+    f.w11 = fy * fx;
+    f.kind = (x < 0.f ? 1 : 0) | (x > g.rmax ? 2 : 0) | (y < 0.f ? 4 : 0) | (y > g.cmax ? 8 : 0);
+    return f;
 }
 
-__device__ __forceinline__ void splat1(float* img, int pitch, int i, int j, float v, int H, int W) {
-    if (v == 0.f) return;
-    float* p = img + i * pitch + j;
-    if (in_frame(i, j, H, W))
-        atomicAdd(p, v);
-    else
-        *p += v;
+// Contribution v of a clamped sample of reference r into the frame buffers
+// (or, clamped in both coordinates, r < kCornerR and REG -- the reference
+// count is a compile-time constant -- the corner registers).
+// One form for both buffers: the four taps sit at base + {0, 1, S, S + 1}.
+// A row clamp below 0 has fx == 0 (no weight on the second row) and a column
+// clamp below 0 has fy == 0, so their zero-weight taps are skipped.
+template <bool REG>
+__device__ __forceinline__ void frame_add(const Foot& f, float v, float* srow, float* scol, int H,
+                                          int W, Corners& cs, int r) {
+    const bool rowc = (f.kind & 3) != 0;
+    const bool corner = rowc && (f.kind & 12) != 0;
+    if (REG && corner && r < kCornerR) {
+        cs.add(r, ((f.kind & 2) ? 2 : 0) + ((f.kind & 8) ? 1 : 0), v);
+    } else {
+        float* base = rowc ? srow + r * 3 * W + ((f.kind & 1) ? 0 : W) + f.j0
+                           : scol + r * 3 * H + ((f.kind & 4) ? 0 : H) + f.i0;
+        const int S = rowc ? W : H;
+        const float t1 = rowc ? f.w01 : f.w10, t2 = rowc ? f.w10 : f.w01;
+        if (f.w00 != 0.f) atomicAdd(base, v * f.w00);
+        if (t1 != 0.f) atomicAdd(base + 1, v * t1);
+        if (t2 != 0.f) atomicAdd(base + S, v * t2);
+        if (f.w11 != 0.f) atomicAdd(base + S + 1, v * f.w11);
+    }
 }
 
 // Backward of one (angle, slice): sacc_r += em_r * atten * ratio[w] * bilinear
-// weights, the exact transpose of forward_angle.  Nine phases of disjoint
-// footprints, separated by barriers.
-__device__ void backward_angle(const float* sA, const float* sratio, float* sacc, int img_stride,
-                               int pitch, const float* em_a, int R, const Geo& g, int H, int W,
-                               Corners& cs) {
+// weights, the exact transpose of forward_angle.  Nine phases, separated by
+// barriers: the unclamped samples of a phase have disjoint footprints and
+// update the image with plain read-modify-writes; clamped ones go to the
+// frame buffers.  Each thread takes its items two at a time and issues both
+// footprints' loads before either's stores (legal: they are disjoint), and
+// every lane of a warp runs the same code except for the clamped samples.
+// RC > 0: exactly RC references (unrolled); RC == 0: R at run time.
+template <int RC>
+__device__ void backward_angle(const float* sA, const float* sratio, float* sacc, float* srow,
+                               float* scol, int img_stride, int pitch, const float* em_a, int Rrt,
+                               const Geo& g, int H, int W, Corners& cs) {
+    const int R = RC > 0 ? RC : Rrt;
     const int nthr = blockDim.x;
+    const float tq = (float)threadIdx.x + 0.5f, nq = (float)nthr + 0.5f;
     for (int ph = 0; ph < 3; ++ph) {
         for (int pw = 0; pw < 3; ++pw) {
             const int nh = (H - ph + 2) / 3, nw = (W - pw + 2) / 3;
             // item it = hh * nw + ww walks by nthr: advance (hh, ww) without
-            // division.  A phase can be empty (H or W <= 2): skip to the barrier.
-            const int dh = nw > 0 ? nthr / nw : 0, dw = nthr - dh * nw;
-            int hh = nw > 0 ? threadIdx.x / nw : nh, ww = threadIdx.x - hh * nw;
-            if (nh <= 0 || nw <= 0) hh = nh;
-            for (; hh < nh; hh += dh, ww += dw) {
-                if (ww >= nw) { ww -= nw; ++hh; if (hh >= nh) break; }
-                const int h = ph + 3 * hh, w = pw + 3 * ww;
-                const float av = sA[h * W + w] * sratio[w];
-                const float hf = (float)h - g.cy;
-                const float x = fmaf(g.c, hf, col_bx(g, w)), y = fmaf(g.s, hf, col_by(g, w));
-                if (x >= 1.f && x < (float)(H - 3) && y >= 1.f && y < (float)(W - 3)) {
-                    // interior: unclamped, footprint outside the border frame
-                    float fx, fy;
-                    const int i0 = ffloor(x, fx), j0 = ffloor(y, fy);
-                    const float w00 = (1.f - fy) * (1.f - fx), w01 = fy * (1.f - fx);
-                    const float w10 = (1.f - fy) * fx, w11 = fy * fx;
-                    for (int r = 0; r < R; ++r) {
-                        const float v = em_a[r] * av;
-                        float* p = sacc + r * img_stride + i0 * pitch + j0;
-                        p[0] += v * w00;
-                        p[1] += v * w01;
-                        p[pitch] += v * w10;
-                        p[pitch + 1] += v * w11;
-                    }
-                    continue;
-                }
-                const Smp s = sample_xy(g, x, y);
-                const bool xl = s.x <= 0.f, xh = s.x >= g.rmax;
-                const bool yl = s.y <= 0.f, yh = s.y >= g.cmax;
-                if ((xl || xh) && (yl || yh)) {
-                    const int k = (xh ? 2 : 0) + (yh ? 1 : 0);
-                    for (int r = 0; r < R; ++r) {
-                        if (r < kCornerR) cs.add(r, k, em_a[r] * av);
-                        else corner_add(sacc + r * img_stride, pitch, g, k, em_a[r] * av);
-                    }
-                    continue;
-                }
-                const float w00 = (1.f - s.fy) * (1.f - s.fx), w01 = s.fy * (1.f - s.fx);
-                const float w10 = (1.f - s.fy) * s.fx, w11 = s.fy * s.fx;
-                for (int r = 0; r < R; ++r) {
-                    const float v = em_a[r] * av;
+            // division.  floor((t + 1/2) / nw) in FP32 is exact for t < 2^22
+            // (the quotient stays >= 1/(2 nw) from an integer).  A phase can be
+            // empty (H or W <= 2): skip to the barrier.
+            int hh = nh, ww = 0, dh = 0, dw = 0;
+            if (nh > 0 && nw > 0) {
+                const float inv = 1.f / (float)nw;
+                hh = (int)(tq * inv);
+                ww = (int)threadIdx.x - hh * nw;
+                dh = (int)(nq * inv);
+                dw = nthr - dh * nw;
+            }
+            while (hh < nh) {
+                int hb = hh + dh, wb = ww + dw;
+                if (wb >= nw) { wb -= nw; ++hb; }
+                const bool has_b = hb < nh;
+                const Foot fa = footprint(g, sA, sratio, W, pitch, ph + 3 * hh, pw + 3 * ww);
+                const Foot fb = footprint(g, sA, sratio, W, pitch, has_b ? ph + 3 * hb : ph,
+                                          has_b ? pw + 3 * wb : pw);
+                const bool pa = fa.kind == 0, pb = has_b && fb.kind == 0;
+#pragma unroll
+                for (int r = 0; r < (RC > 0 ? RC : R); ++r) {
+                    const float em = em_a[r];
                     float* img = sacc + r * img_stride;
-                    splat1(img, pitch, s.i0, s.j0, v * w00, H, W);
-                    splat1(img, pitch, s.i0, s.j0 + 1, v * w01, H, W);
-                    splat1(img, pitch, s.i0 + 1, s.j0, v * w10, H, W);
-                    splat1(img, pitch, s.i0 + 1, s.j0 + 1, v * w11, H, W);
+                    float* qa = img + fa.off;
+                    float* qb = img + fb.off;
+                    float a00 = 0.f, a01 = 0.f, a10 = 0.f, a11 = 0.f;
+                    float b00 = 0.f, b01 = 0.f, b10 = 0.f, b11 = 0.f;
+                    if (pa) { a00 = qa[0]; a01 = qa[1]; a10 = qa[pitch]; a11 = qa[pitch + 1]; }
+                    if (pb) { b00 = qb[0]; b01 = qb[1]; b10 = qb[pitch]; b11 = qb[pitch + 1]; }
+                    const float va = em * fa.av, vb = em * fb.av;
+                    if (pa) {
+                        qa[0] = fmaf(va, fa.w00, a00);
+                        qa[1] = fmaf(va, fa.w01, a01);
+                        qa[pitch] = fmaf(va, fa.w10, a10);
+                        qa[pitch + 1] = fmaf(va, fa.w11, a11);
+                    }
+                    if (pb) {
+                        qb[0] = fmaf(vb, fb.w00, b00);
+                        qb[1] = fmaf(vb, fb.w01, b01);
+                        qb[pitch] = fmaf(vb, fb.w10, b10);
+                        qb[pitch + 1] = fmaf(vb, fb.w11, b11);
+                    }
+                    if (!pa) frame_add<(RC > 0)>(fa, va, srow, scol, H, W, cs, r);
+                    if (has_b && !pb) frame_add<(RC > 0)>(fb, vb, srow, scol, H, W, cs, r);
                 }
+                hh = hb + dh;
+                ww = wb + dw;
+                if (ww >= nw) { ww -= nw; ++hh; }
             }
             __syncthreads();
         }
     }
 }
 
-// Adds the register corner sums into the image: warp-reduce, then one atomic
-// per warp and pixel.  The weights are those of the clamped coordinates
-// (0 -> row/col 0 with weight 1; rmax -> rows ih, ih+1 with 1-fxh, fxh).
-__device__ void flush_corners(Corners& cs, float* sacc, int img_stride, int pitch, const Geo& g,
-                              int R, int H, int W) {
+// Adds the register corner sums into the row buffers: warp-reduce, then one
+// atomic per warp and pixel.
+__device__ void flush_corners(Corners& cs, float* srow, const Geo& g, int R, int W) {
     const int lane = threadIdx.x & 31;
 #pragma unroll
     for (int r = 0; r < kCornerR; ++r) {
@@ -280,9 +347,39 @@ __device__ void flush_corners(Corners& cs, float* sacc, int img_stride, int pitc
             float v = cs.v[r][k];
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if (r < R && lane == 0 && v != 0.f) corner_add(sacc + r * img_stride, pitch, g, k, v);
+            if (r < R && lane == 0 && v != 0.f) corner_add(srow + r * 3 * W, W, g, k, v);
         }
     }
+}
+
+// After the last angle: corners into the row buffers, then the row and column
+// buffers into the image (one thread per column / row, slots in order, so a
+// coinciding row or column -- H or W == 2 -- is still summed correctly).
+__device__ void fold_frame(Corners& cs, float* sacc, float* srow, const float* scol,
+                           int img_stride, int pitch, int R, int H, int W) {
+    // every thread passes the barriers below (callers have finished all angles)
+    __syncthreads();
+    const Geo g0 = make_geo(0.f, H, W);
+    flush_corners(cs, srow, g0, R, W);
+    __syncthreads();
+    for (int t = threadIdx.x; t < R * W; t += blockDim.x) {
+        const int r = t / W, j = t - r * W;
+        float* img = sacc + r * img_stride + j;
+        const float* b = srow + r * 3 * W + j;
+        img[0] += b[0];
+        img[(H - 2) * pitch] += b[W];
+        img[(H - 1) * pitch] += b[2 * W];
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < R * H; t += blockDim.x) {
+        const int r = t / H, i = t - r * H;
+        float* img = sacc + r * img_stride + i * pitch;
+        const float* b = scol + r * 3 * H + i;
+        img[0] += b[0];
+        img[W - 2] += b[H];
+        img[W - 1] += b[2 * H];
+    }
+    __syncthreads();
 }
 
 // ---------------------------------------------------------------------------
@@ -361,6 +458,7 @@ __device__ void cluster_reduce(cg::cluster_group& cluster, float* sacc, int R, i
 // splats angles [g*apc, (g+1)*apc).  ratio == nullptr means ratio = 1
 // (sensitivity); clamp_min > 0 applies max(out, clamp_min).
 // ---------------------------------------------------------------------------
+template <int RC>
 __global__ void __launch_bounds__(kThreads, 1)
 proj_bwd_kernel(const float* __restrict__ atten, const float* __restrict__ ratio,
                 const float* __restrict__ em, const float* __restrict__ theta,
@@ -375,10 +473,12 @@ proj_bwd_kernel(const float* __restrict__ atten, const float* __restrict__ ratio
     const int img_stride = H * pitch;
     float* sA = smem;
     float* sacc = sA + (stage_tile ? ((HW + 3) & ~3) : 0);
-    float* sratio = sacc + R * img_stride;
+    float* srow = sacc + R * img_stride;                     // [R][3][W]
+    float* scol = srow + R * 3 * W;                          // [R][3][H]
+    float* sratio = scol + R * 3 * H;
     float* sem = sratio + W;
     const bool vec = stage_tile && ((HW & 3) == 0) && (((uintptr_t)atten & 15) == 0);
-    for (int i = threadIdx.x; i < R * img_stride; i += blockDim.x) sacc[i] = 0.f;
+    for (int i = threadIdx.x; i < R * (img_stride + 3 * W + 3 * H); i += blockDim.x) sacc[i] = 0.f;
     Corners cs;
     cs.zero();
     TileRegs tr;
@@ -393,10 +493,10 @@ proj_bwd_kernel(const float* __restrict__ atten, const float* __restrict__ ratio
             sratio[w] = ratio ? ratio[((int64_t)a * B + b) * W + w] : 1.f;
         __syncthreads();
         if (a + 1 < a1 && vec) tile_issue(tr, atten + ((int64_t)(a + 1) * B + b) * HW, HW);
-        backward_angle(stage_tile ? sA : src, sratio, sacc, img_stride, pitch, sem, R,
-                       make_geo(theta[a], H, W), H, W, cs);
+        backward_angle<RC>(stage_tile ? sA : src, sratio, sacc, srow, scol, img_stride, pitch, sem,
+                       R, make_geo(theta[a], H, W), H, W, cs);
     }
-    flush_corners(cs, sacc, img_stride, pitch, make_geo(0.f, H, W), R, H, W);
+    fold_frame(cs, sacc, srow, scol, img_stride, pitch, R, H, W);
     cluster.sync();
     cluster_reduce(cluster, sacc, R, H, W, pitch, [&](int r, int h, int w, float s) {
         if (clamp_min > 0.f) s = fmaxf(s, clamp_min);
@@ -412,6 +512,7 @@ proj_bwd_kernel(const float* __restrict__ atten, const float* __restrict__ ratio
 // as atten_cuda.cpp:321-342.  Reads C from Cin, writes Cout (ping-pong: the
 // Huber term needs the old neighbours).
 // ---------------------------------------------------------------------------
+template <int RC>
 __global__ void __launch_bounds__(kThreads, 1)
 mlem_iter_kernel(const float* __restrict__ atten, const float* __restrict__ em,
                  const float* __restrict__ theta, const float* __restrict__ I,
@@ -429,12 +530,14 @@ mlem_iter_kernel(const float* __restrict__ atten, const float* __restrict__ em,
     float* sA = smem;
     float* sC = sA + ((HW + 3) & ~3);
     float* sacc = sC + R * img_stride;
-    float* spart = sacc + R * img_stride;
+    float* srow = sacc + R * img_stride;                     // [R][3][W]
+    float* scol = srow + R * 3 * W;                          // [R][3][H]
+    float* spart = scol + R * 3 * H;
     float* sratio = spart + parts * W;
     float* sem = sratio + W;
     const bool vec = ((HW & 3) == 0) && (((uintptr_t)atten & 15) == 0);
     stage_slice(sC, Cin, R, B, b, H, W, pitch);
-    for (int i = threadIdx.x; i < R * img_stride; i += blockDim.x) sacc[i] = 0.f;
+    for (int i = threadIdx.x; i < R * (img_stride + 3 * W + 3 * H); i += blockDim.x) sacc[i] = 0.f;
     Corners cs;
     cs.zero();
     TileRegs tr;
@@ -455,9 +558,9 @@ mlem_iter_kernel(const float* __restrict__ atten, const float* __restrict__ em,
             sratio[w] = I[((int64_t)a * B + b) * W + w] / fmaxf(s, 1e-6f);
         }
         __syncthreads();
-        backward_angle(sA, sratio, sacc, img_stride, pitch, sem, R, g, H, W, cs);
+        backward_angle<RC>(sA, sratio, sacc, srow, scol, img_stride, pitch, sem, R, g, H, W, cs);
     }
-    flush_corners(cs, sacc, img_stride, pitch, make_geo(0.f, H, W), R, H, W);
+    fold_frame(cs, sacc, srow, scol, img_stride, pitch, R, H, W);
     cluster.sync();
     cluster_reduce(cluster, sacc, R, H, W, pitch, [&](int r, int h, int w, float back) {
         const float* img = sC + r * img_stride;
@@ -550,22 +653,72 @@ int check_proj_sizes(int64_t A, int64_t B, int64_t R, int64_t H, int64_t W) {
     return FLC_OK;
 }
 
-// Splits A angles into G groups so that G*B CTAs cover the SMs a few times.
-Plan plan_cluster(int64_t A, int64_t B, size_t smem_per_cta) {
+// Clusters of G CTAs of fn (kThreads threads, smem bytes each) that can be
+// resident at once on the current device; 0 if G is not launchable.  Cached.
+int active_clusters(const void* fn, int G, size_t smem) {
+    struct Entry {
+        const void* fn;
+        int dev, G;
+        size_t smem;
+        int n;
+    };
+    static std::mutex mu;
+    static std::vector<Entry> cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        for (const Entry& e : cache)
+            if (e.fn == fn && e.dev == dev && e.G == G && e.smem == smem) return e.n;
+    }
+    int n = 0;
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) ==
+            cudaSuccess &&
+        cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(G);
+        cfg.blockDim = dim3(kThreads);
+        cfg.dynamicSmemBytes = smem;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = G;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        if (cudaOccupancyMaxActiveClusters(&n, fn, &cfg) != cudaSuccess) n = 0;
+    }
+    (void)cudaGetLastError();  // a refused size is an answer, not a pending error
+    std::lock_guard<std::mutex> lk(mu);
+    cache.push_back({fn, dev, G, smem, n});
+    return n;
+}
+
+// Cluster size G (CTAs per slice, each taking ceil(A/G) angles) minimising
+// waves * (angles per CTA + 2): the B clusters run in ceil(B / resident)
+// waves, and each CTA pays about two angles' worth of staging and reduction.
+// The "proj.cluster" knob forces G.
+Plan plan_cluster(const void* fn, int64_t A, int64_t B, size_t smem_per_cta) {
     Plan p;
-    int sms = sm_count();
-    int per_sm = (int)(max_smem_optin() / (smem_per_cta + 1024));
-    if (per_sm < 1) per_sm = 1;
-    int64_t want = 2LL * sms * per_sm;
-    int G = (int)ceil_div(want, B);
-    int gmax = kMaxCluster;
-    if (int64_t t = tune(kTuneProjCluster)) gmax = (int)(t < kMaxCluster ? t : kMaxCluster);
-    if (G > gmax) G = gmax;
-    if (G > A) G = (int)A;
-    if (G < 1) G = 1;
-    p.apc = (int)ceil_div(A, G);
-    p.G = (int)ceil_div(A, p.apc);
     p.smem = smem_per_cta;
+    int gmax = kMaxCluster < A ? kMaxCluster : (int)A;
+    int best_g = 1;
+    if (int64_t t = tune(kTuneProjCluster)) {
+        best_g = (int)(t < gmax ? t : gmax);
+    } else {
+        int64_t best = -1;
+        for (int G = 1; G <= gmax; ++G) {
+            const int n = active_clusters(fn, G, smem_per_cta);
+            if (n < 1) continue;
+            const int64_t cost = ceil_div(B, n) * (ceil_div(A, G) + 2);
+            if (best < 0 || cost < best) {
+                best = cost;
+                best_g = G;
+            }
+        }
+    }
+    p.apc = (int)ceil_div(A, best_g);
+    p.G = (int)ceil_div(A, p.apc);
     return p;
 }
 
@@ -598,14 +751,14 @@ size_t fwd_smem(int64_t R, int64_t H, int64_t W, bool stage_tile, bool stage_c) 
 }
 
 size_t bwd_smem(int64_t R, int64_t H, int64_t W, bool stage_tile) {
-    return sizeof(float) *
-           ((stage_tile ? tile_floats(H, W) : 0) + R * H * slice_pitch((int)W) + W + kMaxR);
+    return sizeof(float) * ((stage_tile ? tile_floats(H, W) : 0) + R * H * slice_pitch((int)W) +
+                            R * 3 * (H + W) + W + kMaxR);
 }
 
 size_t mlem_smem(int64_t R, int64_t H, int64_t W) {
     int parts = col_parts((int)W, (int)H);
-    return sizeof(float) *
-           (tile_floats(H, W) + 2 * R * H * slice_pitch((int)W) + parts * W + W + kMaxR);
+    return sizeof(float) * (tile_floats(H, W) + 2 * R * H * slice_pitch((int)W) +
+                            R * 3 * (H + W) + parts * W + W + kMaxR);
 }
 
 }  // namespace
@@ -631,11 +784,12 @@ int bwd_emission_launch(const float* atten, const float* ratio, const float* em,
         return FLC_OK;
     }
     size_t smem = bwd_smem(R, H, W, stage_tile);
-    Plan p = plan_cluster(A, B, smem);
+    const void* fn = R == 1 ? (const void*)proj_bwd_kernel<1> : (const void*)proj_bwd_kernel<0>;
+    Plan p = plan_cluster(fn, A, B, smem);
     int iA = (int)A, iB = (int)B, iR = (int)R, iH = (int)H, iW = (int)W, apc = p.apc;
     void* args[] = {(void*)&atten, (void*)&ratio, (void*)&em, (void*)&theta, (void*)&out,
                     &iA, &iB, &iR, &iH, &iW, &apc, &clamp_min, &stage_tile};
-    return launch_cluster((const void*)proj_bwd_kernel, dim3(p.G, (unsigned)B), p.G, smem, st, args);
+    return launch_cluster(fn, dim3(p.G, (unsigned)B), p.G, smem, st, args);
 }
 
 int fwd_emission_launch(const float* atten, const float* C, const float* em, const float* theta,
@@ -671,11 +825,21 @@ int mlem_iter_launch(const float* atten, const float* em, const float* theta, co
     size_t smem = mlem_smem(R, H, W);
     *fused = smem <= (size_t)max_smem_optin();
     if (!*fused) return FLC_OK;
-    Plan p = plan_cluster(A, B, smem);
+    const void* fn = R == 1 ? (const void*)mlem_iter_kernel<1> : (const void*)mlem_iter_kernel<0>;
+    Plan p = plan_cluster(fn, A, B, smem);
     int iA = (int)A, iB = (int)B, iR = (int)R, iH = (int)H, iW = (int)W, apc = p.apc;
     void* args[] = {(void*)&atten, (void*)&em, (void*)&theta, (void*)&I, (void*)&sens,
                     (void*)&Cin, (void*)&Cout, &iA, &iB, &iR, &iH, &iW, &apc, &beta, &delta};
-    return launch_cluster((const void*)mlem_iter_kernel, dim3(p.G, (unsigned)B), p.G, smem, st, args);
+    return launch_cluster(fn, dim3(p.G, (unsigned)B), p.G, smem, st, args);
+}
+
+// Computes (and caches) the launch plan of the fused iteration, so that a
+// later stream capture makes no occupancy queries.
+void mlem_iter_prepare(int64_t A, int64_t B, int64_t R, int64_t H, int64_t W) {
+    const size_t smem = mlem_smem(R, H, W);
+    if (smem > (size_t)max_smem_optin()) return;
+    const void* fn = R == 1 ? (const void*)mlem_iter_kernel<1> : (const void*)mlem_iter_kernel<0>;
+    (void)plan_cluster(fn, A, B, smem);
 }
 
 int huber_launch(const float* C, float* grad, int64_t RB, int64_t H, int64_t W, float delta,

@@ -94,6 +94,7 @@ int mlem_iter_launch(const float* atten, const float* em, const float* theta, co
                      const float* sens, const float* Cin, float* Cout, int64_t A, int64_t B,
                      int64_t R, int64_t H, int64_t W, float beta, float delta, cudaStream_t st,
                      bool* fused);
+void mlem_iter_prepare(int64_t A, int64_t B, int64_t R, int64_t H, int64_t W);
 
 namespace {
 
@@ -237,6 +238,7 @@ extern "C" int flc_mlem(float* C, const float* atten, const float* em, const flo
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int status = FLC_OK;
+    mlem_iter_prepare(A, B, R, H, W);
     FLC_TRY_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
     do {
         const uint64_t before = launches();

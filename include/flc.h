@@ -58,7 +58,7 @@ FLC_API int flc_device_status(int reset);
 FLC_API uint64_t flc_launch_count(void);
 /* Launch-shape knobs of this library (no counterpart in the reference; the
  * autotuner in fl_correction_b200/tune.py sets them).  Names:
- *   "proj.cluster"  max CTAs per slice cluster, backward/MLEM kernels (1..8)
+ *   "proj.cluster"  CTAs per slice cluster, backward/MLEM kernels (1..8)
  *   "proj.apc"      angles per CTA, projector kernels
  *   "cone.variant"  1: TMA 16x8 tile, 2: TMA 8x4 tile, 3: plain kernel
  *   "atten.chunk"   angles per attenuation-pipeline pass

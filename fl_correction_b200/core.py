@@ -108,9 +108,10 @@ def atten_maps(frac_4D, angle_list, coef_x, coef_f, mask_uv=None, incident="own"
 
 def pick_chunk(S, H, W, A, L, chunk=0):
     """Angles per pass of the attenuation pipeline (the native default when 0):
-    about 64 MB of staged fluorescence mu, so a chunk stays L2-resident."""
+    about 256 MB of staged fluorescence mu, enough cone tiles per launch that
+    the last wave of CTAs is a small fraction of the launch."""
     if chunk <= 0:
-        chunk = max(1, (64 << 20) // (L * S * H * W * 4))
+        chunk = max(1, (256 << 20) // (L * S * H * W * 4))
     chunk = min(chunk, A)
     return max(1, min(chunk, 65535 // L))
 

@@ -479,7 +479,7 @@ int64_t pick_chunk(int64_t S, int64_t H, int64_t W, int64_t A, int64_t L, int64_
     if (chunk <= 0) chunk = tune(kTuneAttenChunk);
     if (chunk <= 0) {
         int64_t vol = L * S * H * W * (int64_t)sizeof(float);
-        chunk = (64LL << 20) / (vol > 0 ? vol : 1);
+        chunk = (256LL << 20) / (vol > 0 ? vol : 1);
         if (chunk < 1) chunk = 1;
     }
     if (chunk > A) chunk = A;

@@ -12,10 +12,11 @@
 // double buffer and waits for it on an mbarrier (bounded wait).  For every
 // target the plane feeds (d = p - x), the y filter runs row by row from the
 // staged plane into a z-major scratch X, and the z filter accumulates column
-// by column into registers.  Both filters keep a sliding window of the input
-// in registers, rotated over blocks of four taps, so each block of 4 taps
-// costs one 128-bit shared load of input, one broadcast load of weights and
-// 32 FMAs.
+// by column into registers.  Both filters keep sliding windows of the input
+// in registers, rotated over blocks of four taps, and run several windows
+// under one weight row: a y-filter thread owns two rows at a time and a
+// z-filter thread 32 consecutive outputs, so a block of four taps costs one
+// broadcast weight load and one 128-bit input load per 32 FMAs.
 //
 // Taps are zero-padded to blocks of four; the reference's zero-skip order of
 // summation is not reproduced (FP32 sums in a different order; the result
@@ -128,6 +129,49 @@ __device__ __forceinline__ void corr8(float (&acc)[8], const float* in, const fl
     }
 }
 
+// NR independent 1-D correlations sharing one weight row: acc[k][t] +=
+// sum_m w[m] * in[k * rs + t + m].  Each block of four taps costs one
+// broadcast weight load and NR input loads for NR x 32 FMAs (the windows
+// slide by one float4 per block).  `rs` is a multiple of 4 floats.
+template <int NR>
+__device__ __forceinline__ void corr8_rows(float (&acc)[NR][8], const float* in, int rs,
+                                           const float* w, int mlo, int mhi) {
+    if (mlo >= mhi) return;
+    float4 g0[NR], g1[NR], g2[NR];
+#pragma unroll
+    for (int k = 0; k < NR; ++k) {
+        g0[k] = *reinterpret_cast<const float4*>(in + k * rs + mlo);
+        g1[k] = *reinterpret_cast<const float4*>(in + k * rs + mlo + 4);
+    }
+    int m = mlo;
+    while (true) {
+        float4 wv = *reinterpret_cast<const float4*>(w + m);
+#pragma unroll
+        for (int k = 0; k < NR; ++k) {
+            g2[k] = *reinterpret_cast<const float4*>(in + k * rs + m + 8);
+            fma_block(acc[k], g0[k], g1[k], g2[k], wv);
+        }
+        m += 4;
+        if (m >= mhi) break;
+        wv = *reinterpret_cast<const float4*>(w + m);
+#pragma unroll
+        for (int k = 0; k < NR; ++k) {
+            g0[k] = *reinterpret_cast<const float4*>(in + k * rs + m + 8);
+            fma_block(acc[k], g1[k], g2[k], g0[k], wv);
+        }
+        m += 4;
+        if (m >= mhi) break;
+        wv = *reinterpret_cast<const float4*>(w + m);
+#pragma unroll
+        for (int k = 0; k < NR; ++k) {
+            g1[k] = *reinterpret_cast<const float4*>(in + k * rs + m + 8);
+            fma_block(acc[k], g2[k], g0[k], g1[k], wv);
+        }
+        m += 4;
+        if (m >= mhi) break;
+    }
+}
+
 // Output modes (see flc.h): 0 res, 1 exp(-res) in the reference layout;
 // 2 multiply exp(-res) into the beam-layout attenuation out[l][a][z][Y-1-y][x],
 // volume v = a_local * L + l.
@@ -210,6 +254,12 @@ cone_tma_kernel(const __grid_constant__ CUtensorMap tmap, const float* __restric
         }
     }
 
+    // y-filter ownership: (yf_j, yf_half, yf_r0) with yf_r0 fastest; each
+    // thread takes rows yf_r0 + zq * {0, 1, 2, 3}, zq = 8 * zblocks
+    const int zq = 8 * g.zblocks;
+    const int yf_r0 = tid % zq;
+    const int yf_half = (tid / zq) % (TY / 8);
+    const int yf_j = tid / (zq * (TY / 8));
     // z-filter ownership: (j, t, zb) with t fastest
     const int zt_t = tid % TY;
     const int zt_j = (tid / TY) % XB;
@@ -229,22 +279,34 @@ cone_tma_kernel(const __grid_constant__ CUtensorMap tmap, const float* __restric
         __syncthreads();
         if (s_fail) break;
         // ---- y filter: X[j][t][HZP + z] = sum_m wy[j][m] * S[z][t + m] ----
-        const float* Sb = S + buf * sbuf;
-        const int items = XB * Z * (TY / 8);
-        for (int it = tid; it < items; it += nthr) {
-            int z = it % Z;
-            int rest = it / Z;
-            int half = rest % (TY / 8);
-            int j = rest / (TY / 8);
-            const int d = p - (x0 + j);
-            if (d < 0 || d >= g.Mx || x0 + j >= X || !meta[d * 8]) continue;
-            float a8[8];
+        // this thread: target yf_j, columns yf_half*8.., rows yf_r0 + zq*{0..3}
+        {
+            const float* Sb = S + buf * sbuf;
+            const int d = p - (x0 + yf_j);
+            if (d >= 0 && d < g.Mx && x0 + yf_j < X && meta[d * 8]) {
+                const int mlo = meta[d * 8 + 1], mhi = meta[d * 8 + 2];
+                const float* wr = wy + d * g.WY;
 #pragma unroll
-            for (int k = 0; k < 8; ++k) a8[k] = 0.f;
-            corr8(a8, Sb + z * g.boxW + half * 8, wy + d * g.WY, meta[d * 8 + 1], meta[d * 8 + 2]);
-            float* xo = Xs + (j * TY + half * 8) * g.PZ + g.HZP + z;
+                for (int pr = 0; pr < 2; ++pr) {
+                    // rows z0, z0 + zq (clamped to the staged plane; extra rows are not stored)
+                    const int z0 = yf_r0 + 2 * pr * zq;
+                    const int za = min(z0, Z - 1), zb2 = min(z0 + zq, Z - 1);
+                    float a8[2][8];
 #pragma unroll
-            for (int k = 0; k < 8; ++k) xo[k * g.PZ] = a8[k];
+                    for (int k = 0; k < 8; ++k) a8[0][k] = a8[1][k] = 0.f;
+                    corr8_rows<2>(a8, Sb + za * g.boxW + yf_half * 8, (zb2 - za) * g.boxW, wr,
+                                  mlo, mhi);
+                    float* xo = Xs + (yf_j * TY + yf_half * 8) * g.PZ + g.HZP;
+                    if (z0 < Z) {
+#pragma unroll
+                        for (int k = 0; k < 8; ++k) xo[k * g.PZ + z0] = a8[0][k];
+                    }
+                    if (z0 + zq < Z) {
+#pragma unroll
+                        for (int k = 0; k < 8; ++k) xo[k * g.PZ + z0 + zq] = a8[1][k];
+                    }
+                }
+            }
         }
         __syncthreads();
         // plane buffer `buf` is free: prefetch plane p + 2 into it
@@ -259,8 +321,7 @@ cone_tma_kernel(const __grid_constant__ CUtensorMap tmap, const float* __restric
             const float* xr = Xs + (zt_j * TY + zt_t) * g.PZ;
             const float* wr = wz + dz_ * g.WZ;
             const int mlo = meta[dz_ * 8 + 3], mhi = meta[dz_ * 8 + 4];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) corr8(acc[q], xr + zt_zb * 32 + q * 8, wr, mlo, mhi);
+            corr8_rows<4>(acc, xr + zt_zb * 32, 8, wr, mlo, mhi);
         }
         // the next iteration's first barrier orders this z filter before the
         // next y filter overwrites X

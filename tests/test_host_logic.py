@@ -66,7 +66,7 @@ def test_mlem_bytes():
 
 
 def test_pick_chunk():
-    assert core.pick_chunk(128, 128, 128, 120, 3) == 2
+    assert core.pick_chunk(128, 128, 128, 120, 3) == 10      # 256 MB of staged mu
     assert core.pick_chunk(64, 64, 64, 60, 1) == 60
     assert core.pick_chunk(8, 8, 8, 100000, 3, chunk=100000) == 65535 // 3
 

@@ -36,7 +36,8 @@ enum TuneKey {
     kTuneProjApc = 1,       // angles per CTA for the projector kernels
     kTuneConeVariant = 2,   // 1: TMA 16x8 tile, 2: TMA 8x4 tile, 3: plain kernel
     kTuneAttenChunk = 3,    // angles per attenuation-pipeline pass
-    kTuneCount = 4
+    kTuneProjBwd = 4,       // backward splat: 1 shared atomics, 0/2 nine disjoint phases
+    kTuneCount = 5
 };
 int64_t tune(int key);
 

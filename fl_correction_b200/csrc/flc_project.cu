@@ -336,6 +336,44 @@ __device__ void backward_angle(const float* sA, const float* sratio, float* sacc
     }
 }
 
+// Backward of one (angle, slice) with shared-memory atomics instead of
+// phases (the "proj.bwd" = 1 variant): every thread takes samples it = t,
+// t + nthr, ... (a warp covers a run of consecutive columns of one beam row)
+// and adds its four bilinear weights with atomicAdd; no barrier inside the
+// angle.  Samples clamped in both coordinates pile onto a corner and are
+// summed in registers (compile-time reference count) or added like the rest.
+// Float atomics on shared memory are read-modify-write loops on this part,
+// and neighbouring lanes hit neighbouring cells, so the nine-phase form is
+// the default; this one stays for the autotuner.
+template <int RC>
+__device__ void backward_angle_atomic(const float* sA, const float* sratio, float* sacc,
+                                      int img_stride, int pitch, const float* em_a, int Rrt,
+                                      const Geo& g, int H, int W, Corners& cs, int dh, int dw,
+                                      int h0, int w0) {
+    const int R = RC > 0 ? RC : Rrt;
+    int h = h0, w = w0;
+    while (h < H) {
+        const Foot f = footprint(g, sA, sratio, W, pitch, h, w);
+        const bool corner = (f.kind & 3) && (f.kind & 12);
+#pragma unroll
+        for (int r = 0; r < (RC > 0 ? RC : R); ++r) {
+            const float v = em_a[r] * f.av;
+            if (RC > 0 && corner && r < kCornerR) {
+                cs.add(r, ((f.kind & 2) ? 2 : 0) + ((f.kind & 8) ? 1 : 0), v);
+                continue;
+            }
+            float* q = sacc + r * img_stride + f.off;
+            if (f.w00 != 0.f) atomicAdd(q, v * f.w00);
+            if (f.w01 != 0.f) atomicAdd(q + 1, v * f.w01);
+            if (f.w10 != 0.f) atomicAdd(q + pitch, v * f.w10);
+            if (f.w11 != 0.f) atomicAdd(q + pitch + 1, v * f.w11);
+        }
+        h += dh;
+        w += dw;
+        if (w >= W) { w -= W; ++h; }
+    }
+}
+
 // Adds the register corner sums into the row buffers: warp-reduce, then one
 // atomic per warp and pixel.
 __device__ void flush_corners(Corners& cs, float* srow, const Geo& g, int R, int W) {
@@ -463,7 +501,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 proj_bwd_kernel(const float* __restrict__ atten, const float* __restrict__ ratio,
                 const float* __restrict__ em, const float* __restrict__ theta,
                 float* __restrict__ out, int A, int B, int R, int H, int W, int apc,
-                float clamp_min, int stage_tile) {
+                float clamp_min, int stage_tile, int bwd_mode) {
     extern __shared__ __align__(16) float smem[];
     cg::cluster_group cluster = cg::this_cluster();
     const int b = blockIdx.y;
@@ -479,6 +517,8 @@ proj_bwd_kernel(const float* __restrict__ atten, const float* __restrict__ ratio
     float* sem = sratio + W;
     const bool vec = stage_tile && ((HW & 3) == 0) && (((uintptr_t)atten & 15) == 0);
     for (int i = threadIdx.x; i < R * (img_stride + 3 * W + 3 * H); i += blockDim.x) sacc[i] = 0.f;
+    const int wk_dh = blockDim.x / W, wk_dw = blockDim.x - wk_dh * W;
+    const int wk_h0 = threadIdx.x / W, wk_w0 = threadIdx.x - wk_h0 * W;
     Corners cs;
     cs.zero();
     TileRegs tr;
@@ -493,8 +533,13 @@ proj_bwd_kernel(const float* __restrict__ atten, const float* __restrict__ ratio
             sratio[w] = ratio ? ratio[((int64_t)a * B + b) * W + w] : 1.f;
         __syncthreads();
         if (a + 1 < a1 && vec) tile_issue(tr, atten + ((int64_t)(a + 1) * B + b) * HW, HW);
-        backward_angle<RC>(stage_tile ? sA : src, sratio, sacc, srow, scol, img_stride, pitch, sem,
-                       R, make_geo(theta[a], H, W), H, W, cs);
+        if (bwd_mode != 1)
+            backward_angle<RC>(stage_tile ? sA : src, sratio, sacc, srow, scol, img_stride, pitch,
+                               sem, R, make_geo(theta[a], H, W), H, W, cs);
+        else
+            backward_angle_atomic<RC>(stage_tile ? sA : src, sratio, sacc, img_stride, pitch, sem,
+                                      R, make_geo(theta[a], H, W), H, W, cs, wk_dh, wk_dw, wk_h0,
+                                      wk_w0);
     }
     fold_frame(cs, sacc, srow, scol, img_stride, pitch, R, H, W);
     cluster.sync();
@@ -518,7 +563,7 @@ mlem_iter_kernel(const float* __restrict__ atten, const float* __restrict__ em,
                  const float* __restrict__ theta, const float* __restrict__ I,
                  const float* __restrict__ sens, const float* __restrict__ Cin,
                  float* __restrict__ Cout, int A, int B, int R, int H, int W, int apc,
-                 float beta, float delta) {
+                 float beta, float delta, int bwd_mode) {
     extern __shared__ __align__(16) float smem[];
     cg::cluster_group cluster = cg::this_cluster();
     const int b = blockIdx.y;
@@ -538,6 +583,8 @@ mlem_iter_kernel(const float* __restrict__ atten, const float* __restrict__ em,
     const bool vec = ((HW & 3) == 0) && (((uintptr_t)atten & 15) == 0);
     stage_slice(sC, Cin, R, B, b, H, W, pitch);
     for (int i = threadIdx.x; i < R * (img_stride + 3 * W + 3 * H); i += blockDim.x) sacc[i] = 0.f;
+    const int wk_dh = blockDim.x / W, wk_dw = blockDim.x - wk_dh * W;
+    const int wk_h0 = threadIdx.x / W, wk_w0 = threadIdx.x - wk_h0 * W;
     Corners cs;
     cs.zero();
     TileRegs tr;
@@ -558,7 +605,12 @@ mlem_iter_kernel(const float* __restrict__ atten, const float* __restrict__ em,
             sratio[w] = I[((int64_t)a * B + b) * W + w] / fmaxf(s, 1e-6f);
         }
         __syncthreads();
-        backward_angle<RC>(sA, sratio, sacc, srow, scol, img_stride, pitch, sem, R, g, H, W, cs);
+        if (bwd_mode != 1)
+            backward_angle<RC>(sA, sratio, sacc, srow, scol, img_stride, pitch, sem, R, g, H, W,
+                               cs);
+        else
+            backward_angle_atomic<RC>(sA, sratio, sacc, img_stride, pitch, sem, R, g, H, W, cs,
+                                      wk_dh, wk_dw, wk_h0, wk_w0);
     }
     fold_frame(cs, sacc, srow, scol, img_stride, pitch, R, H, W);
     cluster.sync();
@@ -787,8 +839,9 @@ int bwd_emission_launch(const float* atten, const float* ratio, const float* em,
     const void* fn = R == 1 ? (const void*)proj_bwd_kernel<1> : (const void*)proj_bwd_kernel<0>;
     Plan p = plan_cluster(fn, A, B, smem);
     int iA = (int)A, iB = (int)B, iR = (int)R, iH = (int)H, iW = (int)W, apc = p.apc;
+    int bwd_mode = (int)tune(kTuneProjBwd);
     void* args[] = {(void*)&atten, (void*)&ratio, (void*)&em, (void*)&theta, (void*)&out,
-                    &iA, &iB, &iR, &iH, &iW, &apc, &clamp_min, &stage_tile};
+                    &iA, &iB, &iR, &iH, &iW, &apc, &clamp_min, &stage_tile, &bwd_mode};
     return launch_cluster(fn, dim3(p.G, (unsigned)B), p.G, smem, st, args);
 }
 
@@ -828,8 +881,10 @@ int mlem_iter_launch(const float* atten, const float* em, const float* theta, co
     const void* fn = R == 1 ? (const void*)mlem_iter_kernel<1> : (const void*)mlem_iter_kernel<0>;
     Plan p = plan_cluster(fn, A, B, smem);
     int iA = (int)A, iB = (int)B, iR = (int)R, iH = (int)H, iW = (int)W, apc = p.apc;
+    int bwd_mode = (int)tune(kTuneProjBwd);
     void* args[] = {(void*)&atten, (void*)&em, (void*)&theta, (void*)&I, (void*)&sens,
-                    (void*)&Cin, (void*)&Cout, &iA, &iB, &iR, &iH, &iW, &apc, &beta, &delta};
+                    (void*)&Cin, (void*)&Cout, &iA, &iB, &iR, &iH, &iW, &apc, &beta, &delta,
+                    &bwd_mode};
     return launch_cluster(fn, dim3(p.G, (unsigned)B), p.G, smem, st, args);
 }
 

@@ -9,6 +9,7 @@ CUDA events and keeps the fastest through ``flc_tune_set``:
   proj.apc       angles per CTA of the forward projector
   cone.variant   TMA 16x8 tile, TMA 8x4 tile or the plain separable kernel
   atten.chunk    angles per attenuation-pipeline pass
+  proj.bwd       backward splat with shared atomics or in nine disjoint phases
 
 Every candidate is checked against the automatic choice before it is timed
 (the results must agree to FP32 round-off), so tuning never changes answers
@@ -26,7 +27,7 @@ from . import _lib
 __all__ = ["set_knob", "get_knob", "knobs", "time_ms", "tune_projector", "tune_cone",
            "tune_mlem", "autotune"]
 
-KNOBS = ("proj.cluster", "proj.apc", "cone.variant", "atten.chunk")
+KNOBS = ("proj.cluster", "proj.apc", "cone.variant", "atten.chunk", "proj.bwd")
 
 
 def set_knob(name, value):
@@ -96,13 +97,15 @@ def _proj_inputs(A, B, H, W, dev, seed=0):
 
 
 def tune_projector(A, B, H, W, device="cuda"):
-    """proj.cluster for the backward projector, proj.apc for the forward."""
+    """proj.bwd and proj.cluster for the backward projector, proj.apc for the
+    forward."""
     from .cuda_lib import atten_cuda as AC
     dev = torch.device(device)
     atten, em, th, C, r = _proj_inputs(A, B, H, W, dev)
     bwd = lambda: AC.backward_emission_batch(atten, r, em, th)  # noqa: E731
     fwd = lambda: AC.forward_emission_batch(atten, C, em, th)  # noqa: E731
     out = {}
+    out["proj.bwd"] = _sweep("proj.bwd", [0, 1, 2], bwd, _close)
     out["proj.cluster"] = _sweep("proj.cluster", [0, 1, 2, 4, 8], bwd, _close)
     apcs = sorted({0} | {a for a in (1, 2, 3, 4, 6, 8, 12, 16) if a <= A})
     out["proj.apc"] = _sweep("proj.apc", apcs, fwd, _close)

@@ -62,7 +62,8 @@ def test_graph_and_eager_agree_and_input_untouched():
     a, e, t, i = T(atten), T(em), T(th), T(I)
     _lib.call("flc_mlem", _lib.ptr(C1), _lib.ptr(a), _lib.ptr(e), _lib.ptr(t), _lib.ptr(i), 7,
               1e-3, 0.01, 12, 4, 1, 32, 32, _lib.ptr(ws), ws_b, 0, _lib.stream())
-    assert rel_err(C1.cpu().numpy(), out_graph.cpu().numpy()) < 1e-6
+    # same iterations; the backward's shared-memory atomics sum in run-dependent order
+    assert rel_err(C1.cpu().numpy(), out_graph.cpu().numpy()) < 1e-5
 
 
 def test_numpy_drivers():

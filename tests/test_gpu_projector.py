@@ -124,3 +124,24 @@ def test_non_contiguous_inputs():
     assert not at.is_contiguous()
     out = AC.forward_emission_batch(at, T(C), T(em), T(th)).cpu().numpy()
     assert rel_err(out, O.fwd_emission(atten, C, em, th)) < TOL_MAP
+
+
+@pytest.mark.parametrize("mode", [1, 2])
+@pytest.mark.parametrize("A,B,R,H,W", [(8, 3, 2, 20, 28), (5, 2, 1, 64, 64), (1, 1, 1, 2, 2)])
+def test_backward_splat_variants(mode, A, B, R, H, W):
+    # shared-atomic splat and nine-phase splat give the same transpose
+    from fl_correction_b200 import tune
+    rng = np.random.default_rng(A * 1000 + H + 7)
+    atten, C, em, th = projector_case(rng, A, B, R, H, W, SPECIAL[:A] if A <= 8 else None)
+    ratio = rng.random((A, B, W)).astype(np.float32)
+    old = tune.get_knob("proj.bwd")
+    tune.set_knob("proj.bwd", mode)
+    try:
+        out = AC.backward_emission_batch(T(atten), T(ratio), T(em), T(th)).cpu().numpy()
+        C0 = np.ones_like(C)
+        I = O.fwd_emission(atten, C, em, th)
+        mout = AC.mlem_cuda_batch(T(C0), T(atten), T(em), T(th), T(I), 3, 0.0, 0.01).cpu().numpy()
+    finally:
+        tune.set_knob("proj.bwd", old)
+    assert rel_err(out, O.bwd_emission(atten, ratio, em, th)) < TOL_MAP
+    assert rel_err(mout, O.mlem(C0, atten, em, th, I, 3, 0.0, 0.01)) < 1e-4

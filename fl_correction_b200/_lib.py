@@ -37,6 +37,8 @@ SIGNATURES = {
     "flc_mlem_workspace_bytes": (_sz, [_i64, _i64, _i64, _i64, _i64]),
     "flc_mlem": (_int, [_vp, _vp, _vp, _vp, _vp, _i64, _f64, _f64, _i64, _i64, _i64, _i64, _i64,
                         _vp, _sz, _int, _vp]),
+    "flc_mlem_static": (_int, [_vp, _vp, _vp, _vp, _vp, _i64, _f64, _f64, _i64, _i64, _i64, _i64,
+                               _i64, _vp]),
     "flc_atten_workspace_bytes": (_sz, [_i64, _i64, _i64, _i64, _i64, _i64, _i64]),
     "flc_atten_maps": (_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64,
                               _i64, _i64, _i64, _i64, _int, _int, _i64, _vp, _sz, _vp]),

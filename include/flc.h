@@ -132,6 +132,18 @@ FLC_API int flc_mlem(float* C, const float* atten, const float* em, const float*
              const float* I, int64_t n_iter, double beta, double delta,
              int64_t A, int64_t B, int64_t R, int64_t H, int64_t W,
              void* workspace, size_t workspace_bytes, int use_graph, void* stream);
+/* flc_mlem without a caller workspace: the scratch is a static 32 MiB device
+ * array inside the library, so the call allocates nothing.  For callers that
+ * cannot allocate device memory (an FFI host that passes only the data
+ * buffers, a process whose device memory another framework has reserved).
+ * No counterpart in the reference.  Problems whose flc_mlem_workspace_bytes
+ * exceeds 32 MiB return FLC_ERR_UNSUPPORTED.  The first call on a device
+ * looks up the array's address (make it before any stream capture); calls
+ * that overlap in time share the array and race.  Runs the eager iteration
+ * path (use_graph = 0). */
+FLC_API int flc_mlem_static(float* C, const float* atten, const float* em, const float* theta,
+                    const float* I, int64_t n_iter, double beta, double delta,
+                    int64_t A, int64_t B, int64_t R, int64_t H, int64_t W, void* stream);
 
 /* ---------------------------------------------------------------------
  * Per-angle attenuation maps (rotation + mu assembly + incident scan +

@@ -71,6 +71,14 @@ def mlem_bytes_per_iter(A, S, H, W, R=1):
     return fwd + bwd + upd
 
 
+# DRAM bytes measured by ncu (profiles/cone_tma_kernel_6x128cube.md,
+# profiles/mlem_iter_kernel_24ang_16x128sq.md): the cone moves 19.66 MB per
+# 128^3 volume (read 100.76 MB + write 17.20 MB for 6 volumes); a fused MLEM
+# iteration moves 1.092 bytes per attenuation byte (27.51 MB for 25.17 MB).
+CONE_DRAM_BYTES_PER_VOLUME = (100.76e6 + 17.20e6) / 6
+MLEM_DRAM_PER_ATTEN_BYTE = 27.51e6 / (24 * 16 * 128 * 128 * 4)
+
+
 def cone_work(mask, Z, H, W):
     """(nnz-form MACs, separable MACs) of one cone volume (Z, H, W) with mask
     (Mz, Mx, My), counting only taps that land inside the volume."""
@@ -261,16 +269,17 @@ def run_ours(args, rank, world, device):
                    "l2": "inputs larger than L2 (attenuation %.1f GB per step)" % (L * A * N ** 3 * 4 / 1e9)},
         "corrected_proj_gbs": round(proj_gbs, 1) if proj_gbs else None,
         "corrected_proj_pct_hbm": round(100 * proj_gbs / hbm, 1) if proj_gbs else None,
-        "time_share": {"cone_sep_kernel": round(cone_share, 3),
+        "time_share": {"cone_tma_kernel": round(cone_share, 3),
                        "mlem (sens + fused iterations)": round(t_mlem / ms, 3) if ms else None},
         "roofline": {
-            "kernel": "cone_sep_kernel (fluorescence cone path sum)",
+            "kernel": "cone_tma_kernel (fluorescence cone path sum)",
             "bound": "fp32",
             "achieved": round(2 * sep * vols_per_launch / (cone_avg_ms * 1e-3) / 1e12, 2),
             "peak": round(fp32_peak, 1),
             "unit": "TFLOP/s",
             "frac": round(2 * sep * vols_per_launch / (cone_avg_ms * 1e-3) / 1e12 / fp32_peak, 3),
-            "traffic": None,
+            "traffic": round(CONE_DRAM_BYTES_PER_VOLUME * vols_per_launch * (N / 128) ** 3),
+            "traffic_note": "ncu dram read+write of a 6-volume 128^3 launch, per volume, times volumes per launch",
             "peak_kind": "nominal FP32 (148 SM x 128 lanes x 2 x 1965 MHz); no measured FP32 peak",
             "algorithmic_unit": "separable FLOPs 2*sum(wz+wy) per output and depth = %.3g per volume" % (2 * sep),
             "launches": cone_launches, "avg_ms": round(cone_avg_ms, 4),
@@ -279,7 +288,9 @@ def run_ours(args, rank, world, device):
         "roofline_mlem": {
             "kernel": "mlem_iter_kernel (+ sensitivity backward)", "bound": "hbm",
             "achieved": round(proj_gbs, 1) if proj_gbs else None, "peak": hbm, "unit": "GB/s",
-            "frac": round(proj_gbs / hbm, 3) if proj_gbs else None, "traffic": None,
+            "frac": round(proj_gbs / hbm, 3) if proj_gbs else None,
+            "traffic": round(MLEM_DRAM_PER_ATTEN_BYTE * A * N ** 3 * 4),
+            "traffic_note": "per element-iteration: ncu dram bytes of a 24x16x128^2 iteration per attenuation byte, scaled",
             "peak_kind": peak_kind,
             "algorithmic_unit": "%.4g B per element-iteration (fwd + bwd + update at the reference API boundary)" % bytes_it,
         },

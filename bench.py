@@ -176,6 +176,24 @@ def build_problem(cfg, rank, device):
     return wl, mask, solver, I.contiguous()
 
 
+def max_over_ranks(ms, world, device):
+    """The maximum over ranks of a per-rank device time (every rank gets it)."""
+    if world <= 1:
+        return ms
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t)
+
+
+def job_rate(world, iters_per_rank, ms_max):
+    """Whole-job MLEM iterations per second: every rank runs its own replica of
+    the workload, so the job does world x iters_per_rank in the slowest
+    rank's time."""
+    return world * iters_per_rank / (ms_max * 1e-3)
+
+
 def run_ours(args, rank, world, device):
     import torch
     import torch.distributed as dist
@@ -211,11 +229,7 @@ def run_ours(args, rank, world, device):
     ms = start.elapsed_time(end)
     t_cone = sum(a.elapsed_time(b) for a, b, _ in cone_ev)
     t_mlem = sum(a.elapsed_time(b) for a, b, _ in mlem_ev)
-    ms_max = ms
-    if world > 1:
-        t = torch.tensor([ms], device=device, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t)
+    ms_max = max_over_ranks(ms, world, device)
 
     # ---- end to end through the host-buffer entry point ----------------
     I_host = I.cpu().pin_memory()
@@ -230,11 +244,7 @@ def run_ours(args, rank, world, device):
     e1.record()
     torch.cuda.synchronize()
     barrier()
-    e2e_ms = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([e2e_ms], device=device, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t)
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), world, device)
 
     # ---- derived figures ----------------------------------------------
     n_cone = sum(v for _, _, v in cone_ev)
@@ -246,8 +256,8 @@ def run_ours(args, rank, world, device):
     mlem_iters = sum(v for _, _, v in mlem_ev)      # element-iterations timed
     bytes_it = mlem_bytes_per_iter(A, N, N, N)
     proj_gbs = bytes_it * mlem_iters / (t_mlem * 1e-3) / 1e9 if t_mlem else None
-    value = world * n_iter * args.steps / (ms_max * 1e-3)
-    e2e_value = world * n_iter * args.steps / (e2e_ms * 1e-3)
+    value = job_rate(world, n_iter * args.steps, ms_max)
+    e2e_value = job_rate(world, n_iter * args.steps, e2e_ms)
     cone_share = t_cone / ms if ms else 0.0
     line = {
         "metric": METRIC,

@@ -125,3 +125,26 @@ def test_xrf_project_equals_atten_then_projector():
             att = O.incident_scan(fr[l:l + 1] * cx[a, l])[0] * E[l]
             ref = O.fwd_emission(att[None], frac[l:l + 1], em[l, a].reshape(1, 1), th[a:a + 1])[0]
             assert rel_err(Pf[l, a], ref) < 1e-12
+
+
+def test_xrf_adjoint_matches_torch_autograd_fp64():
+    # a third, independent composition: torch operators (grid_sample, cumprod,
+    # conv3d, gathers) differentiated by autograd in FP64
+    import torch
+    from tests import torch_model as TM
+    rng = np.random.default_rng(8)
+    n_ch, S, N, A, L = 3, 3, 10, 3, 2
+    frac = rng.random((n_ch, S, N, N)) * 0.8
+    th = np.array([0.3, 1.7, -2.4], np.float32)
+    cx = rng.uniform(0.02, 0.1, (A, n_ch))
+    cf = rng.uniform(0.02, 0.1, (A, L, n_ch))
+    mask = generate_detector_mask(13.309, 13.309, N)
+    em = rng.uniform(0.5, 2, (L, A))
+    for inc in ["own", "all", "none"]:
+        ref = O.xrf_project(frac, th, cx, cf, mask, em, inc)
+        C = torch.tensor(frac[:L], dtype=torch.float64, requires_grad=True)
+        Pf = TM.xrf_project(torch.cat([C, torch.tensor(frac[L:])]), th, cx, cf, mask, em, inc)
+        assert rel_err(Pf.detach().numpy(), ref) < 1e-6
+        g = rng.standard_normal(ref.shape)
+        (Pf * torch.tensor(g)).sum().backward()
+        assert rel_err(C.grad.numpy(), O.xrf_project_adjoint(frac, th, cx, cf, mask, em, g, inc)) < 1e-6

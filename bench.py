@@ -42,8 +42,12 @@ def parse():
     p.add_argument("--steps", type=int, default=3)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--config", type=int, default=1, choices=[0, 1])
+    p.add_argument("--config", type=int, default=1, choices=[0, 1, 2, 3, 4],
+                   help="0/1: corrected MLEM (1 is the benchmark); 2/4: gradient "
+                        "reconstruction; 3: batched uneven volumes")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--adam-steps", type=int, default=0,
+                   help="configurations 2/4: Adam steps timed (default 200 / 3)")
     p.add_argument("--case", default=None, choices=["cone", "mlem", "fwd", "bwd"],
                    help="run one kernel on a profiling-sized case instead of the benchmark")
     return p.parse_args()
@@ -393,6 +397,224 @@ def run_reference(args):
     }
 
 
+def param_at_angles(param, n_angle, idx):
+    """The parameter dict restricted to the angles idx: every per-angle array
+    (length n_angle) is indexed, everything else is kept."""
+    def sel(v):
+        if isinstance(v, dict):
+            return {k: sel(x) for k, x in v.items()}
+        a = np.asarray(v) if isinstance(v, (list, np.ndarray)) else None
+        if a is not None and a.dtype.kind in "fiu" and a.ndim >= 1 and a.shape[0] == n_angle:
+            return a[idx]
+        return v
+    return sel(param)
+
+
+def run_grad(args, device):
+    """Configurations 2 and 4: gradient reconstruction through the attenuation.
+
+    Reports Adam steps per second (each step: a corrected projection with the
+    attenuation rebuilt per angle chunk, and its hand-written adjoint), the
+    device-memory high-water mark, the gradient check, and the same step done
+    the plain way: torch autograd through a torch-operator composition of the
+    model (grid_sample, cumprod, conv3d, gathers) on the same GPU.  The
+    gradient check compares, on a subset of the angles, the adjoint gradient
+    with FP64 torch autograd and with FP64 central differences (eps = 1e-4)
+    at random voxels."""
+    import torch
+    from fl_correction_b200 import _lib, phantoms
+    from fl_correction_b200.detector_mask import generate_detector_mask
+    from fl_correction_b200.grad_recon import GradientRecon, gradient_loss
+    from tests import torch_model as TM
+    wl = phantoms.make_workload(args.config)
+    N, L, A = wl.N, len(wl.elements), len(wl.angles)
+    mask = generate_detector_mask(wl.mask_angle, wl.mask_angle, N)
+    frac = wl.frac()
+    torch.cuda.reset_peak_memory_stats(device)
+    rec = GradientRecon(wl.param, wl.angles, mask, (N, N, N), fixed_frac=frac[L:],
+                        tv_weight=1e-3, lr=1e-2, device=device)
+    truth = torch.from_numpy(wl.conc).to(device)
+    I = rec.proj.project(truth)
+    C0 = torch.full_like(truth, 0.5)
+    n_steps = args.adam_steps if args.adam_steps > 0 else (200 if args.config == 2 else 3)
+
+    # ---- gradient check on a subset of angles ---------------------------
+    sub = np.linspace(0, A - 1, 4 if N > 128 else 6).astype(int)
+    chk = GradientRecon(param_at_angles(wl.param, A, sub), wl.angles[sub], mask, (N, N, N),
+                        fixed_frac=frac[L:], tv_weight=1e-3, device=device)
+    Ichk = I[:, sub].contiguous()
+    Cc = (0.8 * truth + 0.1).contiguous()
+    g32, _ = chk.gradient(Cc, Ichk)
+    pr = chk.proj
+    th, cx, cf, em = (pr.theta.cpu().numpy(), pr.coef_x.cpu().numpy(), pr.coef_f.cpu().numpy(),
+                      pr.em.cpu().numpy())
+    fixed64 = torch.from_numpy(frac[L:]).to(device, torch.float64)
+    I64 = Ichk.double()
+
+    def loss64(C):
+        Pf = TM.xrf_project(torch.cat([C, fixed64]), th, cx, cf, mask, em)
+        return torch.mean((Pf - I64) ** 2) / torch.mean(I64 ** 2) + 1e-3 * gradient_loss(C)
+
+    grad_check = {"angles": int(len(sub))}
+    log = lambda *a: print("[grad]", *a, file=sys.stderr, flush=True)  # noqa: E731
+    log("gradient check on", len(sub), "angles")
+    C64 = Cc.double().clone().requires_grad_(True)
+    loss64(C64).backward()
+    grad_check["max_rel_err_vs_torch_fp64_autograd"] = float(
+        (g32.double() - C64.grad).abs().max() / C64.grad.abs().max())
+    with torch.no_grad():
+        Pf64 = TM.xrf_project(torch.cat([Cc.double(), fixed64]), th, cx, cf, mask, em)
+        Pf32 = pr.project(Cc).double()
+        grad_check["projection_max_rel_err_vs_fp64"] = float((Pf32 - Pf64).abs().max() /
+                                                             Pf64.abs().max())
+    del C64, Pf64, Pf32
+    log("autograd comparison done", grad_check)
+    if N <= 128:
+        rng = np.random.default_rng(7)
+        eps, errs = 1e-4, []
+        gmax = float(g32.abs().max())
+        with torch.no_grad():
+            for _ in range(64):
+                idx = tuple(int(rng.integers(0, n)) for n in Cc.shape)
+                Cp = Cc.double().clone()
+                Cm = Cp.clone()
+                Cp[idx] += eps
+                Cm[idx] -= eps
+                fd = (float(loss64(Cp)) - float(loss64(Cm))) / (2 * eps)
+                errs.append(abs(float(g32[idx]) - fd) / gmax)
+        grad_check["fd_voxels"] = 64
+        grad_check["max_abs_err_vs_fd_over_max_grad"] = float(max(errs))
+    del chk
+    torch.cuda.empty_cache()
+    log("check done", grad_check)
+
+    # ---- Adam steps ---------------------------------------------------------
+    torch.cuda.reset_peak_memory_stats(device)
+    rec.run(I, C0, n_steps=max(1, args.warmup))
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = _lib.query("flc_launch_count")
+    e0.record()
+    C = rec.run(I, C0, n_steps=n_steps)
+    e1.record()
+    torch.cuda.synchronize()
+    launches = _lib.query("flc_launch_count") - launches0
+    ms = e0.elapsed_time(e1)
+    misfit = float(torch.mean((rec.proj.project(C) - I) ** 2) / torch.mean(I ** 2))
+    peak_gb = torch.cuda.max_memory_allocated(device) / 1e9
+
+    log("adam: %d steps in %.1f ms" % (n_steps, ms))
+    # ---- the plain way: torch autograd through the operator composition (FP32)
+    plain = None
+    if N <= 128:
+        try:
+            thf = rec.proj.theta.cpu().numpy()
+            cxf, cff, emf = (rec.proj.coef_x.cpu().numpy(), rec.proj.coef_f.cpu().numpy(),
+                             rec.proj.em.cpu().numpy())
+            fixed32 = torch.from_numpy(frac[L:]).to(device)
+            g0, _ = rec.gradient(C0, I)
+            Cp = C0.clone().requires_grad_(True)
+            norm = float(torch.mean(I ** 2)) * I.numel()
+            n_chunk = 6                      # angles per autograd graph (memory)
+
+            def plain_step():
+                # the loss is a sum over angles: one graph per chunk of angles,
+                # gradients accumulated in Cp.grad
+                Cp.grad = None
+                for a0 in range(0, A, n_chunk):
+                    sl = slice(a0, min(A, a0 + n_chunk))
+                    Pf = TM.xrf_project(torch.cat([Cp, fixed32]), thf[sl], cxf[sl], cff[sl], mask,
+                                        emf[:, sl])
+                    (torch.sum((Pf - I[:, sl]) ** 2) / norm).backward()
+                (1e-3 * gradient_loss(Cp)).backward()
+
+            plain_step()
+            torch.cuda.synchronize()
+            p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            p0.record()
+            plain_step()
+            p1.record()
+            torch.cuda.synchronize()
+            plain = {"ms_per_step": round(p0.elapsed_time(p1), 2),
+                     "speedup_of_adjoint": round(p0.elapsed_time(p1) / (ms / n_steps), 2),
+                     "how": "torch autograd (grid_sample, cumprod, separable conv3d, gathers) "
+                            "in FP32, %d angles per graph" % n_chunk,
+                     "grad_max_rel_diff_vs_adjoint": float(
+                         (Cp.grad - g0).abs().max() / g0.abs().max())}
+        except RuntimeError as e:   # e.g. out of memory for the stored graph
+            plain = {"unavailable": str(e).splitlines()[0][:200]}
+    return {
+        "metric": "Adam steps/s (gradient reconstruction through the attenuation)",
+        "value": round(n_steps / (ms * 1e-3), 3), "unit": "steps/s", "n_gpus": 1,
+        "steps": n_steps, "warmup": args.warmup, "ms_per_step": round(ms / n_steps, 3),
+        "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": wl.name, "volume": [N] * 3, "elements": wl.elements, "angles": A,
+                   "loss": "mean((P(C)-I)^2)/mean(I^2) + 1e-3 TV", "optimizer": "Adam lr 1e-2"},
+        "relative_misfit_after": misfit,
+        "memory_high_water_gb": round(peak_gb, 2),
+        "materialised_attenuation_gb": round(L * A * N ** 3 * 4 / 1e9, 1),
+        "gradient_check": grad_check,
+        "plain_torch_autograd": plain,
+        "gpu_launches": int(launches),
+    }
+
+
+def run_batch(args, device):
+    """Configuration 3: 16 uneven volumes (N from {64..192}, 1-3 elements,
+    60-180 angles, energy and detector distance drawn per volume), the
+    corrected MLEM of all of them as one CUDA graph replay with per-shape
+    autotuned launch shapes, against the plain loop over volumes."""
+    import torch
+    from fl_correction_b200 import _lib, phantoms
+    from fl_correction_b200.batch import BatchedMLEM, problems_from_workloads
+    log = lambda *a: print("[batch]", *a, file=sys.stderr, flush=True)  # noqa: E731
+    n_iter, k = 20, 5
+    ws = phantoms.make_batch_workloads(16, n_iter=n_iter, recompute_every=k)
+    log("workloads", [w.name for w in ws])
+    probs = problems_from_workloads(ws, device)
+    b = BatchedMLEM(probs, n_iter=n_iter, recompute_every=k, n_streams=4, autotune=True,
+                    device=device)
+    log("autotuned", b.knobs)
+    for _ in range(max(1, args.warmup)):
+        b.run_loop()
+    torch.cuda.synchronize()
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    e[0].record()
+    for _ in range(args.steps):
+        loop = b.run_loop()
+    e[1].record()
+    torch.cuda.synchronize()
+    loop = [c.clone() for c in loop]
+    b.capture()
+    for _ in range(max(1, args.warmup)):
+        b.run()
+    torch.cuda.synchronize()
+    l0 = _lib.query("flc_launch_count")
+    e[2].record()
+    for _ in range(args.steps):
+        out = b.run()
+    e[3].record()
+    torch.cuda.synchronize()
+    launches = _lib.query("flc_launch_count") - l0
+    t_loop, t_graph = e[0].elapsed_time(e[1]), e[2].elapsed_time(e[3])
+    err = max(float((o - r).abs().max() / r.abs().max()) for o, r in zip(out, loop))
+    vol_iters = len(ws) * n_iter * args.steps
+    return {
+        "metric": "batched corrected MLEM: volume-iterations/s (16 uneven volumes)",
+        "value": round(vol_iters / (t_graph * 1e-3), 3), "unit": "volume-iters/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_graph / args.steps, 2),
+        "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "cfg3-16-uneven", "volumes": [w.name for w in ws],
+                   "mlem_iters": n_iter, "recompute_every": k, "streams": len(b.groups)},
+        "plain_loop": {"value": round(vol_iters / (t_loop * 1e-3), 3),
+                       "ms_per_step": round(t_loop / args.steps, 2)},
+        "speedup_vs_plain_loop": round(t_loop / t_graph, 3),
+        "max_rel_err_vs_plain_loop": err,
+        "gpu_launches": int(launches),
+        "note": "graph replays count every kernel node (flc_launch_count)",
+    }
+
+
 def run_case(args):
     """One kernel on a profiling-sized case (for ncu): W warm-up launches, then
     one more.  cone: the fluorescence cone of one pipeline chunk at the
@@ -469,6 +691,14 @@ def main():
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     device = torch.device("cuda", torch.cuda.current_device())
+    if args.config in (2, 3, 4):
+        if rank == 0:
+            fn = run_batch if args.config == 3 else run_grad
+            print(json.dumps(fn(args, device)), flush=True)
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
     line = run_ours(args, rank, world, device)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, desc, cores, _ = cpu_sample(args.config)

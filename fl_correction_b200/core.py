@@ -52,7 +52,7 @@ def mask_factors(detector_mask, device):
 
 
 def atten_maps(frac_4D, angle_list, coef_x, coef_f, mask_uv=None, incident="own", xrf=True,
-               out=None, chunk=0, workspace=None, cone_events=None):
+               out=None, chunk=0, workspace=None, cone_events=None, theta=None):
     """Attenuation (L, A, S, H, W) for fractions frac_4D (n_ch, S, H, W) on the
     device: incident term (mode 'own' | 'all' | 'none') times exp(-cone).
 
@@ -60,13 +60,16 @@ def atten_maps(frac_4D, angle_list, coef_x, coef_f, mask_uv=None, incident="own"
     device tensors).  mask_uv: (u, v, mask_shape) from mask_factors.
     cone_events: optional list; when given, the two pipeline stages are issued
     per angle chunk and (start, end, volumes) CUDA events of every cone launch
-    are appended to it."""
+    are appended to it.  theta: optional device tensor of the angles in
+    radians (float32), used instead of converting angle_list (no host copy,
+    so the call can be captured in a CUDA graph)."""
     _lib.require_cuda("atten_maps", frac_4D)
     dev = frac_4D.device
     frac = frac_4D.contiguous()
     n_ch, S, H, W = frac.shape
-    theta = torch.as_tensor(np.asarray(angle_list, dtype=np.float64) / 180.0 * np.pi,
-                            dtype=torch.float32, device=dev)
+    if theta is None:
+        theta = torch.as_tensor(np.asarray(angle_list, dtype=np.float64) / 180.0 * np.pi,
+                                dtype=torch.float32, device=dev)
     A = theta.numel()
     cx = torch.as_tensor(coef_x, dtype=torch.float32, device=dev).contiguous()
     cf = torch.as_tensor(coef_f, dtype=torch.float32, device=dev).contiguous()

@@ -19,7 +19,7 @@ import math
 import numpy as np
 
 __all__ = ["ellipsoid_grains", "voronoi_grains", "layered", "xrf_params", "cone_mask_angle",
-           "Workload", "make_workload"]
+           "Workload", "make_workload", "make_batch_workloads"]
 
 
 def cone_mask_angle(diameter_mm=7.0, distance_mm=30.0):
@@ -158,6 +158,28 @@ class Workload:
         """(L+1, N, N, N) fractions: the element concentrations plus the matrix (1)."""
         L, N = self.conc.shape[0], self.N
         return np.concatenate([self.conc, np.ones((1, N, N, N), np.float32)], 0)
+
+
+def make_batch_workloads(n_volumes=16, seed=20240611, sizes=(64, 96, 128, 160, 192),
+                         n_iter=20, recompute_every=5):
+    """The uneven batch of configuration 3: n_volumes seeded Voronoi volumes
+    with side lengths drawn from `sizes`, 1-3 elements, 60-180 angles over
+    [0, 180), incident energy U(10, 16) keV and detector distance U(20, 40)
+    mm (a 7 mm detector, so the cone angle is 2 atan(3.5 / d))."""
+    rng = np.random.default_rng(seed + 3)
+    names = ["Fe", "Ni", "Cu"]
+    out = []
+    for i in range(n_volumes):
+        n = int(rng.choice(sizes))
+        L = int(rng.integers(1, 4))
+        A = int(rng.integers(60, 181))
+        energy = float(rng.uniform(10.0, 16.0))
+        dist = float(rng.uniform(20.0, 40.0))
+        conc = voronoi_grains(n, rng, L, n_seeds=32)
+        out.append(Workload("cfg3-v%02d-%dc-%delem-%dang" % (i, n, L, A), conc, names[:L],
+                            np.linspace(0, 180, A, endpoint=False), energy, 1e-4,
+                            cone_mask_angle(7.0, dist), n_iter, recompute_every, 0, seed + 17 * i))
+    return out
 
 
 def make_workload(cfg, seed=20240611):

@@ -76,7 +76,7 @@ class CorrectedMLEM:
         self.frac[:self.L].copy_(C)
         atten_maps(self.frac, self.angles, self.coef_x, self.coef_f, self.mask_uv,
                    incident=self.incident, xrf=True, out=self.atten, chunk=self.chunk,
-                   workspace=self.ws_atten, cone_events=cone_events)
+                   workspace=self.ws_atten, cone_events=cone_events, theta=self.theta)
         return self.atten
 
     def mlem(self, C, I, n_iter, use_graph=0, mlem_events=None):
@@ -106,6 +106,18 @@ class CorrectedMLEM:
                             for l in range(self.L)])
 
     # -- the corrected reconstruction --------------------------------------
+    def run_into(self, C, I, n_iter=50, recompute_every=5, cone_events=None, mlem_events=None):
+        """The corrected MLEM schedule on C (L, S, H, W) in place, starting from
+        its current contents.  Allocates nothing and copies nothing to or from
+        the host, so the whole schedule can be captured in a CUDA graph."""
+        done = 0
+        while done < n_iter:
+            k = min(recompute_every, n_iter - done)
+            self.recompute_attenuation(C, cone_events)
+            self.mlem(C, I, k, mlem_events=mlem_events)
+            done += k
+        return C
+
     def run(self, I, C0=None, n_iter=50, recompute_every=5, cone_events=None, mlem_events=None):
         """Corrected MLEM: I (L, A, S, W) device projections; returns C (L, S, H, W).
         Attenuation is rebuilt from the current C before every block of
@@ -117,14 +129,7 @@ class CorrectedMLEM:
             C = torch.ones((self.L, S, H, W), dtype=torch.float32, device=self.device)
         else:
             C = torch.as_tensor(C0, dtype=torch.float32, device=self.device).clone()
-        I = I.contiguous()
-        done = 0
-        while done < n_iter:
-            k = min(recompute_every, n_iter - done)
-            self.recompute_attenuation(C, cone_events)
-            self.mlem(C, I, k, mlem_events=mlem_events)
-            done += k
-        return C
+        return self.run_into(C, I.contiguous(), n_iter, recompute_every, cone_events, mlem_events)
 
     def run_host(self, I_host, C0_host=None, n_iter=50, recompute_every=5):
         """End-to-end form: host (pinned) projections in, host result out."""

@@ -85,3 +85,22 @@ def test_optical_depth_in_range():
     cx, cf = core.atten_coefficients(wl.param, 1)
     depth = (wl.conc.mean(axis=(1, 2, 3)) * cf[0, :, :3].max(axis=0)).max() * wl.N
     assert 0.1 < depth < 5
+
+
+def test_assign_streams_balances_work():
+    from fl_correction_b200.batch import assign_streams
+    works = [100, 10, 90, 50, 40, 5, 5]
+    g = assign_streams(works, 3)
+    assert sorted(i for grp in g for i in grp) == list(range(len(works)))
+    loads = [sum(works[i] for i in grp) for grp in g]
+    assert max(loads) - min(loads) <= 20
+    assert assign_streams([1, 2], 4) == [[1], [0]]
+
+
+def test_batch_workloads_are_seeded_and_in_range():
+    ws = phantoms.make_batch_workloads(6, sizes=(16, 24))
+    ws2 = phantoms.make_batch_workloads(6, sizes=(16, 24))
+    for a, b in zip(ws, ws2):
+        assert a.name == b.name and np.array_equal(a.conc, b.conc)
+        assert 1 <= len(a.elements) <= 3 and 60 <= len(a.angles) <= 180
+        assert a.N in (16, 24) and 10.0 <= a.energy <= 16.0

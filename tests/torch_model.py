@@ -41,13 +41,38 @@ def exclusive_reverse_cumprod(f):
 
 
 def cone(mu, mask):
-    """mu (K, S, H, W), mask (Mz, Mx, My) -> res (K, S, H, W)."""
+    """mu (K, S, H, W), mask (Mz, Mx, My) -> res (K, S, H, W).  A mask whose
+    depth planes are rank one (the detector masks) runs as one pair of 1-D
+    correlations per depth plane; any other mask as one dense conv3d."""
     Mz, Mx, My = mask.shape
     hz, hy = Mz // 2, My // 2
-    k = torch.as_tensor(np.ascontiguousarray(np.transpose(mask, (0, 2, 1))[:, ::-1, :]),
-                        dtype=mu.dtype, device=mu.device)         # [dz, My-1-dy, dx]
-    x = F.pad(mu[:, None], (0, Mx - 1, hy, hy, hz, hz))
-    return F.conv3d(x, k[None, None])[:, 0]
+    K, S, H, W = mu.shape
+    from fl_correction_b200.detector_mask import factor_mask
+    fac = factor_mask(mask)
+    if fac is None:
+        k = torch.as_tensor(np.ascontiguousarray(np.transpose(mask, (0, 2, 1))[:, ::-1, :]),
+                            dtype=mu.dtype, device=mu.device)     # [dz, My-1-dy, dx]
+        x = F.pad(mu[:, None], (0, Mx - 1, hy, hy, hz, hz))
+        return F.conv3d(x, k[None, None])[:, 0]
+    # rank one per depth: the factors as FP64 products of the stored mask
+    m = np.asarray(mask, np.float64)
+    res = torch.zeros_like(mu)
+    x = F.pad(mu, (0, Mx - 1))                                   # zero beyond the far face
+    for d in range(min(Mx, W)):
+        p = m[:, d, :]
+        if not p.any():
+            continue
+        k = int(np.argmax(np.abs(p)))
+        i, j = divmod(k, My)
+        u = p[:, j]                                              # slice profile
+        v = p[i, :] / p[i, j]                                    # column profile
+        plane = x[..., d:d + W]
+        # h - (dy - hy): correlate along h with the reversed column profile
+        kv = torch.as_tensor(v[::-1].copy(), dtype=mu.dtype, device=mu.device)
+        t = F.conv3d(F.pad(plane[:, None], (0, 0, hy, hy, 0, 0)), kv.view(1, 1, 1, My, 1))[:, 0]
+        ku = torch.as_tensor(u.copy(), dtype=mu.dtype, device=mu.device)
+        res = res + F.conv3d(F.pad(t[:, None], (0, 0, 0, 0, hz, hz)), ku.view(1, 1, Mz, 1, 1))[:, 0]
+    return res
 
 
 def project(att, C, em, theta):

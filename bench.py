@@ -48,7 +48,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--adam-steps", type=int, default=0,
                    help="configurations 2/4: Adam steps timed (default 200 / 3)")
-    p.add_argument("--case", default=None, choices=["cone", "mlem", "fwd", "bwd"],
+    p.add_argument("--case", default=None, choices=["cone", "mlem", "fwd", "bwd", "stage"],
                    help="run one kernel on a profiling-sized case instead of the benchmark")
     return p.parse_args()
 
@@ -646,6 +646,19 @@ def run_case(args):
         I = AC.forward_emission_batch(atten, C0 * 0.7, em, th)
         def once():
             AC.mlem_cuda_batch(C0, atten, em, th, I, 1)
+    elif args.case == "stage":
+        # the rotation / mu / incident stage of one chunk: 10 angles x 3 lines, 4 channels, 128^3
+        n_ch, L, A, n_a = 4, 3, 120, 10
+        frac = torch.rand((n_ch, N, N, N), device=dev, generator=g)
+        th = torch.linspace(0, math.pi, A + 1, device=dev)[:-1].contiguous()
+        cx = torch.full((A, n_ch), 0.01, device=dev)
+        cf = torch.full((A, L, n_ch), 0.01, device=dev)
+        atten = torch.empty((L, A, N, N, N), device=dev)
+        ws = torch.empty((n_a, L, N, N, N), device=dev)
+        def once():
+            _lib.call("flc_atten_stage", _lib.ptr(frac), _lib.ptr(th), _lib.ptr(cx), _lib.ptr(cf),
+                      _lib.ptr(atten), _lib.ptr(ws), n_ch, N, N, N, A, L, 0, n_a, 0, 1,
+                      _lib.stream())
     elif args.case in ("fwd", "bwd"):
         A, B = 120, 16
         atten = torch.rand((A, B, N, N), device=dev, generator=g)

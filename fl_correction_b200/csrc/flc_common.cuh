@@ -36,7 +36,7 @@ enum TuneKey {
     kTuneProjApc = 1,       // angles per CTA for the projector kernels
     kTuneConeVariant = 2,   // 1: TMA 16x8 tile, 2: TMA 8x4 tile, 3: plain kernel
     kTuneAttenChunk = 3,    // angles per attenuation-pipeline pass
-    kTuneProjBwd = 4,       // backward splat: 1 shared atomics, 0/2 nine disjoint phases
+    kTuneProjBwd = 4,       // backward: 1 shared-atomic splat, 0/2 nine-phase splat, 3 gather
     kTuneCount = 5
 };
 int64_t tune(int key);
@@ -76,45 +76,3 @@ int cone_device_status(int reset);
         int s__ = (call);              \
         if (s__ != FLC_OK) return s__; \
     } while (0)
-
-// -------------------------------------------------------------------------
-// Projector geometry of the reference (atten_cuda_kernel.cu:91-142,
-// :271-337): the sample for detector column w at beam step h of angle th is
-//   row = c*(h-cy) - s*(w-cx) + cy,   col = s*(h-cy) + c*(w-cx) + cx
-// with c = cos(-th), s = sin(-th), cx = (W-1)/2, cy = (H-1)/2, clamped to
-// [0, H-1.001] x [0, W-1.001], then bilinear on the four neighbours.
-// -------------------------------------------------------------------------
-struct ProjGeom {
-    float c, s, cx, cy, rmax, cmax;
-};
-
-__device__ __forceinline__ ProjGeom proj_geom(float th, int H, int W) {
-    ProjGeom g;
-    g.c = cosf(-th);
-    g.s = sinf(-th);
-    g.cx = (W - 1) * 0.5f;
-    g.cy = (H - 1) * 0.5f;
-    g.rmax = H - 1.001f;
-    g.cmax = W - 1.001f;
-    return g;
-}
-
-// One clamped bilinear sample: top-left corner (i0, j0) and fractions.
-struct Tap {
-    int i0, j0;
-    float fr, fc;
-};
-
-__device__ __forceinline__ Tap proj_tap(const ProjGeom& g, float hf, float wf) {
-    float r = g.c * (hf - g.cy) - g.s * (wf - g.cx) + g.cy;
-    float q = g.s * (hf - g.cy) + g.c * (wf - g.cx) + g.cx;
-    r = fminf(fmaxf(r, 0.f), g.rmax);
-    q = fminf(fmaxf(q, 0.f), g.cmax);
-    Tap t;
-    float r0 = floorf(r), q0 = floorf(q);
-    t.i0 = (int)r0;
-    t.j0 = (int)q0;
-    t.fr = r - r0;
-    t.fc = q - q0;
-    return t;
-}

@@ -88,6 +88,7 @@ struct ConeGeom {
     int PZ;          // X row pitch (floats)
     int WY, WZ;      // padded weight row lengths
     int zblocks;     // Z / 32 rounded up
+    int ring;        // 0: every depth's filters preloaded; 1: a ring of 2 XB rows
 };
 
 // 4 taps x 8 outputs from a 12-value window (a,b,c) and 4 weights w.
@@ -100,32 +101,6 @@ __device__ __forceinline__ void fma_block(float (&acc)[8], const float4& a, cons
         acc[t] = fmaf(w.y, v[t + 1], acc[t]);
         acc[t] = fmaf(w.z, v[t + 2], acc[t]);
         acc[t] = fmaf(w.w, v[t + 3], acc[t]);
-    }
-}
-
-// 8 outputs of a 1-D correlation: out[t] = sum_m w[m] * in[t + m] for m in
-// [mlo, mhi) (mlo a multiple of 4, weights zero outside their support).
-// `in` and `w` are 16-byte aligned shared-memory rows.
-__device__ __forceinline__ void corr8(float (&acc)[8], const float* in, const float* w, int mlo,
-                                      int mhi) {
-    if (mlo >= mhi) return;
-    float4 g0 = *reinterpret_cast<const float4*>(in + mlo);
-    float4 g1 = *reinterpret_cast<const float4*>(in + mlo + 4);
-    float4 g2;
-    int m = mlo;
-    while (true) {
-        g2 = *reinterpret_cast<const float4*>(in + m + 8);
-        fma_block(acc, g0, g1, g2, *reinterpret_cast<const float4*>(w + m));
-        m += 4;
-        if (m >= mhi) break;
-        g0 = *reinterpret_cast<const float4*>(in + m + 8);
-        fma_block(acc, g1, g2, g0, *reinterpret_cast<const float4*>(w + m));
-        m += 4;
-        if (m >= mhi) break;
-        g1 = *reinterpret_cast<const float4*>(in + m + 8);
-        fma_block(acc, g2, g0, g1, *reinterpret_cast<const float4*>(w + m));
-        m += 4;
-        if (m >= mhi) break;
     }
 }
 
@@ -175,7 +150,7 @@ __device__ __forceinline__ void corr8_rows(float (&acc)[NR][8], const float* in,
 // Output modes (see flc.h): 0 res, 1 exp(-res) in the reference layout;
 // 2 multiply exp(-res) into the beam-layout attenuation out[l][a][z][Y-1-y][x],
 // volume v = a_local * L + l.
-template <int TY, int XB>
+template <int TY, int XB, bool RING>
 __global__ void __launch_bounds__(512)
 cone_tma_kernel(const __grid_constant__ CUtensorMap tmap, const float* __restrict__ U,
                 const float* __restrict__ V, float* __restrict__ out, ConeGeom g, int mode, int L,
@@ -188,14 +163,20 @@ cone_tma_kernel(const __grid_constant__ CUtensorMap tmap, const float* __restric
     const int tid = threadIdx.x;
     const int nthr = blockDim.x;
 
-    // shared layout: S[2][Z][boxW] | X[XB][TY][PZ] | wy[Mx][WY] | wz[Mx][WZ] |
+    // shared layout: S[2][Z][boxW] | X[XB][TY][PZ] | wy[nw][WY] | wz[nw][WZ] |
     //               meta[Mx][8] | bars[2]
+    // nw = Mx: every depth's filters are preloaded.  nw = 2 XB (long masks,
+    // whose filters do not fit): depth d sits in ring slot d % (2 XB); at
+    // plane p the CTA's targets meet depths p-x0-XB+1 .. p-x0, and the depth
+    // that enters at the next plane reuses the slot of one last used XB
+    // planes ago.
+    const int nw = RING ? 2 * XB : g.Mx;
     const int sbuf = (Z * g.boxW + 31) & ~31;  // 128-byte aligned TMA destinations
     float* S = reinterpret_cast<float*>(smem_raw);
     float* Xs = S + 2 * sbuf;
     float* wy = Xs + XB * TY * g.PZ;
-    float* wz = wy + g.Mx * g.WY;
-    int* meta = reinterpret_cast<int*>(wz + g.Mx * g.WZ);  // per depth: on, ylo, yhi, zlo, zhi
+    float* wz = wy + nw * g.WY;
+    int* meta = reinterpret_cast<int*>(wz + nw * g.WZ);  // per depth: on, ylo, yhi, zlo, zhi
     uint64_t* bars = reinterpret_cast<uint64_t*>(meta + g.Mx * 8);
     __shared__ int s_fail;
 
@@ -217,41 +198,54 @@ cone_tma_kernel(const __grid_constant__ CUtensorMap tmap, const float* __restric
             tma_load_3d(S + q * sbuf, &tmap, y0 - g.HYP, p_begin + q, v * Z, &bars[q]);
         }
     }
-    // every depth's filters, zero-padded and shifted so that tap m of a row
-    // lines up with input column t + m (y) / row z + m (z); then each depth's
-    // tap support, found by warp ballots
-    for (int i = tid; i < g.Mx * g.WY; i += nthr) {
-        const int d = i / g.WY, dy = i - d * g.WY - g.offy;
-        wy[i] = (dy >= 0 && dy < g.My) ? __ldg(V + (int64_t)d * g.My + dy) : 0.f;
-    }
-    for (int i = tid; i < g.Mx * g.WZ; i += nthr) {
-        const int d = i / g.WZ, dz = i - d * g.WZ - g.offz;
-        wz[i] = (dz >= 0 && dz < g.Mz) ? __ldg(U + (int64_t)d * g.Mz + dz) : 0.f;
+    // Element e of depth d's filter row, zero-padded and shifted so that tap m
+    // lines up with input column t + m (y, e < WY) / row z + m (z, e >= WY).
+    auto wval = [&](int d, int e) -> float {
+        if (e < g.WY) {
+            const int dy = e - g.offy;
+            return (dy >= 0 && dy < g.My) ? __ldg(V + (int64_t)d * g.My + dy) : 0.f;
+        }
+        const int dz = e - g.WY - g.offz;
+        return (dz >= 0 && dz < g.Mz) ? __ldg(U + (int64_t)d * g.Mz + dz) : 0.f;
+    };
+    auto wput = [&](int d, int e, float x) {
+        const int slot = RING ? d % (2 * XB) : d;
+        if (e < g.WY) wy[slot * g.WY + e] = x;
+        else wz[slot * g.WZ + e - g.WY] = x;
+    };
+    // depth 0's filters into the ring (the others stream in one per plane)
+    for (int e = tid; e < g.WY + g.WZ; e += nthr) wput(0, e, wval(0, e));
+    // each depth's tap support [lo, hi] in y and z: every element of every
+    // depth's rows is loaded once, in parallel, and the non-zero ones fold
+    // into shared min / max (integer atomics)
+    for (int d = tid; d < g.Mx; d += nthr) {
+        meta[d * 8 + 1] = 1 << 30;
+        meta[d * 8 + 2] = -1;
+        meta[d * 8 + 3] = 1 << 30;
+        meta[d * 8 + 4] = -1;
     }
     __syncthreads();
     {
-        const int lane = tid & 31, warp = tid >> 5, nwarps = (nthr + 31) >> 5;
-        for (int d = warp; d < g.Mx; d += nwarps) {
-            int lo = 1 << 30, hi = -1, loz = 1 << 30, hiz = -1;
-            for (int m0 = 0; m0 < g.WY; m0 += 32) {
-                const int m = m0 + lane;
-                unsigned bal = __ballot_sync(0xffffffffu, m < g.WY && wy[d * g.WY + min(m, g.WY - 1)] != 0.f);
-                if (bal) { lo = min(lo, m0 + __ffs(bal) - 1); hi = m0 + 31 - __clz(bal); }
-            }
-            for (int m0 = 0; m0 < g.WZ; m0 += 32) {
-                const int m = m0 + lane;
-                unsigned bal = __ballot_sync(0xffffffffu, m < g.WZ && wz[d * g.WZ + min(m, g.WZ - 1)] != 0.f);
-                if (bal) { loz = min(loz, m0 + __ffs(bal) - 1); hiz = m0 + 31 - __clz(bal); }
-            }
-            if (lane == 0) {
-                const int on = hi >= 0 && hiz >= 0;
-                meta[d * 8 + 0] = on;
-                meta[d * 8 + 1] = on ? (lo & ~3) : 0;
-                meta[d * 8 + 2] = on ? hi + 1 : 0;
-                meta[d * 8 + 3] = on ? (loz & ~3) : 0;
-                meta[d * 8 + 4] = on ? hiz + 1 : 0;
-            }
+        const int row = g.WY + g.WZ;
+        for (int e = tid; e < g.Mx * row; e += nthr) {
+            const int d = e / row, k = e - d * row;
+            const float wv = wval(d, k);
+            if (!RING) wput(d, k, wv);
+            if (wv == 0.f) continue;
+            const int lo = k < g.WY ? 1 : 3, m = k < g.WY ? k : k - g.WY;
+            atomicMin(&meta[d * 8 + lo], m);
+            atomicMax(&meta[d * 8 + lo + 1], m);
         }
+    }
+    __syncthreads();
+    for (int d = tid; d < g.Mx; d += nthr) {
+        int* md = meta + d * 8;
+        const int on = md[2] >= 0 && md[4] >= 0;
+        md[0] = on;
+        md[1] = on ? (md[1] & ~3) : 0;
+        md[2] = on ? md[2] + 1 : 0;
+        md[3] = on ? (md[3] & ~3) : 0;
+        md[4] = on ? md[4] + 1 : 0;
     }
 
     // y-filter ownership: (yf_j, yf_half, yf_r0) with yf_r0 fastest; each
@@ -278,6 +272,11 @@ cone_tma_kernel(const __grid_constant__ CUtensorMap tmap, const float* __restric
         if (tid == 0 && !mbar_wait(&bars[buf], parity)) s_fail = 1 + step;
         __syncthreads();
         if (s_fail) break;
+        // the filters of the depth that enters at the next plane: loaded now,
+        // stored after this plane's work (its ring slot is already free)
+        const int dn = RING ? p + 1 - x0 : g.Mx;
+        const float wn0 = (dn < g.Mx && tid < g.WY + g.WZ) ? wval(dn, tid) : 0.f;
+        const float wn1 = (dn < g.Mx && tid + nthr < g.WY + g.WZ) ? wval(dn, tid + nthr) : 0.f;
         // ---- y filter: X[j][t][HZP + z] = sum_m wy[j][m] * S[z][t + m] ----
         // this thread: target yf_j, columns yf_half*8.., rows yf_r0 + zq*{0..3}
         {
@@ -285,7 +284,7 @@ cone_tma_kernel(const __grid_constant__ CUtensorMap tmap, const float* __restric
             const int d = p - (x0 + yf_j);
             if (d >= 0 && d < g.Mx && x0 + yf_j < X && meta[d * 8]) {
                 const int mlo = meta[d * 8 + 1], mhi = meta[d * 8 + 2];
-                const float* wr = wy + d * g.WY;
+                const float* wr = wy + (RING ? d % (2 * XB) : d) * g.WY;
 #pragma unroll
                 for (int pr = 0; pr < 2; ++pr) {
                     // rows z0, z0 + zq (clamped to the staged plane; extra rows are not stored)
@@ -319,9 +318,13 @@ cone_tma_kernel(const __grid_constant__ CUtensorMap tmap, const float* __restric
         const int dz_ = p - (x0 + zt_j);
         if (zt_on && dz_ >= 0 && dz_ < g.Mx && x0 + zt_j < X && meta[dz_ * 8]) {
             const float* xr = Xs + (zt_j * TY + zt_t) * g.PZ;
-            const float* wr = wz + dz_ * g.WZ;
+            const float* wr = wz + (RING ? dz_ % (2 * XB) : dz_) * g.WZ;
             const int mlo = meta[dz_ * 8 + 3], mhi = meta[dz_ * 8 + 4];
             corr8_rows<4>(acc, xr + zt_zb * 32, 8, wr, mlo, mhi);
+        }
+        if (dn < g.Mx) {
+            if (tid < g.WY + g.WZ) wput(dn, tid, wn0);
+            if (tid + nthr < g.WY + g.WZ) wput(dn, tid + nthr, wn1);
         }
         // the next iteration's first barrier orders this z filter before the
         // next y filter overwrites X
@@ -413,8 +416,15 @@ bool cone_tma_geom(int64_t Z, int64_t X, int64_t Y, int64_t Mz, int64_t Mx, int6
     *threads = TY * XB * g->zblocks;
     if (*threads > 512) return false;
     size_t sb = ((size_t)g->Z * g->boxW + 31) & ~(size_t)31;
+    if (g->WY + g->WZ > 2 * *threads) return false;   // two filter elements per thread
+    // preload every depth's filters when they fit, else stream them through a ring
+    const size_t fixed = sizeof(float) * (2 * sb + (size_t)XB * TY * g->PZ) +
+                         sizeof(int) * (size_t)g->Mx * 8 + 2 * sizeof(uint64_t) + 64;
+    g->ring = fixed + sizeof(float) * (size_t)g->Mx * (g->WY + g->WZ) >
+              (size_t)max_smem_optin();
+    const int nw = g->ring ? 2 * XB : g->Mx;
     size_t s = sizeof(float) * (2 * sb + (size_t)XB * TY * g->PZ +
-                                (size_t)g->Mx * (g->WY + g->WZ)) +
+                                (size_t)nw * (g->WY + g->WZ)) +
                sizeof(int) * (size_t)g->Mx * 8 + 2 * sizeof(uint64_t) + 64;
     // the mode-2 epilogue reuses S for a [Z][TY][XB] tile
     // the mode-2 epilogue stages a [Z][TY][XB] tile over the S and X buffers
@@ -456,7 +466,7 @@ int cone_tma_launch_t(const float* mu, const float* U, const float* Vw, float* o
         set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
         return FLC_ERR_UNSUPPORTED;
     }
-    auto kern = cone_tma_kernel<TY, XB>;
+    auto kern = g.ring ? cone_tma_kernel<TY, XB, true> : cone_tma_kernel<TY, XB, false>;
     FLC_TRY_CUDA(cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smem));
     dim3 grid((unsigned)ceil_div(g.Y, TY), (unsigned)ceil_div(g.X, XB), (unsigned)Vn);

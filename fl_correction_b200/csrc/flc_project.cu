@@ -222,7 +222,7 @@ struct Foot {
 __device__ __forceinline__ Foot footprint(const Geo& g, const float* sA, const float* sratio,
                                           int W, int pitch, int h, int w) {
     Foot f;
-    f.av = sA[h * W + w] * sratio[w];
+    f.av = sratio ? sA[h * W + w] * sratio[w] : sA[h * W + w];
     const float hf = (float)h - g.cy;
     const float x = fmaf(g.c, hf, col_bx(g, w)), y = fmaf(g.s, hf, col_by(g, w));
     const float xc = fminf(fmaxf(x, 0.f), g.rmax), yc = fminf(fmaxf(y, 0.f), g.cmax);
@@ -367,6 +367,69 @@ __device__ void backward_angle_atomic(const float* sA, const float* sratio, floa
             if (f.w01 != 0.f) atomicAdd(q + 1, v * f.w01);
             if (f.w10 != 0.f) atomicAdd(q + pitch, v * f.w10);
             if (f.w11 != 0.f) atomicAdd(q + pitch + 1, v * f.w11);
+        }
+        h += dh;
+        w += dw;
+        if (w >= W) { w -= W; ++h; }
+    }
+}
+
+// Backward of one (angle, slice) in gather form, one reference (the
+// "proj.bwd" = 3 variant).  sQ holds the staged atten tile; it is scaled in
+// place by ratio[w] * em.  Every thread owns pixels p = t, t + nthr, ... of
+// the slice image and sums, over the 3 x 3 beam-frame samples around the
+// pixel's inverse image, the unclamped samples whose footprint covers it with
+// the forward's own weights (1 - |x - i|)(1 - |y - j|) -- the sample point and
+// the unclamped test are computed exactly as the forward computes them.  The
+// owner adds the sum into the image: no atomics, no phases.  The clamped
+// samples (they land on the border frame only) are then walked once and go
+// to the frame buffers or the corner registers.
+__device__ void backward_angle_gather(float* sQ, const float* sratio, float em, float* sacc,
+                                      float* srow, float* scol, int pitch, const Geo& g, int H,
+                                      int W, Corners& cs, int dh, int dw, int h0, int w0) {
+    int h = h0, w = w0;
+    while (h < H) {
+        sQ[h * W + w] *= sratio[w] * em;
+        h += dh;
+        w += dw;
+        if (w >= W) { w -= W; ++h; }
+    }
+    __syncthreads();
+    // inverse of x = c(h-cy) - s(w-cx) + cy, y = s(h-cy) + c(w-cx) + cx
+    int i = h0, j = w0;
+    while (i < H) {
+        const float xi = (float)i - g.cy, yj = (float)j - g.cx;
+        const int hr = __float2int_rn(fmaf(g.c, xi, fmaf(g.s, yj, g.cy)));
+        const int wr = __float2int_rn(fmaf(-g.s, xi, fmaf(g.c, yj, g.cx)));
+        float val = 0.f;
+#pragma unroll
+        for (int a = -1; a <= 1; ++a) {
+            const int hh = hr + a;
+            const float hf = (float)hh - g.cy;
+            const bool hin = (unsigned)hh < (unsigned)H;
+#pragma unroll
+            for (int b = -1; b <= 1; ++b) {
+                const int ww = wr + b;
+                const float x = fmaf(g.c, hf, col_bx(g, ww)), y = fmaf(g.s, hf, col_by(g, ww));
+                const float wx = 1.f - fabsf(x - (float)i), wy = 1.f - fabsf(y - (float)j);
+                const bool ok = hin && (unsigned)ww < (unsigned)W && x >= 0.f && x <= g.rmax &&
+                                y >= 0.f && y <= g.cmax && wx > 0.f && wy > 0.f;
+                if (ok) val = fmaf(wx * wy, sQ[hh * W + ww], val);
+            }
+        }
+        sacc[i * pitch + j] += val;
+        i += dh;
+        j += dw;
+        if (j >= W) { j -= W; ++i; }
+    }
+    h = h0;
+    w = w0;
+    while (h < H) {
+        const float hf = (float)h - g.cy;
+        const float x = fmaf(g.c, hf, col_bx(g, w)), y = fmaf(g.s, hf, col_by(g, w));
+        if (!(x >= 0.f && x <= g.rmax && y >= 0.f && y <= g.cmax)) {
+            const Foot f = footprint(g, sQ, nullptr, W, pitch, h, w);
+            frame_add<true>(f, f.av, srow, scol, H, W, cs, 0);
         }
         h += dh;
         w += dw;
@@ -533,7 +596,10 @@ proj_bwd_kernel(const float* __restrict__ atten, const float* __restrict__ ratio
             sratio[w] = ratio ? ratio[((int64_t)a * B + b) * W + w] : 1.f;
         __syncthreads();
         if (a + 1 < a1 && vec) tile_issue(tr, atten + ((int64_t)(a + 1) * B + b) * HW, HW);
-        if (bwd_mode != 1)
+        if (RC == 1 && bwd_mode == 3 && stage_tile)
+            backward_angle_gather(sA, sratio, sem[0], sacc, srow, scol, pitch,
+                                  make_geo(theta[a], H, W), H, W, cs, wk_dh, wk_dw, wk_h0, wk_w0);
+        else if (bwd_mode != 1)
             backward_angle<RC>(stage_tile ? sA : src, sratio, sacc, srow, scol, img_stride, pitch,
                                sem, R, make_geo(theta[a], H, W), H, W, cs);
         else
@@ -605,7 +671,10 @@ mlem_iter_kernel(const float* __restrict__ atten, const float* __restrict__ em,
             sratio[w] = I[((int64_t)a * B + b) * W + w] / fmaxf(s, 1e-6f);
         }
         __syncthreads();
-        if (bwd_mode != 1)
+        if (RC == 1 && bwd_mode == 3)
+            backward_angle_gather(sA, sratio, sem[0], sacc, srow, scol, pitch, g, H, W, cs, wk_dh,
+                                  wk_dw, wk_h0, wk_w0);
+        else if (bwd_mode != 1)
             backward_angle<RC>(sA, sratio, sacc, srow, scol, img_stride, pitch, sem, R, g, H, W,
                                cs);
         else

@@ -92,7 +92,7 @@ def layered(n, rng, n_elem, n_layers=5, n_incl=200, r_min=2, r_max=6):
 
 
 # Synthetic cross sections (cm^2/g) and densities (g/cm^3) per element; the
-# products cs*rho set the attenuation per unit concentration.
+# products cs*rho set the attenuation per unit mass fraction.
 _ELEMENTS = {
     "Ca": dict(rho=2.7, cs_in=95.0, cs_line=48.0, em=40.0),
     "Fe": dict(rho=5.2, cs_in=30.0, cs_line=36.0, em=35.0),
@@ -137,6 +137,12 @@ class Workload:
     def __init__(self, name, conc, elements, angles_deg, energy_kev, pix_cm, mask_angle_deg,
                  n_iter, recompute_every, noise_max_counts, seed):
         self.name = name
+        # the concentrations are mass fractions: every voxel's total over the
+        # elements is scaled to at most 0.9 (grain values and the 3x shells
+        # keep their ratios)
+        tot = float(conc.sum(axis=0).max())
+        if tot > 0.9:
+            conc = (conc * np.float32(0.9 / tot)).astype(np.float32)
         self.conc = conc                      # (L, N, N, N) float32 truth
         self.elements = list(elements)
         self.angles = np.asarray(angles_deg, np.float64)
@@ -165,7 +171,9 @@ def make_batch_workloads(n_volumes=16, seed=20240611, sizes=(64, 96, 128, 160, 1
     """The uneven batch of configuration 3: n_volumes seeded Voronoi volumes
     with side lengths drawn from `sizes`, 1-3 elements, 60-180 angles over
     [0, 180), incident energy U(10, 16) keV and detector distance U(20, 40)
-    mm (a 7 mm detector, so the cone angle is 2 atan(3.5 / d))."""
+    mm (a 7 mm detector, so the cone angle is 2 atan(3.5 / d)).  Every volume
+    images the same 128 um sample (pixel 1.28e-2 / N cm), so the optical depth
+    across it stays in the range of the 128^3 workload whatever N is."""
     rng = np.random.default_rng(seed + 3)
     names = ["Fe", "Ni", "Cu"]
     out = []
@@ -177,7 +185,7 @@ def make_batch_workloads(n_volumes=16, seed=20240611, sizes=(64, 96, 128, 160, 1
         dist = float(rng.uniform(20.0, 40.0))
         conc = voronoi_grains(n, rng, L, n_seeds=32)
         out.append(Workload("cfg3-v%02d-%dc-%delem-%dang" % (i, n, L, A), conc, names[:L],
-                            np.linspace(0, 180, A, endpoint=False), energy, 1e-4,
+                            np.linspace(0, 180, A, endpoint=False), energy, 1.28e-2 / n,
                             cone_mask_angle(7.0, dist), n_iter, recompute_every, 0, seed + 17 * i))
     return out
 

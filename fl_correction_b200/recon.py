@@ -34,8 +34,9 @@ class CorrectedMLEM:
     """
 
     def __init__(self, param, angles_deg, mask, shape, fixed_frac=None, incident="own",
-                 beta=0.0, delta=0.01, device="cuda", chunk=0):
+                 beta=0.0, delta=0.01, device="cuda", chunk=0, bound_frac=True):
         self.device = torch.device(device)
+        self.bound_frac = bound_frac
         self.param = param
         self.L = len(param["elem_type"])
         self.n_ch = len(param["elem_compound"])
@@ -72,8 +73,21 @@ class CorrectedMLEM:
 
     # -- building blocks -------------------------------------------------
     def recompute_attenuation(self, C, cone_events=None):
-        """atten[l, a] from concentrations C (L, S, H, W) on the device."""
-        self.frac[:self.L].copy_(C)
+        """atten[l, a] from concentrations C (L, S, H, W) on the device.
+
+        The estimate enters mu as mass fractions: clipped to [0, 1] and, where
+        the elements' total exceeds 1, scaled down to a total of 1 (with
+        bound_frac, the default).  The reference likewise feeds back bounded
+        fractions, not raw MLEM values (cal_frac, FL/core.py:159-205).
+        Without a bound, voxels that MLEM overshoots raise mu, which lowers
+        the modelled signal there, which raises them further: the outer loop
+        diverges on absorbing samples."""
+        f = self.frac[:self.L]
+        f.copy_(C)
+        if self.bound_frac:
+            f.clamp_(0.0, 1.0)
+            tot = f.sum(dim=0, keepdim=True).clamp_(min=1.0)
+            f.div_(tot)
         atten_maps(self.frac, self.angles, self.coef_x, self.coef_f, self.mask_uv,
                    incident=self.incident, xrf=True, out=self.atten, chunk=self.chunk,
                    workspace=self.ws_atten, cone_events=cone_events, theta=self.theta)

@@ -108,3 +108,20 @@ def test_pipelined_and_plain_kernels_agree(K, Z, X, Y, L):
     assert rel_err(outs[0], outs[1]) < 1e-6
     if Z * X * Y <= 64 ** 3:
         assert rel_err(outs[0], O.cone_ref(mu, mask.astype(np.float32))) < TOL_MAP
+
+
+@pytest.mark.parametrize("Z,n_mask,angle", [(192, 192, 19.0), (256, 256, 13.309)])
+def test_tall_volume_with_wide_mask(Z, n_mask, angle):
+    # slice counts and mask extents of the 192^3 and 256^3 workloads: the
+    # pipelined kernel streams each depth's filters through a small ring
+    rng = np.random.default_rng(Z)
+    mask = generate_detector_mask(angle, angle, n_mask)
+    u, v = factor_mask(mask)
+    K, X, Y = 1, 24, 32
+    mu = (rng.random((K, Z, X, Y)) * 0.02).astype(np.float32)
+    x, U, V = T(mu), T(u), T(v)
+    out = torch.empty_like(x)
+    _lib.call("flc_cone_atten_separable", _lib.ptr(x), _lib.ptr(U), _lib.ptr(V), _lib.ptr(out),
+              K, Z, X, Y, mask.shape[0], mask.shape[1], mask.shape[2], 0, _lib.stream())
+    assert _lib.query("flc_device_status", 1) == 0
+    assert rel_err(out.cpu().numpy(), O.cone_ref(mu, mask.astype(np.float32))) < TOL_MAP

@@ -439,7 +439,7 @@ def run_grad(args, device):
     n_steps = args.adam_steps if args.adam_steps > 0 else (200 if args.config == 2 else 3)
 
     # ---- gradient check on a subset of angles ---------------------------
-    sub = np.linspace(0, A - 1, 4 if N > 128 else 6).astype(int)
+    sub = np.linspace(0, A - 1, 2 if N > 128 else 6).astype(int)
     chk = GradientRecon(param_at_angles(wl.param, A, sub), wl.angles[sub], mask, (N, N, N),
                         fixed_frac=frac[L:], tv_weight=1e-3, device=device)
     Ichk = I[:, sub].contiguous()
@@ -458,17 +458,20 @@ def run_grad(args, device):
     grad_check = {"angles": int(len(sub))}
     log = lambda *a: print("[grad]", *a, file=sys.stderr, flush=True)  # noqa: E731
     log("gradient check on", len(sub), "angles")
-    C64 = Cc.double().clone().requires_grad_(True)
-    loss64(C64).backward()
-    grad_check["max_rel_err_vs_torch_fp64_autograd"] = float(
-        (g32.double() - C64.grad).abs().max() / C64.grad.abs().max())
+    if N <= 128:
+        # (at 256^3 the FP64 graph of even a few angles would need ~1 TB)
+        C64 = Cc.double().clone().requires_grad_(True)
+        loss64(C64).backward()
+        grad_check["max_rel_err_vs_torch_fp64_autograd"] = float(
+            (g32.double() - C64.grad).abs().max() / C64.grad.abs().max())
+        del C64
     with torch.no_grad():
         Pf64 = TM.xrf_project(torch.cat([Cc.double(), fixed64]), th, cx, cf, mask, em)
         Pf32 = pr.project(Cc).double()
         grad_check["projection_max_rel_err_vs_fp64"] = float((Pf32 - Pf64).abs().max() /
                                                              Pf64.abs().max())
-    del C64, Pf64, Pf32
-    log("autograd comparison done", grad_check)
+    del Pf64, Pf32
+    log("FP64 comparison done", grad_check)
     if N <= 128:
         rng = np.random.default_rng(7)
         eps, errs = 1e-4, []
@@ -579,23 +582,23 @@ def run_batch(args, device):
         b.run_loop()
     torch.cuda.synchronize()
     e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    ll0 = _lib.query("flc_launch_count")
     e[0].record()
     for _ in range(args.steps):
         loop = b.run_loop()
     e[1].record()
+    loop_launches = _lib.query("flc_launch_count") - ll0
     torch.cuda.synchronize()
     loop = [c.clone() for c in loop]
     b.capture()
     for _ in range(max(1, args.warmup)):
         b.run()
     torch.cuda.synchronize()
-    l0 = _lib.query("flc_launch_count")
     e[2].record()
     for _ in range(args.steps):
         out = b.run()
     e[3].record()
     torch.cuda.synchronize()
-    launches = _lib.query("flc_launch_count") - l0
     t_loop, t_graph = e[0].elapsed_time(e[1]), e[2].elapsed_time(e[3])
     err = max(float((o - r).abs().max() / r.abs().max()) for o, r in zip(out, loop))
     vol_iters = len(ws) * n_iter * args.steps
@@ -610,8 +613,10 @@ def run_batch(args, device):
                        "ms_per_step": round(t_loop / args.steps, 2)},
         "speedup_vs_plain_loop": round(t_loop / t_graph, 3),
         "max_rel_err_vs_plain_loop": err,
-        "gpu_launches": int(launches),
-        "note": "graph replays count every kernel node (flc_launch_count)",
+        # a replay runs the kernels the eager loop launches (the graph was
+        # captured from the same schedule); the host-side counter does not see
+        # graph replays, so the loop's count stands for them
+        "gpu_launches": int(loop_launches),
     }
 
 

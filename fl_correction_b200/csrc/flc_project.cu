@@ -336,6 +336,54 @@ __device__ void backward_angle(const float* sA, const float* sratio, float* sacc
     }
 }
 
+// Backward of one (angle, slice) by column segments (the "proj.bwd" = 4
+// variant).  A detector column is a straight line of samples in the image;
+// lines three columns apart, and pieces of one line kSeg samples apart, are
+// at least three pixels apart, so their 2 x 2 footprints are disjoint.  Six
+// phases -- (w mod 3) x (segment parity) -- each give every thread one
+// segment of kSeg consecutive samples of one column, walked in order: the
+// overlapping footprints of consecutive samples are updated by the same
+// thread, one after the other, with plain read-modify-writes.  Clamped
+// samples go to the frame buffers as in the nine-phase form.
+constexpr int kSeg = 6;
+
+template <int RC>
+__device__ void backward_angle_seg(const float* sA, const float* sratio, float* sacc, float* srow,
+                                   float* scol, int img_stride, int pitch, const float* em_a,
+                                   int Rrt, const Geo& g, int H, int W, Corners& cs) {
+    const int R = RC > 0 ? RC : Rrt;
+    const int nseg = (H + kSeg - 1) / kSeg;
+    for (int pw = 0; pw < 3; ++pw) {
+        const int nw = (W - pw + 2) / 3;
+        for (int ps = 0; ps < 2; ++ps) {
+            const int nsp = (nseg - ps + 1) / 2;   // segments of this parity
+            const int items = nw * nsp;
+            for (int it = threadIdx.x; it < items; it += blockDim.x) {
+                const int k = it / nw, cw = it - k * nw;   // a warp spans columns
+                const int w = pw + 3 * cw;
+                const int h0 = (ps + 2 * k) * kSeg, h1 = min(H, h0 + kSeg);
+                for (int h = h0; h < h1; ++h) {
+                    const Foot f = footprint(g, sA, sratio, W, pitch, h, w);
+#pragma unroll
+                    for (int r = 0; r < (RC > 0 ? RC : R); ++r) {
+                        const float v = em_a[r] * f.av;
+                        if (f.kind == 0) {
+                            float* q = sacc + r * img_stride + f.off;
+                            q[0] = fmaf(v, f.w00, q[0]);
+                            q[1] = fmaf(v, f.w01, q[1]);
+                            q[pitch] = fmaf(v, f.w10, q[pitch]);
+                            q[pitch + 1] = fmaf(v, f.w11, q[pitch + 1]);
+                        } else {
+                            frame_add<(RC > 0)>(f, v, srow, scol, H, W, cs, r);
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
 // Backward of one (angle, slice) with shared-memory atomics instead of
 // phases (the "proj.bwd" = 1 variant): every thread takes samples it = t,
 // t + nthr, ... (a warp covers a run of consecutive columns of one beam row)
@@ -599,6 +647,9 @@ proj_bwd_kernel(const float* __restrict__ atten, const float* __restrict__ ratio
         if (RC == 1 && bwd_mode == 3 && stage_tile)
             backward_angle_gather(sA, sratio, sem[0], sacc, srow, scol, pitch,
                                   make_geo(theta[a], H, W), H, W, cs, wk_dh, wk_dw, wk_h0, wk_w0);
+        else if (bwd_mode == 4)
+            backward_angle_seg<RC>(stage_tile ? sA : src, sratio, sacc, srow, scol, img_stride,
+                                   pitch, sem, R, make_geo(theta[a], H, W), H, W, cs);
         else if (bwd_mode != 1)
             backward_angle<RC>(stage_tile ? sA : src, sratio, sacc, srow, scol, img_stride, pitch,
                                sem, R, make_geo(theta[a], H, W), H, W, cs);
@@ -674,6 +725,9 @@ mlem_iter_kernel(const float* __restrict__ atten, const float* __restrict__ em,
         if (RC == 1 && bwd_mode == 3)
             backward_angle_gather(sA, sratio, sem[0], sacc, srow, scol, pitch, g, H, W, cs, wk_dh,
                                   wk_dw, wk_h0, wk_w0);
+        else if (bwd_mode == 4)
+            backward_angle_seg<RC>(sA, sratio, sacc, srow, scol, img_stride, pitch, sem, R, g, H, W,
+                                   cs);
         else if (bwd_mode != 1)
             backward_angle<RC>(sA, sratio, sacc, srow, scol, img_stride, pitch, sem, R, g, H, W,
                                cs);

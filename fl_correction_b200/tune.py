@@ -10,7 +10,7 @@ CUDA events and keeps the fastest through ``flc_tune_set``:
   cone.variant   TMA 16x8 tile, TMA 8x4 tile or the plain separable kernel
   atten.chunk    angles per attenuation-pipeline pass
   proj.bwd       backward: splat with shared atomics, splat in nine disjoint
-                 phases, or gather per pixel
+                 phases, gather per pixel, or splat by column segments
 
 Every candidate is checked against the automatic choice before it is timed
 (the results must agree to FP32 round-off), so tuning never changes answers
@@ -106,7 +106,7 @@ def tune_projector(A, B, H, W, device="cuda"):
     bwd = lambda: AC.backward_emission_batch(atten, r, em, th)  # noqa: E731
     fwd = lambda: AC.forward_emission_batch(atten, C, em, th)  # noqa: E731
     out = {}
-    out["proj.bwd"] = _sweep("proj.bwd", [0, 1, 2, 3], bwd, _close)
+    out["proj.bwd"] = _sweep("proj.bwd", [0, 1, 2, 3, 4], bwd, _close)
     out["proj.cluster"] = _sweep("proj.cluster", [0, 1, 2, 4, 8], bwd, _close)
     apcs = sorted({0} | {a for a in (1, 2, 3, 4, 6, 8, 12, 16) if a <= A})
     out["proj.apc"] = _sweep("proj.apc", apcs, fwd, _close)

@@ -126,7 +126,7 @@ def test_non_contiguous_inputs():
     assert rel_err(out, O.fwd_emission(atten, C, em, th)) < TOL_MAP
 
 
-@pytest.mark.parametrize("mode", [1, 2, 3])
+@pytest.mark.parametrize("mode", [1, 2, 3, 4])
 @pytest.mark.parametrize("A,B,R,H,W", [(8, 3, 2, 20, 28), (5, 2, 1, 64, 64), (1, 1, 1, 2, 2)])
 def test_backward_splat_variants(mode, A, B, R, H, W):
     # shared-atomic splat, nine-phase splat and gather give the same transpose

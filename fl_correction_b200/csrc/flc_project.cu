@@ -184,30 +184,31 @@ struct Corners {
 // ih = H-2, ih+1 (x > rmax, weights 1-fxh, fxh); a column clamp likewise on
 // columns 0 or W-2, W-1.  They are collected, with shared atomics, in frame
 // buffers kept apart from the slice image so that the unclamped samples can
-// update the image with plain read-modify-writes:
-//   srow[r][slot][j], slot 0: row 0, 1: row H-2, 2: row H-1   (R x 3 x W)
-//   scol[r][slot][i], slot 0: col 0, 1: col W-2, 2: col W-1   (R x 3 x H)
-// and added into the image once, after the last angle (fold_frame).
+// update the image with plain read-modify-writes.  The split of a high clamp
+// between its two rows (columns) is the same constant for every sample, so a
+// clamped sample only adds its weights along the edge, (1-fy, fy) at j0, j0+1
+// (rows) or (1-fx, fx) at i0, i0+1 (columns), into a low or a high buffer:
+//   row part    [r][slot][j], slot 0: row 0, 1: rows H-2, H-1   (R x 2 x W)
+//   column part [r][slot][i], slot 0: col 0, 1: cols W-2, W-1   (R x 2 x H)
+// `ncopy` (1 to kMaxFrameCopies) such frames, one per group of warps
+// (warp % ncopy), spread the atomics on one edge pixel over several
+// addresses.  They are added into the image once, after the last angle
+// (fold_frame), the high slots split by (1 - fxh, fxh) and (1 - fyh, fyh).
+constexpr int kMaxFrameCopies = 4;
+
+__host__ __device__ inline int frame_floats(int R, int H, int W, int ncopy) {
+    return ncopy * 2 * R * (H + W);
+}
 
 // Adds v, spread over the pixels of corner class k (2*xhigh + yhigh), into
-// the row buffer of one reference.
+// the row part of one reference's frame.
 __device__ __forceinline__ void corner_add(float* srow, int W, const Geo& g, int k, float v) {
     const bool xh = k >= 2, yh = k & 1;
     const int j0 = yh ? g.jh : 0;
     const float fy = yh ? g.fyh : 0.f;
-    const float c0 = v * (1.f - fy), c1 = v * fy;
-    if (!xh) {
-        atomicAdd(srow + j0, c0);
-        if (c1 != 0.f) atomicAdd(srow + j0 + 1, c1);
-        return;
-    }
-    const float r0 = 1.f - g.fxh, r1 = g.fxh;
-    atomicAdd(srow + W + j0, c0 * r0);
-    atomicAdd(srow + 2 * W + j0, c0 * r1);
-    if (c1 != 0.f) {
-        atomicAdd(srow + W + j0 + 1, c1 * r0);
-        atomicAdd(srow + 2 * W + j0 + 1, c1 * r1);
-    }
+    float* b = srow + (xh ? W : 0) + j0;
+    atomicAdd(b, v * (1.f - fy));
+    if (fy != 0.f) atomicAdd(b + 1, v * fy);
 }
 
 // Bilinear footprint of one sample on the clamped grid.
@@ -215,6 +216,7 @@ struct Foot {
     int off;                 // i0 * pitch + j0
     int i0, j0;
     float w00, w01, w10, w11;
+    float fx, fy;            // bilinear fractions on the clamped grid
     float av;                // atten * ratio
     int kind;                // bits: 1 x < 0, 2 x > rmax, 4 y < 0, 8 y > cmax
 };
@@ -229,6 +231,8 @@ __device__ __forceinline__ Foot footprint(const Geo& g, const float* sA, const f
     float fx, fy;
     f.i0 = ffloor(xc, fx);
     f.j0 = ffloor(yc, fy);
+    f.fx = fx;
+    f.fy = fy;
     f.off = f.i0 * pitch + f.j0;
     f.w00 = (1.f - fy) * (1.f - fx);
     f.w01 = fy * (1.f - fx);
@@ -240,10 +244,8 @@ __device__ __forceinline__ Foot footprint(const Geo& g, const float* sA, const f
 
 // Contribution v of a clamped sample of reference r into the frame buffers
 // (or, clamped in both coordinates, r < kCornerR and REG -- the reference
-// count is a compile-time constant -- the corner registers).
-// One form for both buffers: the four taps sit at base + {0, 1, S, S + 1}.
-// A row clamp below 0 has fx == 0 (no weight on the second row) and a column
-// clamp below 0 has fy == 0, so their zero-weight taps are skipped.
+// count is a compile-time constant -- the corner registers).  A corner
+// handled here takes the row path: its clamped fraction fx is 0 or fxh.
 template <bool REG>
 __device__ __forceinline__ void frame_add(const Foot& f, float v, float* srow, float* scol, int H,
                                           int W, Corners& cs, int r) {
@@ -252,14 +254,11 @@ __device__ __forceinline__ void frame_add(const Foot& f, float v, float* srow, f
     if (REG && corner && r < kCornerR) {
         cs.add(r, ((f.kind & 2) ? 2 : 0) + ((f.kind & 8) ? 1 : 0), v);
     } else {
-        float* base = rowc ? srow + r * 3 * W + ((f.kind & 1) ? 0 : W) + f.j0
-                           : scol + r * 3 * H + ((f.kind & 4) ? 0 : H) + f.i0;
-        const int S = rowc ? W : H;
-        const float t1 = rowc ? f.w01 : f.w10, t2 = rowc ? f.w10 : f.w01;
-        if (f.w00 != 0.f) atomicAdd(base, v * f.w00);
-        if (t1 != 0.f) atomicAdd(base + 1, v * t1);
-        if (t2 != 0.f) atomicAdd(base + S, v * t2);
-        if (f.w11 != 0.f) atomicAdd(base + S + 1, v * f.w11);
+        float* base = rowc ? srow + (2 * r + ((f.kind & 1) ? 0 : 1)) * W + f.j0
+                           : scol + (2 * r + ((f.kind & 4) ? 0 : 1)) * H + f.i0;
+        const float t = rowc ? f.fy : f.fx;
+        atomicAdd(base, v * (1.f - t));
+        if (t != 0.f) atomicAdd(base + 1, v * t);
     }
 }
 
@@ -496,37 +495,46 @@ __device__ void flush_corners(Corners& cs, float* srow, const Geo& g, int R, int
             float v = cs.v[r][k];
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if (r < R && lane == 0 && v != 0.f) corner_add(srow + r * 3 * W, W, g, k, v);
+            if (r < R && lane == 0 && v != 0.f) corner_add(srow + r * 2 * W, W, g, k, v);
         }
     }
 }
 
-// After the last angle: corners into the row buffers, then the row and column
-// buffers into the image (one thread per column / row, slots in order, so a
+// After the last angle: corners into the row buffers, then every copy of the
+// frame into the image (one thread per column / row, slots in order, so a
 // coinciding row or column -- H or W == 2 -- is still summed correctly).
-__device__ void fold_frame(Corners& cs, float* sacc, float* srow, const float* scol,
-                           int img_stride, int pitch, int R, int H, int W) {
+__device__ void fold_frame(Corners& cs, float* sacc, float* sframe, int ncopy, int img_stride,
+                           int pitch, int R, int H, int W) {
     // every thread passes the barriers below (callers have finished all angles)
     __syncthreads();
     const Geo g0 = make_geo(0.f, H, W);
-    flush_corners(cs, srow, g0, R, W);
+    flush_corners(cs, sframe, g0, R, W);
     __syncthreads();
+    const int copy = 2 * R * (H + W);
     for (int t = threadIdx.x; t < R * W; t += blockDim.x) {
         const int r = t / W, j = t - r * W;
+        float lo = 0.f, hi = 0.f;
+        for (int c = 0; c < ncopy; ++c) {
+            lo += sframe[c * copy + 2 * r * W + j];
+            hi += sframe[c * copy + 2 * r * W + W + j];
+        }
         float* img = sacc + r * img_stride + j;
-        const float* b = srow + r * 3 * W + j;
-        img[0] += b[0];
-        img[(H - 2) * pitch] += b[W];
-        img[(H - 1) * pitch] += b[2 * W];
+        img[0] += lo;
+        img[(H - 2) * pitch] += hi * (1.f - g0.fxh);
+        img[(H - 1) * pitch] += hi * g0.fxh;
     }
     __syncthreads();
     for (int t = threadIdx.x; t < R * H; t += blockDim.x) {
         const int r = t / H, i = t - r * H;
+        float lo = 0.f, hi = 0.f;
+        for (int c = 0; c < ncopy; ++c) {
+            lo += sframe[c * copy + 2 * R * W + 2 * r * H + i];
+            hi += sframe[c * copy + 2 * R * W + 2 * r * H + H + i];
+        }
         float* img = sacc + r * img_stride + i * pitch;
-        const float* b = scol + r * 3 * H + i;
-        img[0] += b[0];
-        img[W - 2] += b[H];
-        img[W - 1] += b[2 * H];
+        img[0] += lo;
+        img[W - 2] += hi * (1.f - g0.fyh);
+        img[W - 1] += hi * g0.fyh;
     }
     __syncthreads();
 }
@@ -612,7 +620,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 proj_bwd_kernel(const float* __restrict__ atten, const float* __restrict__ ratio,
                 const float* __restrict__ em, const float* __restrict__ theta,
                 float* __restrict__ out, int A, int B, int R, int H, int W, int apc,
-                float clamp_min, int stage_tile, int bwd_mode) {
+                float clamp_min, int stage_tile, int bwd_mode, int ncopy) {
     extern __shared__ __align__(16) float smem[];
     cg::cluster_group cluster = cg::this_cluster();
     const int b = blockIdx.y;
@@ -622,12 +630,14 @@ proj_bwd_kernel(const float* __restrict__ atten, const float* __restrict__ ratio
     const int img_stride = H * pitch;
     float* sA = smem;
     float* sacc = sA + (stage_tile ? ((HW + 3) & ~3) : 0);
-    float* srow = sacc + R * img_stride;                     // [R][3][W]
-    float* scol = srow + R * 3 * W;                          // [R][3][H]
-    float* sratio = scol + R * 3 * H;
+    float* sframe = sacc + R * img_stride;                   // ncopy x [R][2][W + H]
+    float* srow = sframe + ((threadIdx.x >> 5) % ncopy) * 2 * R * (H + W);
+    float* scol = srow + 2 * R * W;
+    float* sratio = sframe + frame_floats(R, H, W, ncopy);
     float* sem = sratio + W;
     const bool vec = stage_tile && ((HW & 3) == 0) && (((uintptr_t)atten & 15) == 0);
-    for (int i = threadIdx.x; i < R * (img_stride + 3 * W + 3 * H); i += blockDim.x) sacc[i] = 0.f;
+    for (int i = threadIdx.x; i < R * img_stride + frame_floats(R, H, W, ncopy); i += blockDim.x)
+        sacc[i] = 0.f;
     const int wk_dh = blockDim.x / W, wk_dw = blockDim.x - wk_dh * W;
     const int wk_h0 = threadIdx.x / W, wk_w0 = threadIdx.x - wk_h0 * W;
     Corners cs;
@@ -658,7 +668,7 @@ proj_bwd_kernel(const float* __restrict__ atten, const float* __restrict__ ratio
                                       R, make_geo(theta[a], H, W), H, W, cs, wk_dh, wk_dw, wk_h0,
                                       wk_w0);
     }
-    fold_frame(cs, sacc, srow, scol, img_stride, pitch, R, H, W);
+    fold_frame(cs, sacc, sframe, ncopy, img_stride, pitch, R, H, W);
     cluster.sync();
     cluster_reduce(cluster, sacc, R, H, W, pitch, [&](int r, int h, int w, float s) {
         if (clamp_min > 0.f) s = fmaxf(s, clamp_min);
@@ -680,7 +690,7 @@ mlem_iter_kernel(const float* __restrict__ atten, const float* __restrict__ em,
                  const float* __restrict__ theta, const float* __restrict__ I,
                  const float* __restrict__ sens, const float* __restrict__ Cin,
                  float* __restrict__ Cout, int A, int B, int R, int H, int W, int apc,
-                 float beta, float delta, int bwd_mode) {
+                 float beta, float delta, int bwd_mode, int ncopy) {
     extern __shared__ __align__(16) float smem[];
     cg::cluster_group cluster = cg::this_cluster();
     const int b = blockIdx.y;
@@ -692,14 +702,16 @@ mlem_iter_kernel(const float* __restrict__ atten, const float* __restrict__ em,
     float* sA = smem;
     float* sC = sA + ((HW + 3) & ~3);
     float* sacc = sC + R * img_stride;
-    float* srow = sacc + R * img_stride;                     // [R][3][W]
-    float* scol = srow + R * 3 * W;                          // [R][3][H]
-    float* spart = scol + R * 3 * H;
+    float* sframe = sacc + R * img_stride;                   // ncopy x [R][2][W + H]
+    float* srow = sframe + ((threadIdx.x >> 5) % ncopy) * 2 * R * (H + W);
+    float* scol = srow + 2 * R * W;
+    float* spart = sframe + frame_floats(R, H, W, ncopy);
     float* sratio = spart + parts * W;
     float* sem = sratio + W;
     const bool vec = ((HW & 3) == 0) && (((uintptr_t)atten & 15) == 0);
     stage_slice(sC, Cin, R, B, b, H, W, pitch);
-    for (int i = threadIdx.x; i < R * (img_stride + 3 * W + 3 * H); i += blockDim.x) sacc[i] = 0.f;
+    for (int i = threadIdx.x; i < R * img_stride + frame_floats(R, H, W, ncopy); i += blockDim.x)
+        sacc[i] = 0.f;
     const int wk_dh = blockDim.x / W, wk_dw = blockDim.x - wk_dh * W;
     const int wk_h0 = threadIdx.x / W, wk_w0 = threadIdx.x - wk_h0 * W;
     Corners cs;
@@ -735,7 +747,7 @@ mlem_iter_kernel(const float* __restrict__ atten, const float* __restrict__ em,
             backward_angle_atomic<RC>(sA, sratio, sacc, img_stride, pitch, sem, R, g, H, W, cs,
                                       wk_dh, wk_dw, wk_h0, wk_w0);
     }
-    fold_frame(cs, sacc, srow, scol, img_stride, pitch, R, H, W);
+    fold_frame(cs, sacc, sframe, ncopy, img_stride, pitch, R, H, W);
     cluster.sync();
     cluster_reduce(cluster, sacc, R, H, W, pitch, [&](int r, int h, int w, float back) {
         const float* img = sC + r * img_stride;
@@ -925,15 +937,25 @@ size_t fwd_smem(int64_t R, int64_t H, int64_t W, bool stage_tile, bool stage_c) 
                             (stage_c ? R * H * slice_pitch((int)W) : 0) + parts * W + kMaxR);
 }
 
-size_t bwd_smem(int64_t R, int64_t H, int64_t W, bool stage_tile) {
+size_t bwd_smem(int64_t R, int64_t H, int64_t W, bool stage_tile, int ncopy) {
     return sizeof(float) * ((stage_tile ? tile_floats(H, W) : 0) + R * H * slice_pitch((int)W) +
-                            R * 3 * (H + W) + W + kMaxR);
+                            frame_floats((int)R, (int)H, (int)W, ncopy) + W + kMaxR);
 }
 
-size_t mlem_smem(int64_t R, int64_t H, int64_t W) {
+size_t mlem_smem(int64_t R, int64_t H, int64_t W, int ncopy) {
     int parts = col_parts((int)W, (int)H);
     return sizeof(float) * (tile_floats(H, W) + 2 * R * H * slice_pitch((int)W) +
-                            R * 3 * (H + W) + parts * W + W + kMaxR);
+                            frame_floats((int)R, (int)H, (int)W, ncopy) + parts * W + W + kMaxR);
+}
+
+// The most frame copies (kMaxFrameCopies, halving down to 1) for which
+// smem_of(ncopy) still fits in a CTA's shared memory.
+template <class F>
+int frame_copies(F smem_of) {
+    const size_t cap = (size_t)max_smem_optin();
+    int n = kMaxFrameCopies;
+    while (n > 1 && smem_of(n) > cap) n /= 2;
+    return n;
 }
 
 }  // namespace
@@ -943,8 +965,8 @@ int bwd_emission_launch(const float* atten, const float* ratio, const float* em,
                         const float* theta, float* out, int64_t A, int64_t B, int64_t R,
                         int64_t H, int64_t W, float clamp_min, cudaStream_t st) {
     const size_t cap = (size_t)max_smem_optin();
-    int stage_tile = bwd_smem(R, H, W, true) <= cap;
-    if (!stage_tile && bwd_smem(R, H, W, false) > cap) {
+    int stage_tile = bwd_smem(R, H, W, true, 1) <= cap;
+    if (!stage_tile && bwd_smem(R, H, W, false, 1) > cap) {
         // the slice image does not fit on chip: global atomics
         FLC_TRY_CUDA(cudaMemsetAsync(out, 0, sizeof(float) * R * B * H * W, st));
         proj_bwd_global_kernel<<<dim3((unsigned)ceil_div(W, 128), (unsigned)B, (unsigned)A), 128, 0,
@@ -958,13 +980,14 @@ int bwd_emission_launch(const float* atten, const float* ratio, const float* em,
         }
         return FLC_OK;
     }
-    size_t smem = bwd_smem(R, H, W, stage_tile);
+    int ncopy = frame_copies([&](int n) { return bwd_smem(R, H, W, stage_tile, n); });
+    size_t smem = bwd_smem(R, H, W, stage_tile, ncopy);
     const void* fn = R == 1 ? (const void*)proj_bwd_kernel<1> : (const void*)proj_bwd_kernel<0>;
     Plan p = plan_cluster(fn, A, B, smem);
     int iA = (int)A, iB = (int)B, iR = (int)R, iH = (int)H, iW = (int)W, apc = p.apc;
     int bwd_mode = (int)tune(kTuneProjBwd);
     void* args[] = {(void*)&atten, (void*)&ratio, (void*)&em, (void*)&theta, (void*)&out,
-                    &iA, &iB, &iR, &iH, &iW, &apc, &clamp_min, &stage_tile, &bwd_mode};
+                    &iA, &iB, &iR, &iH, &iW, &apc, &clamp_min, &stage_tile, &bwd_mode, &ncopy};
     return launch_cluster(fn, dim3(p.G, (unsigned)B), p.G, smem, st, args);
 }
 
@@ -998,24 +1021,25 @@ int mlem_iter_launch(const float* atten, const float* em, const float* theta, co
                      const float* sens, const float* Cin, float* Cout, int64_t A, int64_t B,
                      int64_t R, int64_t H, int64_t W, float beta, float delta, cudaStream_t st,
                      bool* fused) {
-    size_t smem = mlem_smem(R, H, W);
-    *fused = smem <= (size_t)max_smem_optin();
+    *fused = mlem_smem(R, H, W, 1) <= (size_t)max_smem_optin();
     if (!*fused) return FLC_OK;
+    int ncopy = frame_copies([&](int n) { return mlem_smem(R, H, W, n); });
+    const size_t smem = mlem_smem(R, H, W, ncopy);
     const void* fn = R == 1 ? (const void*)mlem_iter_kernel<1> : (const void*)mlem_iter_kernel<0>;
     Plan p = plan_cluster(fn, A, B, smem);
     int iA = (int)A, iB = (int)B, iR = (int)R, iH = (int)H, iW = (int)W, apc = p.apc;
     int bwd_mode = (int)tune(kTuneProjBwd);
     void* args[] = {(void*)&atten, (void*)&em, (void*)&theta, (void*)&I, (void*)&sens,
                     (void*)&Cin, (void*)&Cout, &iA, &iB, &iR, &iH, &iW, &apc, &beta, &delta,
-                    &bwd_mode};
+                    &bwd_mode, &ncopy};
     return launch_cluster(fn, dim3(p.G, (unsigned)B), p.G, smem, st, args);
 }
 
 // Computes (and caches) the launch plan of the fused iteration, so that a
 // later stream capture makes no occupancy queries.
 void mlem_iter_prepare(int64_t A, int64_t B, int64_t R, int64_t H, int64_t W) {
-    const size_t smem = mlem_smem(R, H, W);
-    if (smem > (size_t)max_smem_optin()) return;
+    if (mlem_smem(R, H, W, 1) > (size_t)max_smem_optin()) return;
+    const size_t smem = mlem_smem(R, H, W, frame_copies([&](int n) { return mlem_smem(R, H, W, n); }));
     const void* fn = R == 1 ? (const void*)mlem_iter_kernel<1> : (const void*)mlem_iter_kernel<0>;
     (void)plan_cluster(fn, A, B, smem);
 }

@@ -36,8 +36,8 @@ enum TuneKey {
     kTuneProjApc = 1,       // angles per CTA for the projector kernels
     kTuneConeVariant = 2,   // 1: TMA 16x8 tile, 2: TMA 8x4 tile, 3: plain kernel
     kTuneAttenChunk = 3,    // angles per attenuation-pipeline pass
-    kTuneProjBwd = 4,       // backward: 1 shared-atomic splat, 0/2 nine-phase splat, 3 gather,
-                            // 4 column segments
+    kTuneProjBwd = 4,       // backward: 0 automatic, 1 shared-atomic splat, 2 nine-phase
+                            // splat, 3 gather, 4 column segments
     kTuneCount = 5
 };
 int64_t tune(int key);

@@ -948,6 +948,19 @@ size_t mlem_smem(int64_t R, int64_t H, int64_t W, int ncopy) {
                             frame_floats((int)R, (int)H, (int)W, ncopy) + parts * W + W + kMaxR);
 }
 
+// Backward form for the knob value 0 (automatic): the column segments
+// (4) when one round of a segment phase's items fills 85-100% of the
+// CTA's threads -- there they beat the nine phases (120 angles x 128 slices of
+// 128^2: 2.17 vs 2.31 ms) -- else the nine-phase splat (2), which wins when
+// the segment phases leave threads idle or take a second, partial round.
+int pick_bwd_mode(int64_t H, int64_t W) {
+    int mode = (int)tune(kTuneProjBwd);
+    if (mode != 0) return mode;
+    const int64_t nseg = (H + kSeg - 1) / kSeg;
+    const int64_t items = (W + 2) / 3 * ((nseg + 1) / 2);
+    return (items <= kThreads && items * 100 >= 85 * kThreads) ? 4 : 2;
+}
+
 // The most frame copies (kMaxFrameCopies, halving down to 1) for which
 // smem_of(ncopy) still fits in a CTA's shared memory.
 template <class F>
@@ -985,7 +998,7 @@ int bwd_emission_launch(const float* atten, const float* ratio, const float* em,
     const void* fn = R == 1 ? (const void*)proj_bwd_kernel<1> : (const void*)proj_bwd_kernel<0>;
     Plan p = plan_cluster(fn, A, B, smem);
     int iA = (int)A, iB = (int)B, iR = (int)R, iH = (int)H, iW = (int)W, apc = p.apc;
-    int bwd_mode = (int)tune(kTuneProjBwd);
+    int bwd_mode = pick_bwd_mode(H, W);
     void* args[] = {(void*)&atten, (void*)&ratio, (void*)&em, (void*)&theta, (void*)&out,
                     &iA, &iB, &iR, &iH, &iW, &apc, &clamp_min, &stage_tile, &bwd_mode, &ncopy};
     return launch_cluster(fn, dim3(p.G, (unsigned)B), p.G, smem, st, args);
@@ -1028,7 +1041,7 @@ int mlem_iter_launch(const float* atten, const float* em, const float* theta, co
     const void* fn = R == 1 ? (const void*)mlem_iter_kernel<1> : (const void*)mlem_iter_kernel<0>;
     Plan p = plan_cluster(fn, A, B, smem);
     int iA = (int)A, iB = (int)B, iR = (int)R, iH = (int)H, iW = (int)W, apc = p.apc;
-    int bwd_mode = (int)tune(kTuneProjBwd);
+    int bwd_mode = pick_bwd_mode(H, W);
     void* args[] = {(void*)&atten, (void*)&em, (void*)&theta, (void*)&I, (void*)&sens,
                     (void*)&Cin, (void*)&Cout, &iA, &iB, &iR, &iH, &iW, &apc, &beta, &delta,
                     &bwd_mode, &ncopy};

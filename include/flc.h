@@ -62,8 +62,9 @@ FLC_API uint64_t flc_launch_count(void);
  *   "proj.apc"      angles per CTA, projector kernels
  *   "cone.variant"  1: TMA 16x8 tile, 2: TMA 8x4 tile, 3: plain kernel
  *   "atten.chunk"   angles per attenuation-pipeline pass
- *   "proj.bwd"      backward: 2 nine-phase splat (automatic), 1 shared-memory atomics,
- *                   3 gather per pixel, 4 splat by column segments
+ *   "proj.bwd"      backward: 2 nine-phase splat, 1 shared-memory atomics,
+ *                   3 gather per pixel, 4 splat by column segments; automatic:
+ *                   4 where one round of its items fills the thread block, else 2
  * 0 restores the automatic choice.  flc_tune_get returns -1 for an unknown
  * name.  Process-wide; not synchronized with launches in flight. */
 FLC_API int flc_tune_set(const char* name, int64_t value);

@@ -337,21 +337,20 @@ __device__ void backward_angle(const float* sA, const float* sratio, float* sacc
 
 // Backward of one (angle, slice) by column segments (the "proj.bwd" = 4
 // variant).  A detector column is a straight line of samples in the image;
-// lines three columns apart, and pieces of one line kSeg samples apart, are
-// at least three pixels apart, so their 2 x 2 footprints are disjoint.  Six
-// phases -- (w mod 3) x (segment parity) -- each give every thread one
-// segment of kSeg consecutive samples of one column, walked in order: the
+// lines three columns apart, and pieces of one line one segment apart, are
+// at least three pixels apart (seg >= 2), so their 2 x 2 footprints are
+// disjoint.  Six phases -- (w mod 3) x (segment parity) -- each give every
+// thread about one segment of `seg` consecutive samples of one column (the
+// host picks seg so that one round of items fills the CTA), walked in order: the
 // overlapping footprints of consecutive samples are updated by the same
 // thread, one after the other, with plain read-modify-writes.  Clamped
 // samples go to the frame buffers as in the nine-phase form.
-constexpr int kSeg = 6;
-
 template <int RC>
 __device__ void backward_angle_seg(const float* sA, const float* sratio, float* sacc, float* srow,
                                    float* scol, int img_stride, int pitch, const float* em_a,
-                                   int Rrt, const Geo& g, int H, int W, Corners& cs) {
+                                   int Rrt, const Geo& g, int H, int W, Corners& cs, int seg) {
     const int R = RC > 0 ? RC : Rrt;
-    const int nseg = (H + kSeg - 1) / kSeg;
+    const int nseg = (H + seg - 1) / seg;
     for (int pw = 0; pw < 3; ++pw) {
         const int nw = (W - pw + 2) / 3;
         for (int ps = 0; ps < 2; ++ps) {
@@ -360,7 +359,7 @@ __device__ void backward_angle_seg(const float* sA, const float* sratio, float* 
             for (int it = threadIdx.x; it < items; it += blockDim.x) {
                 const int k = it / nw, cw = it - k * nw;   // a warp spans columns
                 const int w = pw + 3 * cw;
-                const int h0 = (ps + 2 * k) * kSeg, h1 = min(H, h0 + kSeg);
+                const int h0 = (ps + 2 * k) * seg, h1 = min(H, h0 + seg);
                 for (int h = h0; h < h1; ++h) {
                     const Foot f = footprint(g, sA, sratio, W, pitch, h, w);
 #pragma unroll
@@ -620,7 +619,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 proj_bwd_kernel(const float* __restrict__ atten, const float* __restrict__ ratio,
                 const float* __restrict__ em, const float* __restrict__ theta,
                 float* __restrict__ out, int A, int B, int R, int H, int W, int apc,
-                float clamp_min, int stage_tile, int bwd_mode, int ncopy) {
+                float clamp_min, int stage_tile, int bwd_mode, int ncopy, int seg) {
     extern __shared__ __align__(16) float smem[];
     cg::cluster_group cluster = cg::this_cluster();
     const int b = blockIdx.y;
@@ -659,7 +658,7 @@ proj_bwd_kernel(const float* __restrict__ atten, const float* __restrict__ ratio
                                   make_geo(theta[a], H, W), H, W, cs, wk_dh, wk_dw, wk_h0, wk_w0);
         else if (bwd_mode == 4)
             backward_angle_seg<RC>(stage_tile ? sA : src, sratio, sacc, srow, scol, img_stride,
-                                   pitch, sem, R, make_geo(theta[a], H, W), H, W, cs);
+                                   pitch, sem, R, make_geo(theta[a], H, W), H, W, cs, seg);
         else if (bwd_mode != 1)
             backward_angle<RC>(stage_tile ? sA : src, sratio, sacc, srow, scol, img_stride, pitch,
                                sem, R, make_geo(theta[a], H, W), H, W, cs);
@@ -690,7 +689,7 @@ mlem_iter_kernel(const float* __restrict__ atten, const float* __restrict__ em,
                  const float* __restrict__ theta, const float* __restrict__ I,
                  const float* __restrict__ sens, const float* __restrict__ Cin,
                  float* __restrict__ Cout, int A, int B, int R, int H, int W, int apc,
-                 float beta, float delta, int bwd_mode, int ncopy) {
+                 float beta, float delta, int bwd_mode, int ncopy, int seg) {
     extern __shared__ __align__(16) float smem[];
     cg::cluster_group cluster = cg::this_cluster();
     const int b = blockIdx.y;
@@ -739,7 +738,7 @@ mlem_iter_kernel(const float* __restrict__ atten, const float* __restrict__ em,
                                   wk_dw, wk_h0, wk_w0);
         else if (bwd_mode == 4)
             backward_angle_seg<RC>(sA, sratio, sacc, srow, scol, img_stride, pitch, sem, R, g, H, W,
-                                   cs);
+                                   cs, seg);
         else if (bwd_mode != 1)
             backward_angle<RC>(sA, sratio, sacc, srow, scol, img_stride, pitch, sem, R, g, H, W,
                                cs);
@@ -948,17 +947,28 @@ size_t mlem_smem(int64_t R, int64_t H, int64_t W, int ncopy) {
                             frame_floats((int)R, (int)H, (int)W, ncopy) + parts * W + W + kMaxR);
 }
 
-// Backward form for the knob value 0 (automatic): the column segments
-// (4) when one round of a segment phase's items fills 85-100% of the
-// CTA's threads -- there they beat the nine phases (120 angles x 128 slices of
-// 128^2: 2.17 vs 2.31 ms) -- else the nine-phase splat (2), which wins when
-// the segment phases leave threads idle or take a second, partial round.
+// Segment length of the column-segment backward: the shortest (>= 2) for
+// which one round of a segment phase's items fits the CTA's threads.
+int seg_length(int64_t H, int64_t W) {
+    const int64_t nw = (W + 2) / 3;
+    int seg = 2;
+    while (seg < H && nw * (((H + seg - 1) / seg + 1) / 2) > kThreads) ++seg;
+    return seg;
+}
+
+// Backward form for the knob value 0 (automatic): the column segments (4)
+// when one round of a segment phase's items fills 85-100% of the CTA's
+// threads with segments of at most 8 samples -- measured faster there
+// (fused MLEM iteration, 120 angles: 96^2 1.03 vs 1.14 ms, 112^2 2.30 vs
+// 2.61, 128^2 2.80 vs 3.06) -- else the nine-phase splat (2), which wins
+// when the segment phases leave threads idle or the segments grow long
+// (192^2, 12 samples: 5.98 vs 5.75 ms).
 int pick_bwd_mode(int64_t H, int64_t W) {
     int mode = (int)tune(kTuneProjBwd);
     if (mode != 0) return mode;
-    const int64_t nseg = (H + kSeg - 1) / kSeg;
-    const int64_t items = (W + 2) / 3 * ((nseg + 1) / 2);
-    return (items <= kThreads && items * 100 >= 85 * kThreads) ? 4 : 2;
+    const int seg = seg_length(H, W);
+    const int64_t items = (W + 2) / 3 * (((H + seg - 1) / seg + 1) / 2);
+    return (seg <= 8 && items <= kThreads && items * 100 >= 85 * kThreads) ? 4 : 2;
 }
 
 // The most frame copies (kMaxFrameCopies, halving down to 1) for which
@@ -998,9 +1008,10 @@ int bwd_emission_launch(const float* atten, const float* ratio, const float* em,
     const void* fn = R == 1 ? (const void*)proj_bwd_kernel<1> : (const void*)proj_bwd_kernel<0>;
     Plan p = plan_cluster(fn, A, B, smem);
     int iA = (int)A, iB = (int)B, iR = (int)R, iH = (int)H, iW = (int)W, apc = p.apc;
-    int bwd_mode = pick_bwd_mode(H, W);
+    int bwd_mode = pick_bwd_mode(H, W), seg = seg_length(H, W);
     void* args[] = {(void*)&atten, (void*)&ratio, (void*)&em, (void*)&theta, (void*)&out,
-                    &iA, &iB, &iR, &iH, &iW, &apc, &clamp_min, &stage_tile, &bwd_mode, &ncopy};
+                    &iA, &iB, &iR, &iH, &iW, &apc, &clamp_min, &stage_tile, &bwd_mode, &ncopy,
+                    &seg};
     return launch_cluster(fn, dim3(p.G, (unsigned)B), p.G, smem, st, args);
 }
 
@@ -1041,10 +1052,10 @@ int mlem_iter_launch(const float* atten, const float* em, const float* theta, co
     const void* fn = R == 1 ? (const void*)mlem_iter_kernel<1> : (const void*)mlem_iter_kernel<0>;
     Plan p = plan_cluster(fn, A, B, smem);
     int iA = (int)A, iB = (int)B, iR = (int)R, iH = (int)H, iW = (int)W, apc = p.apc;
-    int bwd_mode = pick_bwd_mode(H, W);
+    int bwd_mode = pick_bwd_mode(H, W), seg = seg_length(H, W);
     void* args[] = {(void*)&atten, (void*)&em, (void*)&theta, (void*)&I, (void*)&sens,
                     (void*)&Cin, (void*)&Cout, &iA, &iB, &iR, &iH, &iW, &apc, &beta, &delta,
-                    &bwd_mode, &ncopy};
+                    &bwd_mode, &ncopy, &seg};
     return launch_cluster(fn, dim3(p.G, (unsigned)B), p.G, smem, st, args);
 }
 

@@ -127,9 +127,11 @@ def test_non_contiguous_inputs():
 
 
 @pytest.mark.parametrize("mode", [1, 2, 3, 4])
-@pytest.mark.parametrize("A,B,R,H,W", [(8, 3, 2, 20, 28), (5, 2, 1, 64, 64), (1, 1, 1, 2, 2)])
+@pytest.mark.parametrize("A,B,R,H,W", [(8, 3, 2, 20, 28), (5, 2, 1, 64, 64), (1, 1, 1, 2, 2),
+                                       (4, 2, 1, 112, 112)])
 def test_backward_splat_variants(mode, A, B, R, H, W):
-    # shared-atomic splat, nine-phase splat and gather give the same transpose
+    # shared-atomic splat, nine-phase splat, gather and column segments (of 2
+    # samples at 64^2, 5 at 112^2) give the same transpose
     from fl_correction_b200 import tune
     rng = np.random.default_rng(A * 1000 + H + 7)
     atten, C, em, th = projector_case(rng, A, B, R, H, W, SPECIAL[:A] if A <= 8 else None)

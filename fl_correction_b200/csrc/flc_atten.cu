@@ -64,25 +64,30 @@ __global__ void incident_scan_kernel(const float* __restrict__ mu, float* __rest
 // Fused per-angle stage: grid (S, A_chunk), block W threads (one per detector
 // column).  Walks the beam from h = H-1 to 0:
 //   out[i][a][s][h][w] = incident term (exclusive product, mode-dependent)
-//   mu_ref[a][i][s][x=w][y=H-1-h] = mu_f[i] (staged 32 rows at a time in smem
-//   so that the transposed store is a run of 32 contiguous floats)
+//   mu_ref[a][i][s][x=w][y=H-1-h] = mu_f[i]
+// A thread's mu_f values of consecutive beam steps are consecutive y of its
+// own row x of mu_ref: it keeps kRun of them in registers and stores them as
+// whole 32-byte sectors (two float4), so the stage needs no shared-memory
+// transpose and no barriers, and the kRun beam steps of a group, unrolled,
+// issue their rotation loads together.
 // ---------------------------------------------------------------------------
 constexpr int kMaxCh = 8;
 constexpr int kMaxL = 8;
-constexpr int kStageRows = 32;
+constexpr int kRun = 8;
 
 struct StageCoef {
     float cx[kMaxCh];
     float cf[kMaxL][kMaxCh];
 };
 
+// LM: lines held in registers (>= L).
+template <int LM>
 __global__ void atten_stage_kernel(const float* __restrict__ frac, const float* __restrict__ theta,
                                    const float* __restrict__ coef_x,
                                    const float* __restrict__ coef_f, float* __restrict__ out,
                                    float* __restrict__ mu_ref, int n_ch, int S, int H, int W,
                                    int L, int64_t out_a_stride, int64_t out_l_stride, int a_base,
                                    int incident_mode, int write_mu, int out_a0) {
-    extern __shared__ float stage[];  // [L][kStageRows][W]
     __shared__ StageCoef cf;
     const int s = blockIdx.x;
     const int al = blockIdx.y;
@@ -96,64 +101,74 @@ __global__ void atten_stage_kernel(const float* __restrict__ frac, const float* 
             cf.cf[i][j] = (i < L && j < n_ch) ? coef_f[((int64_t)a * L + i) * n_ch + j] : 0.f;
     }
     __syncthreads();
+    if (w >= W) return;
     // the reference rounds math.cos / math.sin of the angle to an FP32 matrix
     const double th = (double)theta[a];
     const RotGeom g = rot_geom((float)cos(th), (float)sin(th), H, W);
-    float prod[kMaxL];
+    float prod[LM];
 #pragma unroll
-    for (int i = 0; i < kMaxL; ++i) prod[i] = 1.f;
+    for (int i = 0; i < LM; ++i) prod[i] = 1.f;
     const int64_t HW = (int64_t)H * W;
-    for (int h = H - 1; h >= 0; --h) {
-        float fr[kMaxCh];
+    float* outw = out + (int64_t)(out_a0 + al) * out_a_stride + s * HW + w;
+    // mu_ref row x = w of each line; whole-sector stores need H % 4 == 0
+    float* murow = mu_ref + ((int64_t)al * L * S + s) * HW + (int64_t)w * H;
+    const int64_t mu_l = (int64_t)S * HW;
+    const bool vec = (H & 3) == 0;
+    for (int y0 = 0; y0 < H; y0 += kRun) {
+        const int n = min(kRun, H - y0);
+        float mb[LM][kRun];
 #pragma unroll
-        for (int j = 0; j < kMaxCh; ++j)
-            fr[j] = (j < n_ch && w < W) ? rot_sample(frac + ((int64_t)j * S + s) * HW, H, W, g, h, w) : 0.f;
-        // incident term: write the exclusive product, then fold in this voxel
-        if (w < W && incident_mode != 2) {
-#pragma unroll
-            for (int i = 0; i < kMaxL; ++i)
-                if (i < L) out[i * out_l_stride + (int64_t)(out_a0 + al) * out_a_stride + s * HW + (int64_t)h * W + w] = prod[i];
-            if (incident_mode == 0) {
-#pragma unroll
-                for (int i = 0; i < kMaxL; ++i)
-                    if (i < L) prod[i] *= 1.f - fr[i] * cf.cx[i];
-            } else {
-                float f = 1.f;
-#pragma unroll
-                for (int j = 0; j < kMaxCh; ++j)
-                    if (j < n_ch) f *= 1.f - fr[j] * cf.cx[j];
-#pragma unroll
-                for (int i = 0; i < kMaxL; ++i) prod[i] *= f;
-            }
-        } else if (w < W) {
-#pragma unroll
-            for (int i = 0; i < kMaxL; ++i)
-                if (i < L) out[i * out_l_stride + (int64_t)(out_a0 + al) * out_a_stride + s * HW + (int64_t)h * W + w] = 1.f;
-        }
-        if (!write_mu) continue;
-        const int row = (H - 1 - h) % kStageRows;  // y = H-1-h within the staged block
-#pragma unroll
-        for (int i = 0; i < kMaxL; ++i) {
-            if (i >= L) break;
-            float m = 0.f;
+        for (int r = 0; r < kRun; ++r) {
+            if (r >= n) break;
+            const int h = H - 1 - (y0 + r);
+            float fr[kMaxCh];
 #pragma unroll
             for (int j = 0; j < kMaxCh; ++j)
-                if (j < n_ch) m += fr[j] * cf.cf[i][j];
-            if (w < W) stage[(i * kStageRows + row) * W + w] = m;
-        }
-        const int y = H - 1 - h;
-        if (row == kStageRows - 1 || h == 0) {
-            __syncthreads();
-            const int y0 = y - row, nrows = row + 1;
-            // transposed store: mu_ref[al][i][s][x][y0 + r], r contiguous
-            for (int idx = threadIdx.x; idx < L * W * nrows; idx += blockDim.x) {
-                int r = idx % nrows;
-                int rest = idx / nrows;
-                int x = rest % W, i = rest / W;
-                mu_ref[(((int64_t)al * L + i) * S + s) * HW + (int64_t)x * H + y0 + r] =
-                    stage[(i * kStageRows + r) * W + x];
+                fr[j] = j < n_ch ? rot_sample(frac + ((int64_t)j * S + s) * HW, H, W, g, h, w) : 0.f;
+            // incident term: write the exclusive product, then fold in this voxel
+            if (incident_mode != 2) {
+#pragma unroll
+                for (int i = 0; i < LM; ++i)
+                    if (i < L) outw[i * out_l_stride + (int64_t)h * W] = prod[i];
+                if (incident_mode == 0) {
+#pragma unroll
+                    for (int i = 0; i < LM; ++i)
+                        if (i < L) prod[i] *= 1.f - fr[i] * cf.cx[i];
+                } else {
+                    float f = 1.f;
+#pragma unroll
+                    for (int j = 0; j < kMaxCh; ++j)
+                        if (j < n_ch) f *= 1.f - fr[j] * cf.cx[j];
+#pragma unroll
+                    for (int i = 0; i < LM; ++i) prod[i] *= f;
+                }
+            } else {
+#pragma unroll
+                for (int i = 0; i < LM; ++i)
+                    if (i < L) outw[i * out_l_stride + (int64_t)h * W] = 1.f;
             }
-            __syncthreads();
+#pragma unroll
+            for (int i = 0; i < LM; ++i) {
+                float m = 0.f;
+#pragma unroll
+                for (int j = 0; j < kMaxCh; ++j)
+                    if (j < n_ch) m += fr[j] * cf.cf[i][j];
+                mb[i][r] = m;
+            }
+        }
+        if (!write_mu) continue;
+#pragma unroll
+        for (int i = 0; i < LM; ++i) {
+            if (i >= L) break;
+            float* dst = murow + i * mu_l + y0;
+            if (vec && n == kRun) {
+                reinterpret_cast<float4*>(dst)[0] = make_float4(mb[i][0], mb[i][1], mb[i][2], mb[i][3]);
+                reinterpret_cast<float4*>(dst)[1] = make_float4(mb[i][4], mb[i][5], mb[i][6], mb[i][7]);
+            } else {
+#pragma unroll
+                for (int r = 0; r < kRun; ++r)
+                    if (r < n) dst[r] = mb[i][r];
+            }
         }
     }
 }
@@ -498,11 +513,10 @@ int atten_stage_launch(const float* frac, const float* theta, const float* coef_
                        const float* coef_f, float* out, float* mu_ref, int n_ch, int S, int H,
                        int W, int L, int64_t out_a_stride, int64_t out_l_stride, int a_base,
                        int n_a, int incident_mode, int write_mu, cudaStream_t st, int out_a0) {
-    size_t smem = sizeof(float) * (size_t)L * kStageRows * W;
-    int threads = (W + 31) & ~31;
-    FLC_TRY_CUDA(cudaFuncSetAttribute((const void*)atten_stage_kernel,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    atten_stage_kernel<<<dim3((unsigned)S, (unsigned)n_a), threads, smem, st>>>(
+    const int threads = (W + 31) & ~31;
+    auto kern = L <= 1 ? atten_stage_kernel<1> : L <= 2 ? atten_stage_kernel<2>
+              : L <= 4 ? atten_stage_kernel<4> : atten_stage_kernel<8>;
+    kern<<<dim3((unsigned)S, (unsigned)n_a), threads, 0, st>>>(
         frac, theta, coef_x, coef_f, out, mu_ref, n_ch, S, H, W, L, out_a_stride, out_l_stride,
         a_base, incident_mode, write_mu, out_a0 < 0 ? a_base : out_a0);
     return check_launch("atten_stage_kernel");

@@ -8,6 +8,8 @@ None) optionally writes one ``.npy`` per element instead of per-angle TIFFs.
 """
 import os
 
+import ctypes
+
 import numpy as np
 import torch
 
@@ -82,8 +84,10 @@ def atten_maps(frac_4D, angle_list, coef_x, coef_f, mask_uv=None, incident="own"
         u = v = None
         Mz = Mx = My = 1
     chunk = pick_chunk(S, H, W, A, L, chunk)
-    ws_bytes = _lib.query("flc_atten_workspace_bytes", n_ch, S, H, W, A, L, chunk)
+    ws_bytes, mu_bytes, fft_bytes = atten_workspace_bytes(n_ch, S, H, W, A, L, chunk,
+                                                          (Mz, Mx, My) if xrf else None)
     ws = workspace if workspace is not None and workspace.numel() >= ws_bytes else _lib.workspace(ws_bytes, dev)
+    fft_ws = ctypes.c_void_p(ws.data_ptr() + mu_bytes) if fft_bytes else None
     mode = INCIDENT_MODES[incident]
     with torch.cuda.device(dev):
         st = _lib.stream()
@@ -102,11 +106,25 @@ def atten_maps(frac_4D, angle_list, coef_x, coef_f, mask_uv=None, incident="own"
                 continue
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
-            _lib.call("flc_cone_atten_apply", _lib.ptr(ws), _lib.ptr(u), _lib.ptr(v),
-                      _lib.ptr(out), n_a, L, S, H, W, A, a0, Mz, Mx, My, st)
+            _lib.call("flc_cone_atten_apply_ws", _lib.ptr(ws), _lib.ptr(u), _lib.ptr(v),
+                      _lib.ptr(out), n_a, L, S, H, W, A, a0, Mz, Mx, My, fft_ws, fft_bytes, st)
             e1.record()
             cone_events.append((e0, e1, n_a * L))
     return out
+
+
+def atten_workspace_bytes(n_ch, S, H, W, A, L, chunk=0, mask_shape=None):
+    """(total, staged-mu, spectral-cone) workspace bytes of atten_maps for
+    `chunk` angles per pass (0: the default chunk).  mask_shape (Mz, Mx, My):
+    the cone's mask, None for the incident term alone; the spectral-cone part
+    is 0 where that form does not take the shape."""
+    chunk = pick_chunk(S, H, W, A, L, chunk)
+    mu_bytes = int(_lib.query("flc_atten_workspace_bytes", n_ch, S, H, W, A, L, chunk))
+    fft_bytes = 0
+    if mask_shape is not None:
+        Mz, Mx, My = mask_shape
+        fft_bytes = int(_lib.query("flc_cone_fft_workspace_bytes", chunk * L, S, H, W, Mz, Mx, My))
+    return mu_bytes + fft_bytes, mu_bytes, fft_bytes
 
 
 def pick_chunk(S, H, W, A, L, chunk=0):

@@ -418,6 +418,14 @@ int cone_tma_launch(const float* mu, const float* U, const float* Vw, float* out
                     int64_t Z, int64_t X, int64_t Y, int64_t Mz, int64_t Mx, int64_t My, int mode,
                     int L, int a_base, int64_t out_a_stride, int64_t out_l_stride, cudaStream_t st);
 
+// Spectral form (flc_cone_fft.cu).
+size_t cone_fft_ws_bytes(int64_t Vn, int64_t Z, int64_t X, int64_t Y, int64_t Mz, int64_t Mx,
+                         int64_t My, int mode);
+int cone_fft_launch(const float* mu, const float* U, const float* Vw, float* out, int64_t Vn,
+                    int64_t Z, int64_t X, int64_t Y, int64_t Mz, int64_t Mx, int64_t My, int mode,
+                    int L, int a_base, int64_t out_a_stride, int64_t out_l_stride,
+                    void* workspace, size_t ws_bytes, cudaStream_t st);
+
 // Separable cone path sum.  `mode` (0/1/2, see cone_sep_kernel) may carry
 // kConePlain to select the plain kernel below even where the pipelined one fits.
 int cone_sep_launch(const float* mu, const float* U, const float* Vw, float* out, int64_t Vn,
@@ -448,6 +456,24 @@ int cone_sep_launch(const float* mu, const float* U, const float* Vw, float* out
 }
 
 namespace {
+
+// Cone path sum with scratch for the spectral form: the spectral kernels run
+// when the "cone.variant" knob allows them (0 automatic, 4 spectral) and the
+// shape and scratch fit; otherwise cone_sep_launch.
+int cone_launch_ws(const float* mu, const float* U, const float* Vw, float* out, int64_t Vn,
+                   int64_t Z, int64_t X, int64_t Y, int64_t Mz, int64_t Mx, int64_t My, int mode,
+                   int L, int a_base, int64_t out_a_stride, int64_t out_l_stride, void* ws,
+                   size_t ws_bytes, cudaStream_t st) {
+    const int64_t var = tune(kTuneConeVariant);
+    if (ws && (var == 0 || var == 4)) {
+        int r = cone_fft_launch(mu, U, Vw, out, Vn, Z, X, Y, Mz, Mx, My, mode, L, a_base,
+                                out_a_stride, out_l_stride, ws, ws_bytes, st);
+        if (r != FLC_ERR_UNSUPPORTED) return r;
+        clear_error();
+    }
+    return cone_sep_launch(mu, U, Vw, out, Vn, Z, X, Y, Mz, Mx, My, mode, L, a_base, out_a_stride,
+                           out_l_stride, st);
+}
 
 // Splits each depth plane of a host mask into u (Mz) x v (My) if it is rank
 // one to FP32 precision.  Returns false otherwise.
@@ -526,9 +552,13 @@ int atten_maps_launch(const float* frac, const float* theta, const float* coef_x
                       const float* coef_f, const float* u, const float* v, float* out,
                       int64_t n_ch, int64_t S, int64_t H, int64_t W, int64_t A, int64_t L,
                       int64_t Mz, int64_t Mx, int64_t My, int incident_mode, int xrf_mode,
-                      int64_t chunk, void* workspace, cudaStream_t st) {
+                      int64_t chunk, void* workspace, size_t ws_bytes, cudaStream_t st) {
     chunk = pick_chunk(S, H, W, A, L, chunk);
     float* mu_ref = (float*)workspace;
+    // scratch of the spectral cone: the workspace past the staged mu
+    const size_t mu_bytes = atten_ws_bytes(S, H, W, A, L, chunk);
+    void* fft_ws = ws_bytes > mu_bytes ? (char*)workspace + mu_bytes : nullptr;
+    const size_t fft_bytes = ws_bytes > mu_bytes ? ws_bytes - mu_bytes : 0;
     const int64_t out_a = S * H * W, out_l = A * S * H * W;
     for (int64_t a0 = 0; a0 < A; a0 += chunk) {
         int n_a = (int)(A - a0 < chunk ? A - a0 : chunk);
@@ -537,8 +567,8 @@ int atten_maps_launch(const float* frac, const float* theta, const float* coef_x
                                    incident_mode, xrf_mode == 0, st, -1));
         if (xrf_mode != 0) continue;
         // reference frame of the cone: (Z=S, X=W, Y=H)
-        FLC_TRY(cone_sep_launch(mu_ref, u, v, out, (int64_t)n_a * L, S, W, H, Mz, Mx, My, 2,
-                                (int)L, (int)a0, out_a, out_l, st));
+        FLC_TRY(cone_launch_ws(mu_ref, u, v, out, (int64_t)n_a * L, S, W, H, Mz, Mx, My, 2,
+                               (int)L, (int)a0, out_a, out_l, fft_ws, fft_bytes, st));
     }
     return FLC_OK;
 }
@@ -677,7 +707,8 @@ extern "C" int flc_atten_maps(const float* frac, const float* theta, const float
         return FLC_ERR_WORKSPACE;
     }
     return atten_maps_launch(frac, theta, coef_x, coef_f, u, v, out, n_ch, S, H, W, A, L, Mz, Mx,
-                             My, incident_mode, xrf_mode, chunk, workspace, as_stream(stream));
+                             My, incident_mode, xrf_mode, chunk, workspace, workspace_bytes,
+                             as_stream(stream));
 }
 
 extern "C" int flc_atten_stage(const float* frac, const float* theta, const float* coef_x,
@@ -712,6 +743,33 @@ extern "C" int flc_cone_atten_apply(const float* mu_ref, const float* u, const f
                 "flc_cone_atten_apply: bad sizes");
     return cone_sep_launch(mu_ref, u, v, atten, n_a * L, S, W, H, Mz, Mx, My, 2, (int)L, (int)a0,
                            S * H * W, A * S * H * W, as_stream(stream));
+}
+
+extern "C" size_t flc_cone_fft_workspace_bytes(int64_t n_vol, int64_t S, int64_t H, int64_t W,
+                                               int64_t Mz, int64_t Mx, int64_t My) {
+    if (n_vol < 1 || S < 1 || H < 1 || W < 1 || Mz < 1 || Mx < 1 || My < 1) return 0;
+    // cone frame (Z = S, X = W, Y = H), beam-layout output
+    return cone_fft_ws_bytes(n_vol, S, W, H, Mz, Mx, My, 2);
+}
+
+extern "C" int flc_cone_atten_apply_ws(const float* mu_ref, const float* u, const float* v,
+                                       float* atten, int64_t n_a, int64_t L, int64_t S, int64_t H,
+                                       int64_t W, int64_t A, int64_t a0, int64_t Mz, int64_t Mx,
+                                       int64_t My, void* workspace, size_t workspace_bytes,
+                                       void* stream) {
+    clear_error();
+    FLC_REQUIRE(mu_ref && u && v && atten, "flc_cone_atten_apply_ws: null pointer argument");
+    FLC_REQUIRE(H == W && H >= 2 && S >= 1 && L >= 1 && n_a >= 1 && a0 >= 0 && a0 + n_a <= A,
+                "flc_cone_atten_apply_ws: bad sizes");
+    FLC_REQUIRE(n_a * L <= 65535 && Mz >= 1 && Mx >= 1 && My >= 1,
+                "flc_cone_atten_apply_ws: bad sizes");
+    if (workspace && ((uintptr_t)workspace & 255) != 0) {
+        set_error("flc_cone_atten_apply_ws: workspace must be 256-byte aligned");
+        return FLC_ERR_ALIGNMENT;
+    }
+    return cone_launch_ws(mu_ref, u, v, atten, n_a * L, S, W, H, Mz, Mx, My, 2, (int)L, (int)a0,
+                          S * H * W, A * S * H * W, workspace, workspace_bytes,
+                          as_stream(stream));
 }
 
 extern "C" int flc_device_status(int reset) {

@@ -34,7 +34,7 @@ inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s
 enum TuneKey {
     kTuneProjCluster = 0,   // CTAs per slice cluster for the backward / MLEM kernels
     kTuneProjApc = 1,       // angles per CTA for the projector kernels
-    kTuneConeVariant = 2,   // 1: TMA 16x8 tile, 2: TMA 8x4 tile, 3: plain kernel
+    kTuneConeVariant = 2,   // 1: TMA 16x8 tile, 2: TMA 8x4 tile, 3: plain kernel, 4: spectral
     kTuneAttenChunk = 3,    // angles per attenuation-pipeline pass
     kTuneProjBwd = 4,       // backward: 0 automatic, 1 shared-atomic splat, 2 nine-phase
                             // splat, 3 gather, 4 column segments

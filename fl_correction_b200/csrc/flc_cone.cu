@@ -485,7 +485,8 @@ int cone_tma_launch(const float* mu, const float* U, const float* Vw, float* out
     ConeGeom g;
     size_t smem;
     int threads;
-    const int64_t variant = tune(kTuneConeVariant);  // 0 auto, 1 16x8, 2 8x4, 3 plain
+    int64_t variant = tune(kTuneConeVariant);  // 0 auto, 1 16x8, 2 8x4, 3 plain, 4 spectral
+    if (variant == 4) variant = 0;              // the spectral form fell back to this kernel
     if (variant == 3) return FLC_ERR_UNSUPPORTED;
     if ((variant == 1 || (variant == 0 && Z <= 128)) &&
         cone_tma_geom<16, 8>(Z, X, Y, Mz, Mx, My, &g, &smem, &threads))

@@ -14,7 +14,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .core import atten_coefficients, atten_maps, mask_factors
+from .core import atten_coefficients, atten_maps, atten_workspace_bytes, mask_factors
 from .detector_mask import generate_detector_mask
 
 __all__ = ["CorrectedMLEM"]
@@ -65,7 +65,7 @@ class CorrectedMLEM:
                                  dtype=torch.float32, device=dev)
             self.frac[self.L:] = ff
         self.atten = torch.empty((self.L, A, S, H, W), dtype=torch.float32, device=dev)
-        ws = _lib.query("flc_atten_workspace_bytes", self.n_ch, S, H, W, A, self.L, chunk)
+        ws, _, _ = atten_workspace_bytes(self.n_ch, S, H, W, A, self.L, chunk, self.mask_uv[2])
         self.chunk = chunk
         self.ws_atten = _lib.workspace(ws, dev)
         self.ws_mlem_bytes = _lib.query("flc_mlem_workspace_bytes", A, S, 1, H, W)

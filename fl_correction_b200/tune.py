@@ -7,7 +7,8 @@ CUDA events and keeps the fastest through ``flc_tune_set``:
   proj.cluster   CTAs per slice cluster of the backward projector / fused
                  MLEM kernel (1, 2, 4, 8)
   proj.apc       angles per CTA of the forward projector
-  cone.variant   TMA 16x8 tile, TMA 8x4 tile or the plain separable kernel
+  cone.variant   TMA 16x8 tile, TMA 8x4 tile, the plain separable kernel or
+                 the spectral form (FFTs of the depth planes)
   atten.chunk    angles per attenuation-pipeline pass
   proj.bwd       backward: splat with shared atomics, splat in nine disjoint
                  phases, gather per pixel, or splat by column segments
@@ -132,14 +133,17 @@ def tune_cone(n_a, L, N, A, mask, device="cuda"):
     g = torch.Generator(device=dev).manual_seed(0)
     mu = torch.rand((n_a, L, N, N, N), device=dev, generator=g) * 0.01
     atten = torch.ones((L, A, N, N, N), device=dev)
+    nb = int(_lib.query("flc_cone_fft_workspace_bytes", n_a * L, N, N, N, *mask.shape))
+    ws = _lib.workspace(nb, dev) if nb else None
 
     def run():
         atten.fill_(1.0)
-        _lib.call("flc_cone_atten_apply", _lib.ptr(mu), _lib.ptr(u), _lib.ptr(v),
-                  _lib.ptr(atten), n_a, L, N, N, N, A, 0, *mask.shape, _lib.stream())
+        _lib.call("flc_cone_atten_apply_ws", _lib.ptr(mu), _lib.ptr(u), _lib.ptr(v),
+                  _lib.ptr(atten), n_a, L, N, N, N, A, 0, *mask.shape, _lib.ptr(ws), nb,
+                  _lib.stream())
         return atten[:, :n_a].clone()
 
-    return {"cone.variant": _sweep("cone.variant", [0, 1, 2, 3], run, _close)}
+    return {"cone.variant": _sweep("cone.variant", [0, 1, 2, 3, 4], run, _close)}
 
 
 def autotune(A, S, N, L, mask, chunk, device="cuda"):

@@ -60,7 +60,8 @@ FLC_API uint64_t flc_launch_count(void);
  * autotuner in fl_correction_b200/tune.py sets them).  Names:
  *   "proj.cluster"  CTAs per slice cluster, backward/MLEM kernels (1..8)
  *   "proj.apc"      angles per CTA, projector kernels
- *   "cone.variant"  1: TMA 16x8 tile, 2: TMA 8x4 tile, 3: plain kernel
+ *   "cone.variant"  1: TMA 16x8 tile, 2: TMA 8x4 tile, 3: plain kernel, 4: spectral
+ *                   (where scratch is given; automatic: spectral where it fits)
  *   "atten.chunk"   angles per attenuation-pipeline pass
  *   "proj.bwd"      backward: 2 nine-phase splat, 1 shared-memory atomics,
  *                   3 gather per pixel, 4 splat by column segments; automatic:
@@ -165,7 +166,11 @@ FLC_API int flc_mlem_static(float* C, const float* atten, const float* em, const
  *   (FL/legacy/FL_correction_core.py:1855-1860).  2: no incident term.
  * xrf_mode 0: fluorescence term on; 1: off (incident only).
  * workspace: flc_atten_workspace_bytes(...) bytes; `chunk` angles are
- * processed per pass (0 = choose).
+ * processed per pass (0 = choose).  A workspace larger by
+ * flc_cone_fft_workspace_bytes(chunk * L, S, H, W, Mz, Mx, My) bytes (the
+ * chunk as chosen, pick it explicitly to size this) lets the cone run in its
+ * spectral form (2-D FFTs of the depth planes, a per-frequency correlation
+ * along the depth, inverse FFTs); without it the direct separable kernels run.
  * --------------------------------------------------------------------- */
 FLC_API size_t flc_atten_workspace_bytes(int64_t n_ch, int64_t S, int64_t H, int64_t W, int64_t A,
                                  int64_t L, int64_t chunk);
@@ -191,6 +196,18 @@ FLC_API int flc_cone_atten_apply(const float* mu_ref, const float* u, const floa
                                  float* atten, int64_t n_a, int64_t L, int64_t S, int64_t H,
                                  int64_t W, int64_t A, int64_t a0, int64_t Mz, int64_t Mx,
                                  int64_t My, void* stream);
+/* flc_cone_atten_apply with scratch for the spectral cone: `workspace`
+ * (256-byte aligned) of flc_cone_fft_workspace_bytes(n_a * L, S, H, W, Mz,
+ * Mx, My) bytes, or NULL for the direct kernels.  The query returns 0 for a
+ * shape the spectral form does not take (its planes must fit in shared
+ * memory); the "cone.variant" knob selects among the forms. */
+FLC_API size_t flc_cone_fft_workspace_bytes(int64_t n_vol, int64_t S, int64_t H, int64_t W,
+                                            int64_t Mz, int64_t Mx, int64_t My);
+FLC_API int flc_cone_atten_apply_ws(const float* mu_ref, const float* u, const float* v,
+                                    float* atten, int64_t n_a, int64_t L, int64_t S, int64_t H,
+                                    int64_t W, int64_t A, int64_t a0, int64_t Mz, int64_t Mx,
+                                    int64_t My, void* workspace, size_t workspace_bytes,
+                                    void* stream);
 
 /* ---------------------------------------------------------------------
  * Differentiable corrected projection with per-angle recomputation.

@@ -125,3 +125,78 @@ def test_tall_volume_with_wide_mask(Z, n_mask, angle):
               K, Z, X, Y, mask.shape[0], mask.shape[1], mask.shape[2], 0, _lib.stream())
     assert _lib.query("flc_device_status", 1) == 0
     assert rel_err(out.cpu().numpy(), O.cone_ref(mu, mask.astype(np.float32))) < TOL_MAP
+
+
+@pytest.mark.parametrize("n_a,L,S,N,mask_args", [
+    (2, 3, 9, 20, (13.309, 13.309, 20)),
+    (1, 2, 16, 31, (13.309, 13.309, 31)),     # odd planes: radix-3/5 padding
+    (2, 1, 5, 12, (15.0, 60.0, 12)),          # mask taller (13) than the volume (5)
+    (1, 1, 7, 2, (13.309, 13.309, 2)),        # 2 x 2 planes
+    (1, 2, 6, 40, (19.0, 19.0, 60)),          # mask deeper (60) than the volume (40)
+])
+def test_spectral_cone_matches_oracle(n_a, L, S, N, mask_args):
+    # the spectral form (2-D FFTs of the depth planes, per-frequency depth
+    # correlation, inverse FFTs) and the plain direct kernel, both through the
+    # beam-layout entry point, against the FP64 path sum of the staged mu
+    from fl_correction_b200 import tune
+    rng = np.random.default_rng(S * 100 + N)
+    mask = generate_detector_mask(*mask_args)
+    u, v = factor_mask(mask)
+    Mz, Mx, My = mask.shape
+    A, a0 = n_a + 1, 1
+    mu = (rng.random((n_a, L, S, N, N)) * 0.05).astype(np.float32)   # (n_a, L, S, W, H)
+    base = rng.uniform(0.5, 1.0, (L, A, S, N, N)).astype(np.float32)
+    nb = _lib.query("flc_cone_fft_workspace_bytes", n_a * L, S, N, N, Mz, Mx, My)
+    assert nb > 0
+    ws = _lib.workspace(nb, "cuda")
+    x, U, V = T(mu), T(u), T(v)
+    outs = {}
+    old = tune.get_knob("cone.variant")
+    try:
+        for variant in (4, 3):
+            tune.set_knob("cone.variant", variant)
+            out = T(base)
+            _lib.call("flc_cone_atten_apply_ws", _lib.ptr(x), _lib.ptr(U), _lib.ptr(V),
+                      _lib.ptr(out), n_a, L, S, N, N, A, a0, Mz, Mx, My,
+                      _lib.ptr(ws) if variant == 4 else None, nb, _lib.stream())
+            outs[variant] = out.cpu().numpy()
+    finally:
+        tune.set_knob("cone.variant", old)
+    res = O.cone_ref(mu.reshape(n_a * L, S, N, N), mask)   # cone frame (Z=S, X=W, Y=H)
+    exp = base.astype(np.float64)
+    for al in range(n_a):
+        for l in range(L):
+            r = res[al * L + l]
+            exp[l, a0 + al] *= np.exp(-r[:, :, ::-1].transpose(0, 2, 1))
+    assert rel_err(outs[4], exp) < TOL_MAP
+    assert rel_err(outs[3], exp) < TOL_MAP
+    assert np.array_equal(outs[4][:, 0], base[:, 0])   # angles outside the chunk untouched
+
+
+def test_spectral_cone_benchmark_size():
+    # 128^2 planes with the 29 x 128 x 29 mask: spectral form against the
+    # pipelined direct kernel (the FP64 sum at this size takes minutes)
+    from fl_correction_b200 import tune
+    rng = np.random.default_rng(12)
+    mask = generate_detector_mask(13.309, 13.309, 128)
+    u, v = factor_mask(mask)
+    Mz, Mx, My = mask.shape
+    n_a, L, S, N, A = 1, 2, 10, 128, 1
+    mu = (rng.random((n_a, L, S, N, N)) * 0.01).astype(np.float32)
+    nb = _lib.query("flc_cone_fft_workspace_bytes", n_a * L, S, N, N, Mz, Mx, My)
+    ws = _lib.workspace(nb, "cuda")
+    x, U, V = T(mu), T(u), T(v)
+    outs = []
+    old = tune.get_knob("cone.variant")
+    try:
+        for variant in (4, 1):
+            tune.set_knob("cone.variant", variant)
+            out = torch.ones((L, A, S, N, N), device="cuda")
+            _lib.call("flc_cone_atten_apply_ws", _lib.ptr(x), _lib.ptr(U), _lib.ptr(V),
+                      _lib.ptr(out), n_a, L, S, N, N, A, 0, Mz, Mx, My, _lib.ptr(ws), nb,
+                      _lib.stream())
+            outs.append(out.cpu().numpy())
+    finally:
+        tune.set_knob("cone.variant", old)
+    assert _lib.query("flc_device_status", 1) == 0
+    assert rel_err(outs[0], outs[1]) < 2e-6

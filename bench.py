@@ -48,7 +48,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--adam-steps", type=int, default=0,
                    help="configurations 2/4: Adam steps timed (default 200 / 3)")
-    p.add_argument("--case", default=None, choices=["cone", "mlem", "fwd", "bwd", "stage"],
+    p.add_argument("--case", default=None, choices=["cone", "cone_direct", "mlem", "fwd", "bwd", "stage"],
                    help="run one kernel on a profiling-sized case instead of the benchmark")
     return p.parse_args()
 
@@ -623,7 +623,8 @@ def run_batch(args, device):
 def run_case(args):
     """One kernel on a profiling-sized case (for ncu): W warm-up launches, then
     one more.  cone: the fluorescence cone of one pipeline chunk at the
-    benchmark size (2 angles x 3 lines of 128^3); mlem: one fused MLEM
+    benchmark size (2 angles x 3 lines of 128^3), spectral form (cone_direct:
+    the direct separable kernel); mlem: one fused MLEM
     iteration (plus the sensitivity pass) at 24 angles x 16 slices of 128^2;
     fwd / bwd: the projector at 120 angles x 16 slices of 128^2."""
     import torch
@@ -633,15 +634,18 @@ def run_case(args):
     dev = torch.device("cuda", 0)
     g = torch.Generator(device=dev).manual_seed(0)
     N = 128
-    if args.case == "cone":
+    if args.case in ("cone", "cone_direct"):
         n_a, L, A = 2, 3, 120
         mask = generate_detector_mask(13.309, 13.309, N)
         u, v = (torch.from_numpy(x).to(dev) for x in factor_mask(mask))
         mu = torch.rand((n_a, L, N, N, N), device=dev, generator=g) * 0.01
         atten = torch.ones((L, A, N, N, N), device=dev)
+        nb = _lib.query("flc_cone_fft_workspace_bytes", n_a * L, N, N, N, *mask.shape)
+        ws = _lib.workspace(nb, dev) if args.case == "cone" else None
         def once():
-            _lib.call("flc_cone_atten_apply", _lib.ptr(mu), _lib.ptr(u), _lib.ptr(v),
-                      _lib.ptr(atten), n_a, L, N, N, N, A, 0, *mask.shape, _lib.stream())
+            _lib.call("flc_cone_atten_apply_ws", _lib.ptr(mu), _lib.ptr(u), _lib.ptr(v),
+                      _lib.ptr(atten), n_a, L, N, N, N, A, 0, *mask.shape, _lib.ptr(ws), nb,
+                      _lib.stream())
     elif args.case == "mlem":
         A, B = 24, 16
         atten = torch.rand((A, B, N, N), device=dev, generator=g)

@@ -40,10 +40,11 @@
 namespace flc {
 namespace {
 
-constexpr int kFftThreads = 512;
+constexpr int kFftThreads = 1024;
 constexpr int kCorrK = 32;       // frequencies per correlation CTA, one per lane
 constexpr int kCorrWarps = 8;
 constexpr int kMaxStages = 16;
+constexpr int kLoadBatch = 4;    // global loads per thread issued before their shared stores
 
 struct Radices {
     int n;               // transform length
@@ -113,23 +114,30 @@ __device__ __forceinline__ void dft_small(float2 (&v)[R], float sg) {
 // takes the R-point DFT and writes elements (j div Ns)*Ns*R + (j mod Ns) + r*Ns.
 // tw[m] = e^{-2 pi i m / N}; sg = +1 uses its conjugate.  seq_fast: adjacent
 // threads take adjacent sequences (columns) rather than adjacent butterflies.
+// floor(a / b) for 0 <= a < 2^22, b >= 1, from b's reciprocal: (a + 1/2) / b
+// stays at least 1/(2b) from an integer, far more than the rounding error.
+__device__ __forceinline__ int div_small(int a, float rb) {
+    return (int)(((float)a + 0.5f) * rb);
+}
+
 template <int R>
 __device__ void fft_pass(const float2* in, float2* out, int N, int Ns, int nseq, int ss, int es,
                          const float2* tw, float sg, bool seq_fast) {
     const int M = N / R;
     const int step = N / (Ns * R);
     const int total = nseq * M;
+    const float r_nseq = 1.f / (float)nseq, r_M = 1.f / (float)M, r_Ns = 1.f / (float)Ns;
     for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
         int s, j;
         if (seq_fast) {
-            j = idx / nseq;
+            j = div_small(idx, r_nseq);
             s = idx - j * nseq;
         } else {
-            s = idx / M;
+            s = div_small(idx, r_M);
             j = idx - s * M;
         }
         const float2* src = in + s * ss;
-        const int jm = j % Ns;
+        const int jm = j - div_small(j, r_Ns) * Ns;
         float2 v[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) v[r] = src[(j + r * M) * es];
@@ -232,18 +240,31 @@ fft_fwd_kernel(const float* __restrict__ mu, const float2* __restrict__ Tzg,
     float2* Ty = Tz + g.Nz;
     const int p = blockIdx.x, v = blockIdx.y;
     const int Z = g.Z, X = g.X, Y = g.Y, Ny = g.Ny, Nyh = g.Nyh;
+    const float rNy = 1.f / (float)Ny, rNyh = 1.f / (float)Nyh;
     for (int m = threadIdx.x; m < g.Nz; m += blockDim.x) Tz[m] = Tzg[m];
     for (int m = threadIdx.x; m < Ny; m += blockDim.x) Ty[m] = Tyg[m];
     // rows 2q, 2q+1 as the real and imaginary parts of sequence q (in B)
     const int npairs = (Z + 1) / 2;
     const float* src = mu + (int64_t)v * Z * X * Y + (int64_t)p * Y;
     const int64_t zs = (int64_t)X * Y;
-    for (int i = threadIdx.x; i < npairs * Ny; i += blockDim.x) {
-        const int q = i / Ny, y = i - q * Ny;
-        const int za = 2 * q, zb = za + 1;
-        const float a = y < Y ? __ldg(src + za * zs + y) : 0.f;
-        const float b = (y < Y && zb < Z) ? __ldg(src + zb * zs + y) : 0.f;
-        B[i] = make_float2(a, b);
+    // kLoadBatch elements per thread in flight before their shared stores
+    const int nrow = npairs * Ny;
+    for (int i0 = threadIdx.x; i0 < nrow; i0 += kLoadBatch * blockDim.x) {
+        float2 t[kLoadBatch];
+#pragma unroll
+        for (int b = 0; b < kLoadBatch; ++b) {
+            const int i = i0 + b * blockDim.x;
+            const int q = div_small(i, rNy), y = i - q * Ny;
+            const int za = 2 * q, zb = za + 1;
+            const bool in = i < nrow && y < Y;
+            t[b] = make_float2(in ? __ldg(src + za * zs + y) : 0.f,
+                               (in && zb < Z) ? __ldg(src + zb * zs + y) : 0.f);
+        }
+#pragma unroll
+        for (int b = 0; b < kLoadBatch; ++b) {
+            const int i = i0 + b * blockDim.x;
+            if (i < nrow) B[i] = t[b];
+        }
     }
     __syncthreads();
     float2* R1 = fft_batch(B, A, g.ry, npairs, Ny, 1, Ty, -1.f, false);
@@ -251,7 +272,7 @@ fft_fwd_kernel(const float* __restrict__ mu, const float2* __restrict__ Tzg,
     // unpack the two real rows' half spectra: Xa = (Zk + conj Zn)/2,
     // Xb = (Zk - conj Zn)/(2i), Zn = Z[(Ny - k) mod Ny]; rows >= Z are zero
     for (int i = threadIdx.x; i < g.NP; i += blockDim.x) {
-        const int z = i / Nyh, k = i - z * Nyh;
+        const int z = div_small(i, rNyh), k = i - z * Nyh;
         float2 o = make_float2(0.f, 0.f);
         if (z < Z) {
             const float2* Zq = R1 + (z >> 1) * Ny;
@@ -283,10 +304,23 @@ fft_corr_kernel(float2* __restrict__ S, const float2* __restrict__ G, FftGeom g)
     const int k = blockIdx.x * kCorrK + lane;
     const bool kin = k < g.NP;
     float2* Sv = S + (int64_t)blockIdx.y * X * g.NP;
-    for (int r = warp; r < prow; r += kCorrWarps)
-        sP[r * kCorrK + lane] = (kin && r < X) ? Sv[(int64_t)r * g.NP + k] : make_float2(0.f, 0.f);
-    for (int r = warp; r < grow; r += kCorrWarps)
-        sG[r * kCorrK + lane] = (kin && r < Mx) ? G[(int64_t)r * g.NP + k] : make_float2(0.f, 0.f);
+    for (int r0 = warp; r0 < prow + grow; r0 += kLoadBatch * kCorrWarps) {
+        float2 t[kLoadBatch];
+#pragma unroll
+        for (int b = 0; b < kLoadBatch; ++b) {
+            const int r = r0 + b * kCorrWarps;
+            const bool p = r < prow;
+            const int rr = p ? r : r - prow;
+            t[b] = (kin && (p ? rr < X : rr < Mx))
+                       ? (p ? Sv[(int64_t)rr * g.NP + k] : __ldg(G + (int64_t)rr * g.NP + k))
+                       : make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int b = 0; b < kLoadBatch; ++b) {
+            const int r = r0 + b * kCorrWarps;
+            if (r < prow + grow) sc[r * kCorrK + lane] = t[b];   // sG follows sP
+        }
+    }
     __syncthreads();
     const int nxg = (X + 7) / 8;
     for (int gi = warp; gi < (nxg + 1) / 2; gi += kCorrWarps) {
@@ -352,10 +386,23 @@ fft_inv_kernel(const float2* __restrict__ S, const float2* __restrict__ Tzg,
     float2* Ty = Tz + g.Nz;
     const int x = blockIdx.x, v = blockIdx.y;
     const int Z = g.Z, X = g.X, Y = g.Y, Ny = g.Ny, Nyh = g.Nyh;
+    const float rNy = 1.f / (float)Ny;
     for (int m = threadIdx.x; m < g.Nz; m += blockDim.x) Tz[m] = Tzg[m];
     for (int m = threadIdx.x; m < Ny; m += blockDim.x) Ty[m] = Tyg[m];
     const float2* src = S + ((int64_t)v * X + x) * g.NP;
-    for (int i = threadIdx.x; i < g.NP; i += blockDim.x) A[i] = src[i];
+    for (int i0 = threadIdx.x; i0 < g.NP; i0 += kLoadBatch * blockDim.x) {
+        float2 t[kLoadBatch];
+#pragma unroll
+        for (int b = 0; b < kLoadBatch; ++b) {
+            const int i = i0 + b * blockDim.x;
+            t[b] = i < g.NP ? __ldg(src + i) : make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int b = 0; b < kLoadBatch; ++b) {
+            const int i = i0 + b * blockDim.x;
+            if (i < g.NP) A[i] = t[b];
+        }
+    }
     __syncthreads();
     float2* R1 = fft_batch(A, B, g.rz, Nyh, 1, Nyh, Tz, 1.f, true);
     float2* O = R1 == A ? B : A;
@@ -365,7 +412,7 @@ fft_inv_kernel(const float2* __restrict__ S, const float2* __restrict__ Tzg,
     const int npairs = (Z + 1) / 2;
     const int half = Ny / 2;
     for (int i = threadIdx.x; i < npairs * Ny; i += blockDim.x) {
-        const int q = i / Ny, k = i - q * Ny;
+        const int q = div_small(i, rNy), k = i - q * Ny;
         const int za = 2 * q, zb = za + 1;
         const bool up = k > half;
         const int kk = up ? Ny - k : k;
@@ -380,7 +427,7 @@ fft_inv_kernel(const float2* __restrict__ S, const float2* __restrict__ Tzg,
     const float scale = 1.f / ((float)g.Nz * (float)Ny);
     float* ov = out + (int64_t)v * Z * X * Y + (int64_t)x * Y;
     for (int i = threadIdx.x; i < Z * Y; i += blockDim.x) {
-        const int z = i / Y, y = i - z * Y;
+        const int z = div_small(i, 1.f / (float)Y), y = i - z * Y;
         const float2 c = R2[(z >> 1) * Ny + y];
         const float r = ((z & 1) ? c.y : c.x) * scale;
         ov[(int64_t)z * X * Y + y] = mode == 1 ? expf(-r) : r;

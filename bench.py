@@ -75,12 +75,43 @@ def mlem_bytes_per_iter(A, S, H, W, R=1):
     return fwd + bwd + upd
 
 
-# DRAM bytes measured by ncu (profiles/cone_tma_kernel_6x128cube.md,
-# profiles/mlem_iter_kernel_24ang_16x128sq.md): the cone moves 19.66 MB per
-# 128^3 volume (read 100.76 MB + write 17.20 MB for 6 volumes); a fused MLEM
-# iteration moves 1.092 bytes per attenuation byte (27.51 MB for 25.17 MB).
-CONE_DRAM_BYTES_PER_VOLUME = (100.76e6 + 17.20e6) / 6
-MLEM_DRAM_PER_ATTEN_BYTE = 27.51e6 / (24 * 16 * 128 * 128 * 4)
+# DRAM bytes measured by ncu (profiles/spectral_cone_6x128cube.md,
+# profiles/mlem_iter_kernel_24ang_16x128sq.md): the spectral cone's five
+# kernels move 54.3 MB per 128^3 volume (325.8 MB read + write for 6
+# volumes); a fused MLEM iteration moves 1.092 bytes per attenuation byte
+# (27.53 MB for 25.17 MB).
+CONE_DRAM_BYTES_PER_VOLUME = 325.8e6 / 6
+MLEM_DRAM_PER_ATTEN_BYTE = 27.53e6 / (24 * 16 * 128 * 128 * 4)
+
+
+def smooth_even(n):
+    """Smallest even m >= n whose only prime factors are 2, 3 and 5 (the
+    spectral cone's transform lengths)."""
+    m = n + (n & 1)
+    while True:
+        k = m
+        for r in (2, 3, 5):
+            while k % r == 0:
+                k //= r
+        if k == 1:
+            return m
+        m += 2
+
+
+def spectral_cone_flops(Z, X, Y, Mz, Mx, My):
+    """FLOPs of the spectral cone for one volume: the depth correlation
+    (8 per complex multiply-add, every frequency of every target plane and
+    depth inside the volume) and the 2-D transforms (5 N log2 N per complex
+    transform of length N; rows in pairs, then the half-spectrum columns),
+    forward and inverse."""
+    hz, hy = Mz // 2, My // 2
+    Nz = smooth_even(Z + max(1, hz, Mz - 1 - hz))
+    Ny = smooth_even(Y + max(hy, My - 1 - hy))
+    Nyh = Ny // 2 + 1
+    pairs = sum(min(Mx, X - x) for x in range(X))
+    corr = 8.0 * Nz * Nyh * pairs
+    plane = ((Z + 1) // 2) * 5 * Ny * np.log2(Ny) + Nyh * 5 * Nz * np.log2(Nz)
+    return corr + 2 * X * plane, (Nz, Ny)
 
 
 def cone_work(mask, Z, H, W):
@@ -253,6 +284,7 @@ def run_ours(args, rank, world, device):
     # ---- derived figures ----------------------------------------------
     n_cone = sum(v for _, _, v in cone_ev)
     nnz, sep = cone_work(mask.astype(np.float32), N, N, N)
+    spec, nz_ny = spectral_cone_flops(N, N, N, *mask.shape)
     cone_launches = len(cone_ev)
     cone_avg_ms = t_cone / max(cone_launches, 1)
     vols_per_launch = n_cone / max(cone_launches, 1)
@@ -283,23 +315,11 @@ def run_ours(args, rank, world, device):
                    "l2": "inputs larger than L2 (attenuation %.1f GB per step)" % (L * A * N ** 3 * 4 / 1e9)},
         "corrected_proj_gbs": round(proj_gbs, 1) if proj_gbs else None,
         "corrected_proj_pct_hbm": round(100 * proj_gbs / hbm, 1) if proj_gbs else None,
-        "time_share": {"cone_tma_kernel": round(cone_share, 3),
+        "time_share": {"cone (spectral, 5 kernels per launch)": round(cone_share, 3),
                        "mlem (sens + fused iterations)": round(t_mlem / ms, 3) if ms else None},
+        # the dominant kernel: the fused MLEM iteration (with the sensitivity
+        # backward of each attenuation rebuild)
         "roofline": {
-            "kernel": "cone_tma_kernel (fluorescence cone path sum)",
-            "bound": "fp32",
-            "achieved": round(2 * sep * vols_per_launch / (cone_avg_ms * 1e-3) / 1e12, 2),
-            "peak": round(fp32_peak, 1),
-            "unit": "TFLOP/s",
-            "frac": round(2 * sep * vols_per_launch / (cone_avg_ms * 1e-3) / 1e12 / fp32_peak, 3),
-            "traffic": round(CONE_DRAM_BYTES_PER_VOLUME * vols_per_launch * (N / 128) ** 3),
-            "traffic_note": "ncu dram read+write of a 6-volume 128^3 launch, per volume, times volumes per launch",
-            "peak_kind": "nominal FP32 (148 SM x 128 lanes x 2 x 1965 MHz); no measured FP32 peak",
-            "algorithmic_unit": "separable FLOPs 2*sum(wz+wy) per output and depth = %.3g per volume" % (2 * sep),
-            "launches": cone_launches, "avg_ms": round(cone_avg_ms, 4),
-            "nnz_form_tflops": round(2 * nnz * vols_per_launch / (cone_avg_ms * 1e-3) / 1e12, 1),
-        },
-        "roofline_mlem": {
             "kernel": "mlem_iter_kernel (+ sensitivity backward)", "bound": "hbm",
             "achieved": round(proj_gbs, 1) if proj_gbs else None, "peak": hbm, "unit": "GB/s",
             "frac": round(proj_gbs / hbm, 3) if proj_gbs else None,
@@ -307,6 +327,21 @@ def run_ours(args, rank, world, device):
             "traffic_note": "per element-iteration: ncu dram bytes of a 24x16x128^2 iteration per attenuation byte, scaled",
             "peak_kind": peak_kind,
             "algorithmic_unit": "%.4g B per element-iteration (fwd + bwd + update at the reference API boundary)" % bytes_it,
+        },
+        "roofline_cone": {
+            "kernel": "spectral cone (fft_filter, fft_fwd, fft_corr, fft_inv, fft_apply)",
+            "bound": "fp32",
+            "achieved": round(spec * vols_per_launch / (cone_avg_ms * 1e-3) / 1e12, 2),
+            "peak": round(fp32_peak, 1),
+            "unit": "TFLOP/s",
+            "frac": round(spec * vols_per_launch / (cone_avg_ms * 1e-3) / 1e12 / fp32_peak, 3),
+            "traffic": round(CONE_DRAM_BYTES_PER_VOLUME * vols_per_launch * (N / 128) ** 3),
+            "traffic_note": "ncu dram read+write of the five kernels on 6 volumes of 128^3, per volume, times volumes per launch",
+            "peak_kind": "nominal FP32 (148 SM x 128 lanes x 2 x 1965 MHz); no measured FP32 peak",
+            "algorithmic_unit": "spectral FLOPs (depth correlation + 2-D FFTs, %dx%d padded planes) = %.3g per volume"
+                                % (nz_ny[0], nz_ny[1], spec),
+            "launches": cone_launches, "avg_ms": round(cone_avg_ms, 4),
+            "separable_equivalent_tflops": round(2 * sep * vols_per_launch / (cone_avg_ms * 1e-3) / 1e12, 1),
         },
         "e2e": {"value": round(e2e_value, 3), "unit": "MLEM iters/s",
                 "h2d_bytes_per_step": int(I_host.numel() * 4),

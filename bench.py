@@ -699,10 +699,12 @@ def run_case(args):
         cf = torch.full((A, L, n_ch), 0.01, device=dev)
         atten = torch.empty((L, A, N, N, N), device=dev)
         ws = torch.empty((n_a, L, N, N, N), device=dev)
+        nb = _lib.query("flc_atten_stage_workspace_bytes", n_ch, N, N, N)
+        ws4 = _lib.workspace(nb, dev)
         def once():
-            _lib.call("flc_atten_stage", _lib.ptr(frac), _lib.ptr(th), _lib.ptr(cx), _lib.ptr(cf),
-                      _lib.ptr(atten), _lib.ptr(ws), n_ch, N, N, N, A, L, 0, n_a, 0, 1,
-                      _lib.stream())
+            _lib.call("flc_atten_stage_ws", _lib.ptr(frac), _lib.ptr(th), _lib.ptr(cx),
+                      _lib.ptr(cf), _lib.ptr(atten), _lib.ptr(ws), n_ch, N, N, N, A, L, 0, n_a,
+                      0, 1, _lib.ptr(ws4), nb, _lib.stream())
     elif args.case in ("fwd", "bwd"):
         A, B = 120, 16
         atten = torch.rand((A, B, N, N), device=dev, generator=g)

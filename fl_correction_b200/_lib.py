@@ -47,6 +47,8 @@ SIGNATURES = {
     "flc_cone_atten_apply": (_int, [_vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _i64, _i64,
                                     _i64, _i64, _i64, _vp]),
     "flc_cone_fft_workspace_bytes": (_sz, [_i64] * 7),
+    "flc_atten_stage_workspace_bytes": (_sz, [_i64] * 4),
+    "flc_atten_stage_ws": (_int, [_vp] * 6 + [_i64] * 8 + [_int, _int, _vp, _sz, _vp]),
     "flc_cone_atten_apply_ws": (_int, [_vp, _vp, _vp, _vp] + [_i64] * 10 + [_vp, _sz, _vp]),
     "flc_xrf_workspace_bytes": (_sz, [_i64, _i64, _i64, _i64, _i64, _i64, _i64]),
     "flc_xrf_project": (_int, [_vp] * 8 + [_i64] * 9 + [_int, _i64, _vp, _sz, _vp]),

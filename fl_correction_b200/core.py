@@ -88,6 +88,9 @@ def atten_maps(frac_4D, angle_list, coef_x, coef_f, mask_uv=None, incident="own"
                                                           (Mz, Mx, My) if xrf else None)
     ws = workspace if workspace is not None and workspace.numel() >= ws_bytes else _lib.workspace(ws_bytes, dev)
     fft_ws = ctypes.c_void_p(ws.data_ptr() + mu_bytes) if fft_bytes else None
+    # the channel-interleaved fractions sit at the end of the pipeline part
+    frac4_bytes = int(_lib.query("flc_atten_stage_workspace_bytes", n_ch, S, H, W))
+    frac4_ws = ctypes.c_void_p(ws.data_ptr() + mu_bytes - frac4_bytes)
     mode = INCIDENT_MODES[incident]
     with torch.cuda.device(dev):
         st = _lib.stream()
@@ -99,9 +102,9 @@ def atten_maps(frac_4D, angle_list, coef_x, coef_f, mask_uv=None, incident="own"
         # same two stages per angle chunk, with CUDA events around each cone launch
         for a0 in range(0, A, chunk):
             n_a = min(chunk, A - a0)
-            _lib.call("flc_atten_stage", _lib.ptr(frac), _lib.ptr(theta), _lib.ptr(cx),
+            _lib.call("flc_atten_stage_ws", _lib.ptr(frac), _lib.ptr(theta), _lib.ptr(cx),
                       _lib.ptr(cf), _lib.ptr(out), _lib.ptr(ws), n_ch, S, H, W, A, L, a0, n_a,
-                      mode, 1 if xrf else 0, st)
+                      mode, 1 if xrf else 0, frac4_ws, frac4_bytes, st)
             if not xrf:
                 continue
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -114,8 +117,9 @@ def atten_maps(frac_4D, angle_list, coef_x, coef_f, mask_uv=None, incident="own"
 
 
 def atten_workspace_bytes(n_ch, S, H, W, A, L, chunk=0, mask_shape=None):
-    """(total, staged-mu, spectral-cone) workspace bytes of atten_maps for
-    `chunk` angles per pass (0: the default chunk).  mask_shape (Mz, Mx, My):
+    """(total, pipeline, spectral-cone) workspace bytes of atten_maps for
+    `chunk` angles per pass (0: the default chunk); the pipeline part holds
+    the staged mu of one chunk and the channel-interleaved fractions.  mask_shape (Mz, Mx, My):
     the cone's mask, None for the incident term alone; the spectral-cone part
     is 0 where that form does not take the shape."""
     chunk = pick_chunk(S, H, W, A, L, chunk)

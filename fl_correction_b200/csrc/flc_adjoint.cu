@@ -28,7 +28,8 @@ namespace flc {
 int atten_stage_launch(const float* frac, const float* theta, const float* coef_x,
                        const float* coef_f, float* out, float* mu_ref, int n_ch, int S, int H,
                        int W, int L, int64_t out_a_stride, int64_t out_l_stride, int a_base,
-                       int n_a, int incident_mode, int write_mu, cudaStream_t st, int out_a0);
+                       int n_a, int incident_mode, int write_mu, cudaStream_t st, int out_a0,
+                       const float4* frac4);
 int cone_sep_launch(const float* mu, const float* U, const float* Vw, float* out, int64_t Vn,
                     int64_t Z, int64_t X, int64_t Y, int64_t Mz, int64_t Mx, int64_t My, int mode,
                     int L, int a_base, int64_t out_a_stride, int64_t out_l_stride, cudaStream_t st);
@@ -277,7 +278,7 @@ extern "C" int flc_xrf_project(const float* frac, const float* theta, const floa
         // incident term straight into ATT, fluorescence mu into MU
         FLC_TRY(atten_stage_launch(frac, theta, coef_x, coef_f, b.ATT, b.MU, (int)n_ch, (int)S,
                                    (int)H, (int)W, (int)L, vol, (int64_t)n_a * vol, (int)a0, n_a,
-                                   incident_mode, 1, st, 0));
+                                   incident_mode, 1, st, 0, nullptr));
         FLC_TRY(cone_sep_launch(b.MU, u, v, b.ATT, (int64_t)n_a * L, S, W, H, Mz, Mx, My, 2,
                                 (int)L, 0, vol, (int64_t)n_a * vol, st));
         for (int64_t l = 0; l < L; ++l)
@@ -317,7 +318,7 @@ extern "C" int flc_xrf_project_adjoint(const float* frac, const float* theta, co
         // recompute the chunk: INC, E = exp(-cone), ATT = INC * E
         FLC_TRY(atten_stage_launch(frac, theta, coef_x, coef_f, b.INC, b.MU, (int)n_ch, (int)S,
                                    (int)H, (int)W, (int)L, vol, (int64_t)n_a * vol, (int)a0, n_a,
-                                   incident_mode, 1, st, 0));
+                                   incident_mode, 1, st, 0, nullptr));
         FLC_TRY(cone_sep_launch(b.MU, u, v, b.E, (int64_t)n_a * L, S, W, H, Mz, Mx, My, 3, (int)L,
                                 0, vol, (int64_t)n_a * vol, st));
         mul_kernel<<<(unsigned)ceil_div(nv, 256), 256, 0, st>>>(b.INC, b.E, b.ATT, nv);

@@ -80,9 +80,59 @@ struct StageCoef {
     float cf[kMaxL][kMaxCh];
 };
 
-// LM: lines held in registers (>= L).
-template <int LM>
-__global__ void atten_stage_kernel(const float* __restrict__ frac, const float* __restrict__ theta,
+// Channel-interleaved copy of the fractions: frac4[s][h][w][q] holds channels
+// 4q .. 4q+3 of pixel (s, h, w) (zero past n_ch), so that one bilinear tap of
+// every channel is G = ceil(n_ch / 4) 16-byte loads instead of n_ch scattered
+// 4-byte ones.
+__global__ void frac_interleave_kernel(const float* __restrict__ frac, float4* __restrict__ frac4,
+                                       int n_ch, int64_t n_pix, int G) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_pix) return;
+    for (int q = 0; q < G; ++q) {
+        float c[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int j = 4 * q + k;
+            c[k] = j < n_ch ? __ldg(frac + (int64_t)j * n_pix + i) : 0.f;
+        }
+        frac4[i * G + q] = make_float4(c[0], c[1], c[2], c[3]);
+    }
+}
+
+// rot_sample_tap (flc_geom.cuh) of the 4G channels of an interleaved slice at
+// once: the same taps, weights and operations per channel.
+template <int G>
+__device__ __forceinline__ void rot_sample_all(const float4* __restrict__ img, int H, int W,
+                                               const RotGeom& g, int h, int w, float (&fr)[kMaxCh]) {
+    const RotTap t = rot_tap(g, h, w);
+    const int x0 = t.x0, y0 = t.y0;
+    const bool xin0 = x0 >= 0 && x0 < W, xin1 = x0 + 1 >= 0 && x0 + 1 < W;
+    const bool yin0 = y0 >= 0 && y0 < H, yin1 = y0 + 1 >= 0 && y0 + 1 < H;
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int q = 0; q < G; ++q) {
+        const float4 v00 = (yin0 && xin0) ? __ldg(img + ((int64_t)y0 * W + x0) * G + q) : z4;
+        const float4 v01 = (yin0 && xin1) ? __ldg(img + ((int64_t)y0 * W + x0 + 1) * G + q) : z4;
+        const float4 v10 = (yin1 && xin0) ? __ldg(img + ((int64_t)(y0 + 1) * W + x0) * G + q) : z4;
+        const float4 v11 = (yin1 && xin1) ? __ldg(img + ((int64_t)(y0 + 1) * W + x0 + 1) * G + q) : z4;
+        const float a00[4] = {v00.x, v00.y, v00.z, v00.w}, a01[4] = {v01.x, v01.y, v01.z, v01.w};
+        const float a10[4] = {v10.x, v10.y, v10.z, v10.w}, a11[4] = {v11.x, v11.y, v11.z, v11.w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const float top = fmaf(t.tx, a01[k] - a00[k], a00[k]);
+            const float bot = fmaf(t.tx, a11[k] - a10[k], a10[k]);
+            fr[4 * q + k] = fmaf(t.ty, bot - top, top);
+        }
+    }
+#pragma unroll
+    for (int j = 4 * G; j < kMaxCh; ++j) fr[j] = 0.f;
+}
+
+// LM: lines held in registers (>= L).  G > 0: the rotation reads the
+// interleaved copy frac4 (G float4 per pixel); G == 0: the planar frac.
+template <int LM, int G>
+__global__ void atten_stage_kernel(const float* __restrict__ frac, const float4* __restrict__ frac4,
+                                   const float* __restrict__ theta,
                                    const float* __restrict__ coef_x,
                                    const float* __restrict__ coef_f, float* __restrict__ out,
                                    float* __restrict__ mu_ref, int n_ch, int S, int H, int W,
@@ -122,9 +172,14 @@ __global__ void atten_stage_kernel(const float* __restrict__ frac, const float* 
             if (r >= n) break;
             const int h = H - 1 - (y0 + r);
             float fr[kMaxCh];
+            if constexpr (G > 0) {
+                rot_sample_all<G>(frac4 + (int64_t)s * HW * G, H, W, g, h, w, fr);
+            } else {
 #pragma unroll
-            for (int j = 0; j < kMaxCh; ++j)
-                fr[j] = j < n_ch ? rot_sample(frac + ((int64_t)j * S + s) * HW, H, W, g, h, w) : 0.f;
+                for (int j = 0; j < kMaxCh; ++j)
+                    fr[j] = j < n_ch ? rot_sample(frac + ((int64_t)j * S + s) * HW, H, W, g, h, w)
+                                     : 0.f;
+            }
             // incident term: write the exclusive product, then fold in this voxel
             if (incident_mode != 2) {
 #pragma unroll
@@ -528,23 +583,55 @@ int64_t pick_chunk(int64_t S, int64_t H, int64_t W, int64_t A, int64_t L, int64_
     return chunk < 1 ? 1 : chunk;
 }
 
-size_t atten_ws_bytes(int64_t S, int64_t H, int64_t W, int64_t A, int64_t L, int64_t chunk) {
+int frac_groups(int64_t n_ch) { return (int)((n_ch + 3) / 4); }
+
+size_t frac4_bytes(int64_t n_ch, int64_t S, int64_t H, int64_t W) {
+    return align256(sizeof(float4) * frac_groups(n_ch) * S * H * W);
+}
+
+// Workspace of the attenuation pipeline: the staged mu of one chunk, then the
+// channel-interleaved fractions.
+size_t atten_ws_bytes(int64_t n_ch, int64_t S, int64_t H, int64_t W, int64_t A, int64_t L,
+                      int64_t chunk) {
     chunk = pick_chunk(S, H, W, A, L, chunk);
-    return align256(sizeof(float) * chunk * L * S * H * W);
+    return align256(sizeof(float) * chunk * L * S * H * W) + frac4_bytes(n_ch, S, H, W);
+}
+
+int frac_interleave_launch(const float* frac, float4* frac4, int64_t n_ch, int64_t S, int64_t H,
+                           int64_t W, cudaStream_t st) {
+    const int64_t n = S * H * W;
+    frac_interleave_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, st>>>(frac, frac4, (int)n_ch, n,
+                                                                       frac_groups(n_ch));
+    return check_launch("frac_interleave_kernel");
 }
 
 }  // namespace
 
+// frac4: the channel-interleaved copy (frac_interleave_launch) or nullptr
+// for the planar frac.
 int atten_stage_launch(const float* frac, const float* theta, const float* coef_x,
                        const float* coef_f, float* out, float* mu_ref, int n_ch, int S, int H,
                        int W, int L, int64_t out_a_stride, int64_t out_l_stride, int a_base,
-                       int n_a, int incident_mode, int write_mu, cudaStream_t st, int out_a0) {
+                       int n_a, int incident_mode, int write_mu, cudaStream_t st, int out_a0,
+                       const float4* frac4) {
     const int threads = (W + 31) & ~31;
-    auto kern = L <= 1 ? atten_stage_kernel<1> : L <= 2 ? atten_stage_kernel<2>
-              : L <= 4 ? atten_stage_kernel<4> : atten_stage_kernel<8>;
+    using K = void (*)(const float*, const float4*, const float*, const float*, const float*,
+                       float*, float*, int, int, int, int, int, int64_t, int64_t, int, int, int,
+                       int);
+    K kern;
+    const int G = frac4 ? frac_groups(n_ch) : 0;
+    if (G == 1)
+        kern = L <= 1 ? atten_stage_kernel<1, 1> : L <= 2 ? atten_stage_kernel<2, 1>
+             : L <= 4 ? atten_stage_kernel<4, 1> : atten_stage_kernel<8, 1>;
+    else if (G == 2)
+        kern = L <= 1 ? atten_stage_kernel<1, 2> : L <= 2 ? atten_stage_kernel<2, 2>
+             : L <= 4 ? atten_stage_kernel<4, 2> : atten_stage_kernel<8, 2>;
+    else
+        kern = L <= 1 ? atten_stage_kernel<1, 0> : L <= 2 ? atten_stage_kernel<2, 0>
+             : L <= 4 ? atten_stage_kernel<4, 0> : atten_stage_kernel<8, 0>;
     kern<<<dim3((unsigned)S, (unsigned)n_a), threads, 0, st>>>(
-        frac, theta, coef_x, coef_f, out, mu_ref, n_ch, S, H, W, L, out_a_stride, out_l_stride,
-        a_base, incident_mode, write_mu, out_a0 < 0 ? a_base : out_a0);
+        frac, frac4, theta, coef_x, coef_f, out, mu_ref, n_ch, S, H, W, L, out_a_stride,
+        out_l_stride, a_base, incident_mode, write_mu, out_a0 < 0 ? a_base : out_a0);
     return check_launch("atten_stage_kernel");
 }
 
@@ -555,16 +642,19 @@ int atten_maps_launch(const float* frac, const float* theta, const float* coef_x
                       int64_t chunk, void* workspace, size_t ws_bytes, cudaStream_t st) {
     chunk = pick_chunk(S, H, W, A, L, chunk);
     float* mu_ref = (float*)workspace;
-    // scratch of the spectral cone: the workspace past the staged mu
-    const size_t mu_bytes = atten_ws_bytes(S, H, W, A, L, chunk);
-    void* fft_ws = ws_bytes > mu_bytes ? (char*)workspace + mu_bytes : nullptr;
-    const size_t fft_bytes = ws_bytes > mu_bytes ? ws_bytes - mu_bytes : 0;
+    // the interleaved fractions follow the staged mu; the spectral cone's
+    // scratch is whatever the workspace holds past both
+    const size_t pipe_bytes = atten_ws_bytes(n_ch, S, H, W, A, L, chunk);
+    float4* frac4 = (float4*)((char*)workspace + (pipe_bytes - frac4_bytes(n_ch, S, H, W)));
+    void* fft_ws = ws_bytes > pipe_bytes ? (char*)workspace + pipe_bytes : nullptr;
+    const size_t fft_bytes = ws_bytes > pipe_bytes ? ws_bytes - pipe_bytes : 0;
+    FLC_TRY(frac_interleave_launch(frac, frac4, n_ch, S, H, W, st));
     const int64_t out_a = S * H * W, out_l = A * S * H * W;
     for (int64_t a0 = 0; a0 < A; a0 += chunk) {
         int n_a = (int)(A - a0 < chunk ? A - a0 : chunk);
         FLC_TRY(atten_stage_launch(frac, theta, coef_x, coef_f, out, mu_ref, (int)n_ch, (int)S,
                                    (int)H, (int)W, (int)L, out_a, out_l, (int)a0, n_a,
-                                   incident_mode, xrf_mode == 0, st, -1));
+                                   incident_mode, xrf_mode == 0, st, -1, frac4));
         if (xrf_mode != 0) continue;
         // reference frame of the cone: (Z=S, X=W, Y=H)
         FLC_TRY(cone_launch_ws(mu_ref, u, v, out, (int64_t)n_a * L, S, W, H, Mz, Mx, My, 2,
@@ -674,7 +764,7 @@ extern "C" int flc_cone_atten(const float* mu, const float* mask, float* out, in
 extern "C" size_t flc_atten_workspace_bytes(int64_t n_ch, int64_t S, int64_t H, int64_t W,
                                             int64_t A, int64_t L, int64_t chunk) {
     if (n_ch < 1 || S < 1 || H < 1 || W < 1 || A < 1 || L < 1) return 0;
-    return atten_ws_bytes(S, H, W, A, L, chunk);
+    return atten_ws_bytes(n_ch, S, H, W, A, L, chunk);
 }
 
 extern "C" int flc_atten_maps(const float* frac, const float* theta, const float* coef_x,
@@ -700,7 +790,7 @@ extern "C" int flc_atten_maps(const float* frac, const float* theta, const float
         set_error("flc_atten_maps: workspace must be 256-byte aligned");
         return FLC_ERR_ALIGNMENT;
     }
-    size_t need = atten_ws_bytes(S, H, W, A, L, chunk);
+    size_t need = atten_ws_bytes(n_ch, S, H, W, A, L, chunk);
     if (workspace_bytes < need) {
         set_error("flc_atten_maps: workspace of %zu bytes is smaller than the %zu required",
                   workspace_bytes, need);
@@ -728,7 +818,46 @@ extern "C" int flc_atten_stage(const float* frac, const float* theta, const floa
     FLC_REQUIRE(incident_mode >= 0 && incident_mode <= 2, "flc_atten_stage: bad incident_mode");
     return atten_stage_launch(frac, theta, coef_x, coef_f, out, mu_ref, (int)n_ch, (int)S, (int)H,
                               (int)W, (int)L, S * H * W, A * S * H * W, (int)a0, (int)n_a,
-                              incident_mode, write_mu, as_stream(stream), -1);
+                              incident_mode, write_mu, as_stream(stream), -1, nullptr);
+}
+
+extern "C" size_t flc_atten_stage_workspace_bytes(int64_t n_ch, int64_t S, int64_t H,
+                                                  int64_t W) {
+    if (n_ch < 1 || n_ch > kMaxCh || S < 1 || H < 1 || W < 1) return 0;
+    return frac4_bytes(n_ch, S, H, W);
+}
+
+extern "C" int flc_atten_stage_ws(const float* frac, const float* theta, const float* coef_x,
+                                  const float* coef_f, float* out, float* mu_ref, int64_t n_ch,
+                                  int64_t S, int64_t H, int64_t W, int64_t A, int64_t L,
+                                  int64_t a0, int64_t n_a, int incident_mode, int write_mu,
+                                  void* workspace, size_t workspace_bytes, void* stream) {
+    clear_error();
+    FLC_REQUIRE(frac && theta && coef_x && coef_f && out && (mu_ref || !write_mu) && workspace,
+                "flc_atten_stage_ws: null pointer argument");
+    FLC_REQUIRE(n_ch >= 1 && n_ch <= kMaxCh && L >= 1 && L <= kMaxL,
+                "flc_atten_stage_ws: 1 <= n_ch <= %d, 1 <= L <= %d", kMaxCh, kMaxL);
+    FLC_REQUIRE(H == W && H >= 2 && W <= 1024 && S >= 1 && S <= 65535,
+                "flc_atten_stage_ws: needs square slices, 2 <= H == W <= 1024");
+    FLC_REQUIRE(a0 >= 0 && n_a >= 1 && a0 + n_a <= A && n_a <= 65535,
+                "flc_atten_stage_ws: angle range [a0, a0+n_a) outside [0, A)");
+    FLC_REQUIRE(incident_mode >= 0 && incident_mode <= 2, "flc_atten_stage_ws: bad incident_mode");
+    if (((uintptr_t)workspace & 255) != 0) {
+        set_error("flc_atten_stage_ws: workspace must be 256-byte aligned");
+        return FLC_ERR_ALIGNMENT;
+    }
+    const size_t need = frac4_bytes(n_ch, S, H, W);
+    if (workspace_bytes < need) {
+        set_error("flc_atten_stage_ws: workspace of %zu bytes is smaller than the %zu required",
+                  workspace_bytes, need);
+        return FLC_ERR_WORKSPACE;
+    }
+    cudaStream_t st = as_stream(stream);
+    float4* frac4 = (float4*)workspace;
+    FLC_TRY(frac_interleave_launch(frac, frac4, n_ch, S, H, W, st));
+    return atten_stage_launch(frac, theta, coef_x, coef_f, out, mu_ref, (int)n_ch, (int)S, (int)H,
+                              (int)W, (int)L, S * H * W, A * S * H * W, (int)a0, (int)n_a,
+                              incident_mode, write_mu, st, -1, frac4);
 }
 
 extern "C" int flc_cone_atten_apply(const float* mu_ref, const float* u, const float* v,

@@ -192,6 +192,16 @@ FLC_API int flc_atten_stage(const float* frac, const float* theta, const float* 
                             const float* coef_f, float* out, float* mu_ref, int64_t n_ch,
                             int64_t S, int64_t H, int64_t W, int64_t A, int64_t L, int64_t a0,
                             int64_t n_a, int incident_mode, int write_mu, void* stream);
+/* flc_atten_stage with scratch (flc_atten_stage_workspace_bytes(n_ch, S, H,
+ * W) bytes, 256-byte aligned) for a channel-interleaved copy of frac, made
+ * on each call: the rotation then reads every channel's bilinear tap in one
+ * 16-byte load.  Same results as flc_atten_stage. */
+FLC_API size_t flc_atten_stage_workspace_bytes(int64_t n_ch, int64_t S, int64_t H, int64_t W);
+FLC_API int flc_atten_stage_ws(const float* frac, const float* theta, const float* coef_x,
+                               const float* coef_f, float* out, float* mu_ref, int64_t n_ch,
+                               int64_t S, int64_t H, int64_t W, int64_t A, int64_t L, int64_t a0,
+                               int64_t n_a, int incident_mode, int write_mu, void* workspace,
+                               size_t workspace_bytes, void* stream);
 FLC_API int flc_cone_atten_apply(const float* mu_ref, const float* u, const float* v,
                                  float* atten, int64_t n_a, int64_t L, int64_t S, int64_t H,
                                  int64_t W, int64_t A, int64_t a0, int64_t Mz, int64_t Mx,

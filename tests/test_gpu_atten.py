@@ -9,7 +9,7 @@ import pytest
 import torch
 
 from oracle import oracle as O
-from fl_correction_b200 import core, torch_functions as TF, torch_image_util as TIU
+from fl_correction_b200 import _lib, core, torch_functions as TF, torch_image_util as TIU
 from fl_correction_b200.detector_mask import generate_detector_mask
 from tests.helpers import TOL_MAP, T, atten_param, golden_cpu, rel_err
 
@@ -152,3 +152,35 @@ def test_errors_for_unsupported_requests():
         TIU.torch_rotate_image_nd(x, 0.3, enable_crop=False)
     with pytest.raises(RuntimeError):
         TIU.torch_rot90_4D(torch.zeros((1, 3, 4, 5)), 0, "clock")
+
+
+@pytest.mark.parametrize("n_ch,L", [(3, 2), (4, 3), (6, 4), (8, 1)])
+def test_interleaved_stage_matches_planar(n_ch, L):
+    # the stage reading a channel-interleaved copy of the fractions gives the
+    # planar stage's incident terms and staged mu within the map tolerance (the
+    # two builds of the kernel may fuse the multiply-adds of the rotated
+    # coordinates differently, which moves a bilinear weight by an ulp)
+    rng = np.random.default_rng(n_ch * 10 + L)
+    S, N, A, a0, n_a = 5, 20, 6, 1, 4
+    frac = T(rng.random((n_ch, S, N, N)).astype(np.float32))
+    th = T(np.deg2rad(np.array([0, 17, 45, 90, 133.0, 271])).astype(np.float32))
+    cx = T(rng.uniform(0.01, 0.05, (A, n_ch)).astype(np.float32))
+    cf = T(rng.uniform(0.01, 0.05, (A, L, n_ch)).astype(np.float32))
+    outs = []
+    for ws_entry in (False, True):
+        out = torch.zeros((L, A, S, N, N), device="cuda")
+        mu = torch.zeros((n_a, L, S, N, N), device="cuda")
+        for mode in (0, 1):
+            if ws_entry:
+                nb = _lib.query("flc_atten_stage_workspace_bytes", n_ch, S, N, N)
+                ws = _lib.workspace(nb, "cuda")
+                _lib.call("flc_atten_stage_ws", _lib.ptr(frac), _lib.ptr(th), _lib.ptr(cx),
+                          _lib.ptr(cf), _lib.ptr(out), _lib.ptr(mu), n_ch, S, N, N, A, L, a0, n_a,
+                          mode, 1, _lib.ptr(ws), nb, _lib.stream())
+            else:
+                _lib.call("flc_atten_stage", _lib.ptr(frac), _lib.ptr(th), _lib.ptr(cx),
+                          _lib.ptr(cf), _lib.ptr(out), _lib.ptr(mu), n_ch, S, N, N, A, L, a0, n_a,
+                          mode, 1, _lib.stream())
+            outs.append((out.cpu().numpy().copy(), mu.cpu().numpy().copy()))
+    for (o1, m1), (o2, m2) in zip(outs[:2], outs[2:]):
+        assert rel_err(o2, o1) < TOL_MAP and rel_err(m2, m1) < TOL_MAP

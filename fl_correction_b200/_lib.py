@@ -51,6 +51,7 @@ SIGNATURES = {
     "flc_atten_stage_ws": (_int, [_vp] * 6 + [_i64] * 8 + [_int, _int, _vp, _sz, _vp]),
     "flc_cone_atten_apply_ws": (_int, [_vp, _vp, _vp, _vp] + [_i64] * 10 + [_vp, _sz, _vp]),
     "flc_xrf_workspace_bytes": (_sz, [_i64, _i64, _i64, _i64, _i64, _i64, _i64]),
+    "flc_xrf_workspace_bytes_ex": (_sz, [_i64] * 10),
     "flc_xrf_project": (_int, [_vp] * 8 + [_i64] * 9 + [_int, _i64, _vp, _sz, _vp]),
     "flc_xrf_project_adjoint": (_int, [_vp] * 11 + [_i64] * 9 + [_int, _i64, _vp, _sz, _vp]),
     "flc_rotate": (_int, [_vp, _vp, _i64, _i64, _i64, _f32, _f32, _vp]),

@@ -30,9 +30,15 @@ int atten_stage_launch(const float* frac, const float* theta, const float* coef_
                        int W, int L, int64_t out_a_stride, int64_t out_l_stride, int a_base,
                        int n_a, int incident_mode, int write_mu, cudaStream_t st, int out_a0,
                        const float4* frac4);
-int cone_sep_launch(const float* mu, const float* U, const float* Vw, float* out, int64_t Vn,
-                    int64_t Z, int64_t X, int64_t Y, int64_t Mz, int64_t Mx, int64_t My, int mode,
-                    int L, int a_base, int64_t out_a_stride, int64_t out_l_stride, cudaStream_t st);
+int cone_launch_ws(const float* mu, const float* U, const float* Vw, float* out, int64_t Vn,
+                   int64_t Z, int64_t X, int64_t Y, int64_t Mz, int64_t Mx, int64_t My, int mode,
+                   int L, int a_base, int64_t out_a_stride, int64_t out_l_stride, void* ws,
+                   size_t ws_bytes, cudaStream_t st);
+size_t cone_fft_ws_bytes(int64_t Vn, int64_t Z, int64_t X, int64_t Y, int64_t Mz, int64_t Mx,
+                         int64_t My, int mode);
+size_t frac4_bytes(int64_t n_ch, int64_t S, int64_t H, int64_t W);
+int frac_interleave_launch(const float* frac, float4* frac4, int64_t n_ch, int64_t S, int64_t H,
+                           int64_t W, cudaStream_t st);
 int fwd_emission_launch(const float* atten, const float* C, const float* em, const float* theta,
                         float* Pf, const float* I, int64_t A, int64_t B, int64_t R, int64_t H,
                         int64_t W, cudaStream_t st);
@@ -243,6 +249,32 @@ size_t xrf_ws_bytes(int64_t S, int64_t H, int64_t W, int64_t A, int64_t L, int64
     return xrf_layout(S, H, W, L, xrf_chunk(S, H, W, A, L, chunk), nullptr, nullptr);
 }
 
+namespace {
+
+// Optional scratch past the base layout: the channel-interleaved fractions
+// (the stage's taps in 16-byte loads), then the spectral cone's scratch.
+// Either is left out (nullptr / 0) when the workspace is too small for it;
+// the planar stage and the direct cone kernels then run.
+struct XrfExtra {
+    float4* frac4;
+    void* fft;
+    size_t fft_bytes;
+};
+
+XrfExtra xrf_extra(char* ws, size_t ws_bytes, size_t base, int64_t n_ch, int64_t S, int64_t H,
+                   int64_t W) {
+    XrfExtra x{nullptr, nullptr, 0};
+    const size_t f4 = frac4_bytes(n_ch, S, H, W);
+    if (ws_bytes >= base + f4) {
+        x.frac4 = (float4*)(ws + base);
+        x.fft = ws + base + f4;
+        x.fft_bytes = ws_bytes - base - f4;
+    }
+    return x;
+}
+
+}  // namespace
+
 }  // namespace flc
 
 using namespace flc;
@@ -251,6 +283,18 @@ extern "C" size_t flc_xrf_workspace_bytes(int64_t n_ch, int64_t S, int64_t H, in
                                           int64_t L, int64_t chunk) {
     if (n_ch < 1 || S < 1 || H < 1 || W < 1 || A < 1 || L < 1) return 0;
     return xrf_ws_bytes(S, H, W, A, L, chunk);
+}
+
+extern "C" size_t flc_xrf_workspace_bytes_ex(int64_t n_ch, int64_t S, int64_t H, int64_t W,
+                                             int64_t A, int64_t L, int64_t chunk, int64_t Mz,
+                                             int64_t Mx, int64_t My) {
+    if (n_ch < 1 || n_ch > kMaxCh || S < 1 || H < 1 || W < 1 || A < 1 || L < 1 || Mz < 1 ||
+        Mx < 1 || My < 1)
+        return 0;
+    const int64_t c = xrf_chunk(S, H, W, A, L, chunk);
+    // cone frame (Z = S, X = W, Y = H); the beam-layout modes need the most
+    return xrf_ws_bytes(S, H, W, A, L, chunk) + frac4_bytes(n_ch, S, H, W) +
+           cone_fft_ws_bytes(c * L, S, W, H, Mz, Mx, My, 2);
 }
 
 extern "C" int flc_xrf_project(const float* frac, const float* theta, const float* coef_x,
@@ -272,15 +316,17 @@ extern "C" int flc_xrf_project(const float* frac, const float* theta, const floa
     cudaStream_t st = as_stream(stream);
     XrfBufs b;
     xrf_layout(S, H, W, L, chunk, (char*)workspace, &b);
+    const XrfExtra x = xrf_extra((char*)workspace, workspace_bytes, need, n_ch, S, H, W);
+    if (x.frac4) FLC_TRY(frac_interleave_launch(frac, x.frac4, n_ch, S, H, W, st));
     const int64_t vol = S * H * W;
     for (int64_t a0 = 0; a0 < A; a0 += chunk) {
         const int n_a = (int)(A - a0 < chunk ? A - a0 : chunk);
         // incident term straight into ATT, fluorescence mu into MU
         FLC_TRY(atten_stage_launch(frac, theta, coef_x, coef_f, b.ATT, b.MU, (int)n_ch, (int)S,
                                    (int)H, (int)W, (int)L, vol, (int64_t)n_a * vol, (int)a0, n_a,
-                                   incident_mode, 1, st, 0, nullptr));
-        FLC_TRY(cone_sep_launch(b.MU, u, v, b.ATT, (int64_t)n_a * L, S, W, H, Mz, Mx, My, 2,
-                                (int)L, 0, vol, (int64_t)n_a * vol, st));
+                                   incident_mode, 1, st, 0, x.frac4));
+        FLC_TRY(cone_launch_ws(b.MU, u, v, b.ATT, (int64_t)n_a * L, S, W, H, Mz, Mx, My, 2,
+                               (int)L, 0, vol, (int64_t)n_a * vol, x.fft, x.fft_bytes, st));
         for (int64_t l = 0; l < L; ++l)
             FLC_TRY(fwd_emission_launch(b.ATT + l * n_a * vol, frac + l * vol, em + l * A + a0,
                                         theta + a0, Pf + (l * A + a0) * S * W, nullptr, n_a, S, 1,
@@ -310,6 +356,8 @@ extern "C" int flc_xrf_project_adjoint(const float* frac, const float* theta, co
     cudaStream_t st = as_stream(stream);
     XrfBufs b;
     xrf_layout(S, H, W, L, chunk, (char*)workspace, &b);
+    const XrfExtra x = xrf_extra((char*)workspace, workspace_bytes, need, n_ch, S, H, W);
+    if (x.frac4) FLC_TRY(frac_interleave_launch(frac, x.frac4, n_ch, S, H, W, st));
     const int64_t vol = S * H * W;
     FLC_TRY_CUDA(cudaMemsetAsync(dC, 0, sizeof(float) * L * vol, st));
     for (int64_t a0 = 0; a0 < A; a0 += chunk) {
@@ -318,9 +366,9 @@ extern "C" int flc_xrf_project_adjoint(const float* frac, const float* theta, co
         // recompute the chunk: INC, E = exp(-cone), ATT = INC * E
         FLC_TRY(atten_stage_launch(frac, theta, coef_x, coef_f, b.INC, b.MU, (int)n_ch, (int)S,
                                    (int)H, (int)W, (int)L, vol, (int64_t)n_a * vol, (int)a0, n_a,
-                                   incident_mode, 1, st, 0, nullptr));
-        FLC_TRY(cone_sep_launch(b.MU, u, v, b.E, (int64_t)n_a * L, S, W, H, Mz, Mx, My, 3, (int)L,
-                                0, vol, (int64_t)n_a * vol, st));
+                                   incident_mode, 1, st, 0, x.frac4));
+        FLC_TRY(cone_launch_ws(b.MU, u, v, b.E, (int64_t)n_a * L, S, W, H, Mz, Mx, My, 3, (int)L,
+                               0, vol, (int64_t)n_a * vol, x.fft, x.fft_bytes, st));
         mul_kernel<<<(unsigned)ceil_div(nv, 256), 256, 0, st>>>(b.INC, b.E, b.ATT, nv);
         FLC_TRY(check_launch("mul_kernel"));
         // direct term: P^T[atten](dL/dPf) per element
@@ -337,8 +385,8 @@ extern "C" int flc_xrf_project_adjoint(const float* frac, const float* theta, co
                                                   (int)L, (int)A, (int)a0, n_a, (int)S, (int)H,
                                                   (int)W);
         FLC_TRY(check_launch("xrf_g_kernel"));
-        FLC_TRY(cone_sep_launch(b.DRES, uf, vf, b.DMU, (int64_t)n_a * L, S, W, H, Mz, Mx, My, 0,
-                                1, 0, 0, 0, st));
+        FLC_TRY(cone_launch_ws(b.DRES, uf, vf, b.DMU, (int64_t)n_a * L, S, W, H, Mz, Mx, My, 0,
+                               1, 0, 0, 0, x.fft, x.fft_bytes, st));
         const int threads = (int)((W + 31) & ~31);
         xrf_stage_adjoint_kernel<<<dim3((unsigned)S, (unsigned)n_a), threads, 0, st>>>(
             frac, theta, coef_x, coef_f, b.INC, b.DINC, b.DMU, dC, (int)n_ch, (int)S, (int)H,

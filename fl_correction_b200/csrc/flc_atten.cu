@@ -510,8 +510,6 @@ int cone_sep_launch(const float* mu, const float* U, const float* Vw, float* out
     return check_launch("cone_sep_kernel");
 }
 
-namespace {
-
 // Cone path sum with scratch for the spectral form: the spectral kernels run
 // when the "cone.variant" knob allows them (0 automatic, 4 spectral) and the
 // shape and scratch fit; otherwise cone_sep_launch.
@@ -529,6 +527,8 @@ int cone_launch_ws(const float* mu, const float* U, const float* Vw, float* out,
     return cone_sep_launch(mu, U, Vw, out, Vn, Z, X, Y, Mz, Mx, My, mode, L, a_base, out_a_stride,
                            out_l_stride, st);
 }
+
+namespace {
 
 // Splits each depth plane of a host mask into u (Mz) x v (My) if it is rank
 // one to FP32 precision.  Returns false otherwise.
@@ -583,6 +583,8 @@ int64_t pick_chunk(int64_t S, int64_t H, int64_t W, int64_t A, int64_t L, int64_
     return chunk < 1 ? 1 : chunk;
 }
 
+}  // namespace
+
 int frac_groups(int64_t n_ch) { return (int)((n_ch + 3) / 4); }
 
 size_t frac4_bytes(int64_t n_ch, int64_t S, int64_t H, int64_t W) {
@@ -604,8 +606,6 @@ int frac_interleave_launch(const float* frac, float4* frac4, int64_t n_ch, int64
                                                                        frac_groups(n_ch));
     return check_launch("frac_interleave_kernel");
 }
-
-}  // namespace
 
 // frac4: the channel-interleaved copy (frac_interleave_launch) or nullptr
 // for the planar frac.

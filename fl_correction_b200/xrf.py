@@ -64,8 +64,9 @@ class XRFProjector:
                   else np.ones((self.n_ch - self.L, S, H, W), np.float32))
             self.frac[self.L:] = torch.as_tensor(ff, dtype=torch.float32, device=dev)
         self.chunk = int(chunk)
-        self.ws_bytes = _lib.query("flc_xrf_workspace_bytes", self.n_ch, S, H, W, A, self.L,
-                                   self.chunk)
+        # with room for the interleaved fractions and the spectral cone's scratch
+        self.ws_bytes = _lib.query("flc_xrf_workspace_bytes_ex", self.n_ch, S, H, W, A, self.L,
+                                   self.chunk, *self.mask_shape)
         self.ws = _lib.workspace(self.ws_bytes, dev)
 
     def _args(self):

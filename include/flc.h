@@ -231,13 +231,19 @@ FLC_API int flc_cone_atten_apply_ws(const float* mu_ref, const float* u, const f
  *   dependence of the attenuation on C (rotation, mu assembly, incident scan
  *   and cone are differentiated by hand).  uf, vf are u, v with the taps of
  *   every depth reversed (uf[d][k] = u[d][Mz-1-k]); Mz and My must be odd.
- * Both take flc_xrf_workspace_bytes(...) of scratch (256-byte aligned).
+ * Both take flc_xrf_workspace_bytes(...) of scratch (256-byte aligned);
+ * with flc_xrf_workspace_bytes_ex(..., Mz, Mx, My) bytes they also keep a
+ * channel-interleaved copy of frac for the stage and run the spectral cone
+ * where its planes fit (same results to FP32 rounding).
  * Counterpart: the reference differentiates only the projector in C
  * (FL/cuda_lib/autograd.py:5-77) with attenuation held fixed
  * (FL/example/demo.py:413-475); this is the full-mu extension of that path.
  * --------------------------------------------------------------------- */
 FLC_API size_t flc_xrf_workspace_bytes(int64_t n_ch, int64_t S, int64_t H, int64_t W, int64_t A,
                                        int64_t L, int64_t chunk);
+FLC_API size_t flc_xrf_workspace_bytes_ex(int64_t n_ch, int64_t S, int64_t H, int64_t W,
+                                          int64_t A, int64_t L, int64_t chunk, int64_t Mz,
+                                          int64_t Mx, int64_t My);
 FLC_API int flc_xrf_project(const float* frac, const float* theta, const float* coef_x,
                             const float* coef_f, const float* u, const float* v, const float* em,
                             float* Pf, int64_t n_ch, int64_t S, int64_t H, int64_t W, int64_t A,

@@ -719,16 +719,26 @@ extern "C" int flc_cone_atten(const float* mu, const float* mask, float* out, in
                K <= 65535 && sep_threads((int)Z) <= kSepMaxThreads &&
                sep_smem(sep_dims(Z, X, Y, Mz, Mx, My)) <= (size_t)max_smem_optin();
     if (sep) {
+        // the factors, then (256-byte aligned) the spectral form's scratch
+        // where the shape takes it
         float* dbuf = nullptr;
-        size_t bytes = sizeof(float) * (U.size() + V.size());
+        const size_t fbytes = align256(sizeof(float) * (U.size() + V.size()));
+        const size_t fft_bytes = cone_fft_ws_bytes(K, Z, X, Y, Mz, Mx, My, 0);
+        const size_t bytes = fbytes + (fft_bytes ? fft_bytes + 256 : 0);
         FLC_TRY_CUDA(cudaMallocAsync((void**)&dbuf, bytes, st));
         int s = FLC_OK;
         cudaError_t e = cudaMemcpyAsync(dbuf, U.data(), sizeof(float) * U.size(), cudaMemcpyHostToDevice, st);
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(dbuf + U.size(), V.data(), sizeof(float) * V.size(), cudaMemcpyHostToDevice, st);
         if (e != cudaSuccess) s = cuda_fail(e, "cudaMemcpyAsync");
+        void* fft_ws = nullptr;
+        if (fft_bytes) {
+            const uintptr_t p = ((uintptr_t)dbuf + fbytes + 255) & ~(uintptr_t)255;
+            fft_ws = (void*)p;
+        }
         if (s == FLC_OK)
-            s = cone_sep_launch(mu, dbuf, dbuf + U.size(), out, K, Z, X, Y, Mz, Mx, My, 0, 1, 0, 0, 0, st);
+            s = cone_launch_ws(mu, dbuf, dbuf + U.size(), out, K, Z, X, Y, Mz, Mx, My, 0, 1, 0, 0,
+                               0, fft_ws, fft_bytes, st);
         cudaFreeAsync(dbuf, st);
         // the host vectors are read by the copies above before they return
         cudaStreamSynchronize(st);

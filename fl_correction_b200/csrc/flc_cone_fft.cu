@@ -23,7 +23,7 @@
 //   fft_filter_kernel : G (Mx x Nz x Nyh) and the twiddle tables, FP64 -> FP32
 //   fft_fwd_kernel    : one CTA per (volume, plane): rows (two real rows per
 //                       complex FFT), then columns; writes P
-//   fft_corr_kernel   : one CTA per (volume, 32 frequencies): R_x for all x,
+//   fft_corr_kernel   : one CTA per (volume, 16 frequencies): R_x for all x,
 //                       written over P in place
 //   fft_inv_kernel    : one CTA per (volume, plane x): columns, then rows
 //                       (two real rows per complex FFT); writes res or
@@ -41,7 +41,7 @@ namespace flc {
 namespace {
 
 constexpr int kFftThreads = 1024;
-constexpr int kCorrK = 32;       // frequencies per correlation CTA, one per lane
+constexpr int kCorrK = 16;       // frequencies per correlation CTA, one per lane of each half-warp
 constexpr int kCorrWarps = 8;
 constexpr int kMaxStages = 16;
 constexpr int kLoadBatch = 4;    // global loads per thread issued before their shared stores
@@ -289,26 +289,31 @@ fft_fwd_kernel(const float* __restrict__ mu, const float2* __restrict__ Tzg,
 }
 
 // R_x(k) = sum_{d < min(Mx, X - x)} G_d(k) P_{x+d}(k), over P in place
-// (grid (ceil(NP / 32), Vn), kCorrWarps warps).  Lane = frequency; a warp
-// owns groups of 8 consecutive x, paired first with last so that every warp
-// sums about the same number of depths.  P rows past X and G rows past Mx
-// are zero in shared memory, so the blocks of 8 depths need no edge tests.
-__global__ void __launch_bounds__(kCorrWarps * 32)
+// (grid (ceil(NP / 16), Vn), kCorrWarps warps).  The two half-warps take the
+// same 16 frequencies (one per lane) and split each group's depth range, so
+// a CTA needs half the shared memory of one frequency per lane and four CTAs
+// fit an SM; a shuffle adds the two halves' sums at the end.  A warp owns
+// groups of 8 consecutive x, paired first with last so that every warp sums
+// about the same number of depths.  P rows past X and G rows past Mx are
+// zero in shared memory, so the blocks of 8 depths need no edge tests.
+__global__ void __launch_bounds__(kCorrWarps * 32, 4)
 fft_corr_kernel(float2* __restrict__ S, const float2* __restrict__ G, FftGeom g) {
     extern __shared__ __align__(16) float2 sc[];
     const int X = g.X, Mx = g.Mx;
     const int prow = X + Mx + 16, grow = Mx + 8;
-    float2* sP = sc;                       // [prow][32]
-    float2* sG = sP + (size_t)prow * kCorrK;   // [grow][32]
+    float2* sP = sc;                           // [prow][16]
+    float2* sG = sP + (size_t)prow * kCorrK;   // [grow][16]
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int k = blockIdx.x * kCorrK + lane;
+    const int half = lane >> 4, l16 = lane & 15;
+    const int k = blockIdx.x * kCorrK + l16;
     const bool kin = k < g.NP;
     float2* Sv = S + (int64_t)blockIdx.y * X * g.NP;
-    for (int r0 = warp; r0 < prow + grow; r0 += kLoadBatch * kCorrWarps) {
+    // a warp loads two rows per step, one per half
+    for (int r0 = 2 * warp; r0 < prow + grow; r0 += kLoadBatch * 2 * kCorrWarps) {
         float2 t[kLoadBatch];
 #pragma unroll
         for (int b = 0; b < kLoadBatch; ++b) {
-            const int r = r0 + b * kCorrWarps;
+            const int r = r0 + b * 2 * kCorrWarps + half;
             const bool p = r < prow;
             const int rr = p ? r : r - prow;
             t[b] = (kin && (p ? rr < X : rr < Mx))
@@ -317,8 +322,8 @@ fft_corr_kernel(float2* __restrict__ S, const float2* __restrict__ G, FftGeom g)
         }
 #pragma unroll
         for (int b = 0; b < kLoadBatch; ++b) {
-            const int r = r0 + b * kCorrWarps;
-            if (r < prow + grow) sc[r * kCorrK + lane] = t[b];   // sG follows sP
+            const int r = r0 + b * 2 * kCorrWarps + half;
+            if (r < prow + grow) sc[r * kCorrK + l16] = t[b];   // sG follows sP
         }
     }
     __syncthreads();
@@ -329,33 +334,37 @@ fft_corr_kernel(float2* __restrict__ S, const float2* __restrict__ G, FftGeom g)
             if (side && grp == gi) break;
             const int x0 = 8 * grp;
             const int dmax = min(Mx, X - x0);
+            // half 0: depths [0, dsplit), half 1: [dsplit, dmax); dsplit is a
+            // multiple of 8 near dmax / 2
+            const int dsplit = ((dmax + 15) / 16) * 8;
+            const int dlo = half ? dsplit : 0, dhi = half ? dmax : dsplit;
             float2 acc[8];
 #pragma unroll
             for (int t = 0; t < 8; ++t) acc[t] = make_float2(0.f, 0.f);
             float2 lo[8], hi[8];
 #pragma unroll
-            for (int i = 0; i < 8; ++i) lo[i] = sP[(x0 + i) * kCorrK + lane];
+            for (int i = 0; i < 8; ++i) lo[i] = sP[(x0 + dlo + i) * kCorrK + l16];
 #define FLC_CMAC(A, W)                                   \
     A.x = fmaf(gv.x, W.x, fmaf(-gv.y, W.y, A.x));       \
     A.y = fmaf(gv.x, W.y, fmaf(gv.y, W.x, A.y));
-            for (int d0 = 0; d0 < dmax; d0 += 16) {
+            for (int d0 = dlo; d0 < dhi; d0 += 16) {
 #pragma unroll
-                for (int i = 0; i < 8; ++i) hi[i] = sP[(x0 + d0 + 8 + i) * kCorrK + lane];
+                for (int i = 0; i < 8; ++i) hi[i] = sP[(x0 + d0 + 8 + i) * kCorrK + l16];
 #pragma unroll
                 for (int e = 0; e < 8; ++e) {
-                    const float2 gv = sG[(d0 + e) * kCorrK + lane];
+                    const float2 gv = sG[(d0 + e) * kCorrK + l16];
 #pragma unroll
                     for (int t = 0; t < 8; ++t) {
                         if (t + e < 8) { FLC_CMAC(acc[t], lo[t + e]) }
                         else { FLC_CMAC(acc[t], hi[t + e - 8]) }
                     }
                 }
-                if (d0 + 8 >= dmax) break;
+                if (d0 + 8 >= dhi) break;
 #pragma unroll
-                for (int i = 0; i < 8; ++i) lo[i] = sP[(x0 + d0 + 16 + i) * kCorrK + lane];
+                for (int i = 0; i < 8; ++i) lo[i] = sP[(x0 + d0 + 16 + i) * kCorrK + l16];
 #pragma unroll
                 for (int e = 0; e < 8; ++e) {
-                    const float2 gv = sG[(d0 + 8 + e) * kCorrK + lane];
+                    const float2 gv = sG[(d0 + 8 + e) * kCorrK + l16];
 #pragma unroll
                     for (int t = 0; t < 8; ++t) {
                         if (t + e < 8) { FLC_CMAC(acc[t], hi[t + e]) }
@@ -364,7 +373,12 @@ fft_corr_kernel(float2* __restrict__ S, const float2* __restrict__ G, FftGeom g)
                 }
             }
 #undef FLC_CMAC
-            if (kin) {
+#pragma unroll
+            for (int t = 0; t < 8; ++t) {
+                acc[t].x += __shfl_xor_sync(0xffffffffu, acc[t].x, 16);
+                acc[t].y += __shfl_xor_sync(0xffffffffu, acc[t].y, 16);
+            }
+            if (kin && half == 0) {
 #pragma unroll
                 for (int t = 0; t < 8; ++t)
                     if (x0 + t < X) Sv[(int64_t)(x0 + t) * g.NP + k] = acc[t];

@@ -78,8 +78,11 @@ FLC_API int64_t flc_tune_get(const char* name);
  *   out[k,z,x,y] = sum_{dz,dx,dy} mask[dz,dx,dy] * mu[k, z+dz-Mz/2, x+dx, y+dy-My/2]
  * with taps outside the volume skipped.  mu (K,Z,X,Y), mask (Mz,Mx,My).
  * When every depth plane mask[:,dx,:] is rank one (true of the masks that
- * FL.detector_mask builds) the separable kernel runs; otherwise a general
- * gather over the non-zero taps.  `flags` is a bit set of FLC_CONE_*.
+ * FL.detector_mask builds) the separable forms run -- the spectral form where
+ * the padded planes fit in shared memory (its scratch is allocated with
+ * cudaMallocAsync and freed on the same stream), else the direct separable
+ * kernel; otherwise a general gather over the non-zero taps.  `flags` is a
+ * bit set of FLC_CONE_*.
  * --------------------------------------------------------------------- */
 #define FLC_CONE_FORCE_GENERAL 1  /* skip the rank-one test, use the general kernel */
 #define FLC_CONE_PLAIN_KERNEL 16  /* separable: plain kernel, not the TMA pipeline */

@@ -76,6 +76,16 @@ def test_workspace_queries():
     assert lib.flc_mlem_workspace_bytes(120, 128, 1, 128, 128) >= 3 * 4 * 128 ** 3
     assert lib.flc_mlem_workspace_bytes(0, 1, 1, 1, 1) == 0
     assert lib.flc_atten_workspace_bytes(4, 128, 128, 128, 120, 3, 2) >= 2 * 3 * 4 * 128 ** 3
+    # the pipeline part: the staged mu of a chunk, then the channel-interleaved
+    # fractions (one float4 per pixel per four channels)
+    v = 128 ** 3
+    assert lib.flc_atten_stage_workspace_bytes(4, 128, 128, 128) == 16 * v
+    assert lib.flc_atten_stage_workspace_bytes(5, 128, 128, 128) == 32 * v
+    assert lib.flc_atten_stage_workspace_bytes(9, 128, 128, 128) == 0      # more than 8 channels
+    assert lib.flc_atten_workspace_bytes(4, 128, 128, 128, 120, 3, 2) == 2 * 3 * 4 * v + 16 * v
+    # the extended adjoint workspace holds the base one and the interleaved fractions
+    base = lib.flc_xrf_workspace_bytes(4, 96, 96, 96, 90, 3, 0)
+    assert lib.flc_xrf_workspace_bytes_ex(4, 96, 96, 96, 90, 3, 0, 25, 96, 25) >= base + 16 * 96 ** 3
 
 
 def test_cpu_tensors_fail_loudly():

@@ -46,6 +46,11 @@ def parse():
                    help="0/1: corrected MLEM (1 is the benchmark); 2/4: gradient "
                         "reconstruction; 3: batched uneven volumes")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-parity", action="store_true",
+                   help="skip the parity leg (errors of the result against the reference's "
+                        "kernels and the FP64 oracle)")
+    p.add_argument("--no-ref-gpu", action="store_true",
+                   help="skip timing the reference's own CUDA kernels on this GPU")
     p.add_argument("--adam-steps", type=int, default=0,
                    help="configurations 2/4: Adam steps timed (default 200 / 3)")
     p.add_argument("--case", default=None, choices=["cone", "cone_direct", "mlem", "fwd", "bwd", "stage"],
@@ -75,11 +80,10 @@ def mlem_bytes_per_iter(A, S, H, W, R=1):
     return fwd + bwd + upd
 
 
-# DRAM bytes measured by ncu (profiles/spectral_cone_6x128cube.md,
-# profiles/mlem_iter_kernel_24ang_16x128sq.md): the spectral cone's five
-# kernels move 54.3 MB per 128^3 volume (325.8 MB read + write for 6
-# volumes); a fused MLEM iteration moves 1.092 bytes per attenuation byte
-# (27.53 MB for 25.17 MB).
+# DRAM bytes measured by ncu on small cases of the same kernels: the spectral
+# cone's five kernels move 54.3 MB per 128^3 volume (325.8 MB read + write
+# for 6 volumes); a fused MLEM iteration moves 1.092 bytes per attenuation
+# byte (27.53 MB for 25.17 MB).
 CONE_DRAM_BYTES_PER_VOLUME = 325.8e6 / 6
 MLEM_DRAM_PER_ATTEN_BYTE = 27.53e6 / (24 * 16 * 128 * 128 * 4)
 
@@ -350,6 +354,151 @@ def run_ours(args, rank, world, device):
         "clocks": clk.summary(),
     }
     return line
+
+
+# ---------------------------------------------------------------------------
+# checker legs (after the timed regions, rank 0 at N=1): the error of the
+# benchmarked result, and the reference's own CUDA kernels timed beside ours
+# ---------------------------------------------------------------------------
+REF_SO = os.path.join(ROOT, "oracle", "_ref", "ref_atten_cuda.so")
+
+
+def load_reference_extension():
+    """The reference's own CUDA extension (FL/cuda_lib, built from its
+    sources into oracle/_ref), or None when it was not built."""
+    if not os.path.exists(REF_SO):
+        return None
+    from oracle.build_ref import load_built
+    return load_built()
+
+
+def parity_leg(wl, mask, solver, I, device):
+    """Errors of this build's corrected MLEM against independent compositions
+    (tests/compose.py), on inputs identical to the benchmark's:
+
+    * first block of the benchmark (128^3, 3 elements, 120 angles; the
+      attenuation built from the start value, then 5 MLEM iterations), all
+      slices, against the reference's own kernels (cal_atten_cuda,
+      mlem_cuda_batch) driven by the reference's torch steps, FP32 on this GPU;
+    * the same block against the FP64 oracle on the centre slice (the
+      oracle runs the slab of slices the cone couples to it);
+    * the whole 64^3 x 60-angle workload (20 iterations, rebuilt every 5,
+      Poisson noise) against the reference's kernels.
+    Errors: max|a-b|/max|b| and the pointwise max |a-b|/|b| over voxels with
+    |b| >= 1e-2 max|b|."""
+    import torch
+    from tests import compose
+    from fl_correction_b200.recon import CorrectedMLEM
+    from fl_correction_b200.detector_mask import generate_detector_mask
+    log = lambda *a: print("[parity]", *a, file=sys.stderr, flush=True)  # noqa: E731
+    out = {"bar": "1e-4 after 20 MLEM iterations, 1e-5 for maps and projections (max|a-b|/max|b|)"}
+    N, L = wl.N, len(wl.elements)
+    k = wl.recompute_every
+    fixed = torch.ones((1, N, N, N), device=device)
+    t0 = time.perf_counter()
+    C1 = solver.run(I, n_iter=k, recompute_every=k)
+    torch.cuda.synchronize()
+    C1h = C1.cpu().numpy()
+    ref = load_reference_extension()
+    if ref is not None:
+        Cr = compose.reference_corrected_mlem(ref, wl.param, wl.angles, mask, I, fixed, k, k)
+        torch.cuda.synchronize()
+        out["block1_vs_reference_kernels"] = compose.relative_errors(C1h, Cr.cpu().numpy())
+        del Cr
+        log("block 1 vs reference kernels", out["block1_vs_reference_kernels"],
+            "%.1f s" % (time.perf_counter() - t0))
+    else:
+        out["block1_vs_reference_kernels"] = {"unavailable": "oracle/_ref not built"}
+    # FP64 oracle on slice z of the first block: slab [z - hz, z + 1 + hz)
+    t0 = time.perf_counter()
+    hz = mask.shape[0] // 2
+    z = N // 2
+    lo, hi = max(0, z - hz), min(N, z + 1 + hz)
+    Ih = I[:, :, lo:hi].cpu().numpy()
+    Co = compose.oracle_corrected_mlem(wl.param, wl.angles, mask, Ih, np.ones((1, hi - lo, N, N)),
+                                       k, k, z_range=(z - lo, z - lo + 1))
+    out["block1_vs_fp64_oracle"] = dict(compose.relative_errors(C1h[:, z:z + 1],
+                                                                Co[:, z - lo:z - lo + 1]),
+                                        slices=[z, z + 1])
+    log("block 1 vs oracle", out["block1_vs_fp64_oracle"], "%.1f s" % (time.perf_counter() - t0))
+    del C1
+    # the whole small workload against the reference's kernels
+    if ref is not None:
+        t0 = time.perf_counter()
+        w0 = __import__("fl_correction_b200.phantoms", fromlist=["x"]).make_workload(0)
+        N0 = w0.N
+        m0 = generate_detector_mask(w0.mask_angle, w0.mask_angle, N0)
+        s0 = CorrectedMLEM(w0.param, w0.angles, m0, (N0, N0, N0), device=device)
+        truth = torch.from_numpy(w0.conc).to(device)
+        s0.recompute_attenuation(truth)
+        I0 = s0.project(truth)
+        g = torch.Generator(device=device).manual_seed(w0.seed)
+        sc = w0.noise_max_counts / float(I0.max())
+        I0 = (torch.poisson(I0 * sc, generator=g) / sc).contiguous()
+        C0 = s0.run(I0, n_iter=w0.n_iter, recompute_every=w0.recompute_every)
+        Cr0 = compose.reference_corrected_mlem(ref, w0.param, w0.angles, m0, I0,
+                                               torch.ones((1, N0, N0, N0), device=device),
+                                               w0.n_iter, w0.recompute_every)
+        out["cfg0_full_schedule_vs_reference_kernels"] = dict(
+            compose.relative_errors(C0.cpu().numpy(), Cr0.cpu().numpy()), workload=w0.name)
+        log("cfg0 vs reference kernels", out["cfg0_full_schedule_vs_reference_kernels"],
+            "%.1f s" % (time.perf_counter() - t0))
+    return out
+
+
+def reference_gpu_leg(device, N=128, A=120, n_vol=30):
+    """CUDA-event times of the reference's own kernels (FL/cuda_lib compiled
+    from its sources for sm_100a) beside this build's drop-ins, through the
+    same Python API, at the benchmark's shapes: the cone path sum of one
+    30-volume attenuation chunk, the batched forward and backward projector
+    (120 angles x 128 slices of 128^2, one reference) and 5 MLEM iterations."""
+    import torch
+    from fl_correction_b200.cuda_lib import atten_cuda as AC
+    from fl_correction_b200.detector_mask import generate_detector_mask
+    ref = load_reference_extension()
+    if ref is None:
+        return {"unavailable": "oracle/_ref not built"}
+    g = torch.Generator(device=device).manual_seed(11)
+    mask = torch.from_numpy(generate_detector_mask(13.309, 13.309, N).astype(np.float32)).to(device)
+    mu = torch.rand((n_vol, N, N, N), device=device, generator=g) * 0.02
+    atten = torch.rand((A, N, N, N), device=device, generator=g)
+    C = torch.rand((1, N, N, N), device=device, generator=g)
+    em = torch.full((A, 1), 0.02, device=device)
+    th = torch.linspace(0, math.pi, A + 1, device=device)[:-1].contiguous()
+    ratio = torch.rand((A, N, N), device=device, generator=g)
+    I = AC.forward_emission_batch(atten, C, em, th) * 1.05
+
+    def ev_ms(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    cases = {
+        "cal_atten_cuda (%d volumes of %d^3, mask %s)" % (n_vol, N, list(mask.shape)):
+            (lambda: ref.cal_atten_cuda(mu, mask), lambda: AC.cal_atten_cuda(mu, mask), 1),
+        "forward_emission_batch (%d angles x %d slices of %d^2)" % (A, N, N):
+            (lambda: ref.forward_emission_batch(atten, C, em, th),
+             lambda: AC.forward_emission_batch(atten, C, em, th), 3),
+        "backward_emission_batch (%d angles x %d slices of %d^2)" % (A, N, N):
+            (lambda: ref.backward_emission_batch(atten, ratio, em, th),
+             lambda: AC.backward_emission_batch(atten, ratio, em, th), 3),
+        "mlem_cuda_batch (5 iterations, beta 0)":
+            (lambda: ref.mlem_cuda_batch(C, atten, em, th, I, 5, 0.0, 0.01),
+             lambda: AC.mlem_cuda_batch(C, atten, em, th, I, 5, 0.0, 0.01), 1),
+    }
+    out = {}
+    for name, (fr, fo, reps) in cases.items():
+        r_ms, o_ms = ev_ms(fr, reps), ev_ms(fo, reps)
+        out[name] = {"reference_ms": round(r_ms, 3), "ours_ms": round(o_ms, 3),
+                     "speedup": round(r_ms / o_ms, 2)}
+        print("[ref-gpu]", name, out[name], file=sys.stderr, flush=True)
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -759,6 +908,14 @@ def main():
             dist.destroy_process_group()
         return
     line = run_ours(args, rank, world, device)
+    if rank == 0 and world == 1 and not args.no_parity:
+        wl, mask, solver, I = build_problem(args.config, rank, device)
+        line["parity"] = parity_leg(wl, mask, solver, I, device)
+        del solver, I
+    if rank == 0 and world == 1 and not args.no_ref_gpu:
+        import torch
+        torch.cuda.empty_cache()
+        line["reference_gpu_kernels"] = reference_gpu_leg(device)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, desc, cores, _ = cpu_sample(args.config)
         line["cpu_baseline"] = {"value": round(v, 6), "unit": "MLEM iters/s", "cores": cores,

@@ -38,7 +38,13 @@ enum TuneKey {
     kTuneAttenChunk = 3,    // angles per attenuation-pipeline pass
     kTuneProjBwd = 4,       // backward: 0 automatic, 1 shared-atomic splat, 2 nine-phase
                             // splat, 3 gather, 4 column segments
-    kTuneCount = 5
+    // test hooks of the bounded waits (0 = off): the polls a TMA-cone wait
+    // makes before it gives up, and a plane step (1-based) whose TMA load is
+    // not issued, so that its wait runs out and the kernel reports
+    // FLC_ERR_TIMEOUT without faulting
+    kTuneConeWaitLimit = 5,
+    kTuneConeSkipLoad = 6,
+    kTuneCount = 7
 };
 int64_t tune(int key);
 

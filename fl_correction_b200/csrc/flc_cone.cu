@@ -34,7 +34,7 @@ __device__ int g_cone_status = 0;
 
 namespace {
 
-constexpr int kWaitLimit = 1 << 26;  // ~ seconds of polling before giving up
+constexpr int kWaitLimit = 1 << 26;  // default polls before a wait gives up (~ seconds)
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return (uint32_t)__cvta_generic_to_shared(p);
@@ -50,9 +50,9 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
                  : "memory");
 }
 
-// Polls the mbarrier phase `parity` at most kWaitLimit times; false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-    for (int i = 0; i < kWaitLimit; ++i) {
+// Polls the mbarrier phase `parity` at most `limit` times; false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int limit) {
+    for (int i = 0; i < limit; ++i) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -89,6 +89,8 @@ struct ConeGeom {
     int WY, WZ;      // padded weight row lengths
     int zblocks;     // Z / 32 rounded up
     int ring;        // 0: every depth's filters preloaded; 1: a ring of 2 XB rows
+    int wait_limit;  // polls of a bounded wait before it gives up
+    int skip_step;   // test hook: the plane step whose load is not issued (-1: none)
 };
 
 // 4 taps x 8 outputs from a 12-value window (a,b,c) and 4 weights w.
@@ -194,6 +196,7 @@ cone_tma_kernel(const __grid_constant__ CUtensorMap tmap, const float* __restric
     __syncthreads();
     if (tid == 0) {
         for (int q = 0; q < 2 && p_begin + q < p_end; ++q) {
+            if (q == g.skip_step) continue;   // test hook: this wait will run out
             mbar_expect_tx(&bars[q], plane_bytes);
             tma_load_3d(S + q * sbuf, &tmap, y0 - g.HYP, p_begin + q, v * Z, &bars[q]);
         }
@@ -269,7 +272,7 @@ cone_tma_kernel(const __grid_constant__ CUtensorMap tmap, const float* __restric
         const int step = p - p_begin;
         const int buf = step & 1;
         const uint32_t parity = (uint32_t)((step >> 1) & 1);
-        if (tid == 0 && !mbar_wait(&bars[buf], parity)) s_fail = 1 + step;
+        if (tid == 0 && !mbar_wait(&bars[buf], parity, g.wait_limit)) s_fail = 1 + step;
         __syncthreads();
         if (s_fail) break;
         // the filters of the depth that enters at the next plane: loaded now,
@@ -309,7 +312,7 @@ cone_tma_kernel(const __grid_constant__ CUtensorMap tmap, const float* __restric
         }
         __syncthreads();
         // plane buffer `buf` is free: prefetch plane p + 2 into it
-        if (tid == 0 && p + 2 < p_end) {
+        if (tid == 0 && p + 2 < p_end && step + 2 != g.skip_step) {
             fence_proxy_async();
             mbar_expect_tx(&bars[buf], plane_bytes);
             tma_load_3d(S + buf * sbuf, &tmap, y0 - g.HYP, p + 2, v * Z, &bars[buf]);
@@ -334,10 +337,12 @@ cone_tma_kernel(const __grid_constant__ CUtensorMap tmap, const float* __restric
     if (s_fail) {
         if (tid == 0) {
             atomicExch(&g_cone_status, FLC_ERR_TIMEOUT);
-            // the load of the following plane may still be in flight
+            // the load the wait gave up on (if it was issued and is only slow)
+            // and the load of the following plane may still be in flight
             const int step = s_fail - 1;
-            if (p_begin + step + 1 < p_end)
-                mbar_wait(&bars[(step + 1) & 1], (uint32_t)(((step + 1) >> 1) & 1));
+            for (int q = step; q <= step + 1; ++q)
+                if (p_begin + q < p_end && q != g.skip_step)
+                    mbar_wait(&bars[q & 1], (uint32_t)((q >> 1) & 1), g.wait_limit);
         }
         __syncthreads();
         return;
@@ -485,6 +490,9 @@ int cone_tma_launch(const float* mu, const float* U, const float* Vw, float* out
     ConeGeom g;
     size_t smem;
     int threads;
+    const int64_t wl = tune(kTuneConeWaitLimit), sk = tune(kTuneConeSkipLoad);
+    g.wait_limit = (wl > 0 && wl < kWaitLimit) ? (int)wl : kWaitLimit;
+    g.skip_step = (sk > 0 && sk < (1 << 30)) ? (int)sk - 1 : -1;
     int64_t variant = tune(kTuneConeVariant);  // 0 auto, 1 16x8, 2 8x4, 3 plain, 4 spectral
     if (variant == 4) variant = 0;              // the spectral form fell back to this kernel
     if (variant == 3) return FLC_ERR_UNSUPPORTED;

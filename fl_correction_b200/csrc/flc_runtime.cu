@@ -58,7 +58,8 @@ static void query_device(int dev) {
 namespace {
 std::atomic<int64_t> g_tune[kTuneCount];
 const char* const kTuneNames[kTuneCount] = {"proj.cluster", "proj.apc", "cone.variant",
-                                            "atten.chunk", "proj.bwd"};
+                                            "atten.chunk", "proj.bwd", "cone.test_wait_limit",
+                                            "cone.test_skip_load"};
 }  // namespace
 
 int64_t tune(int key) { return (key >= 0 && key < kTuneCount) ? g_tune[key].load() : 0; }

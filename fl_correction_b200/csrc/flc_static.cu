@@ -12,7 +12,15 @@
 //    workspace is larger are refused with FLC_ERR_UNSUPPORTED;
 //  * the first call on a device looks up the array's device address with
 //    cudaGetSymbolAddress (once per device, with that device current) -- make
-//    that first call before any stream capture;
+//    that first call before any stream capture.  Under lazy module loading
+//    (the CUDA default) that lookup is also when the driver loads this module
+//    and commits the 32 MiB on the device (CUDA_MODULE_LOADING=EAGER commits
+//    it when the library loads): a process that hands its device memory to
+//    another framework's pool should make the first call at start-up, before
+//    the pool reserves the memory;
+//  * the looked-up address is kept per device ordinal and belongs to the
+//    device's primary context: only the runtime's primary context is
+//    supported, and cudaDeviceReset must not be called between calls;
 //  * every call uses the same array, so calls that overlap in time (other
 //    streams, other host threads) race on it;
 //  * the eager iteration path runs (no CUDA graph, no stream creation).

@@ -66,6 +66,12 @@ FLC_API uint64_t flc_launch_count(void);
  *   "proj.bwd"      backward: 2 nine-phase splat, 1 shared-memory atomics,
  *                   3 gather per pixel, 4 splat by column segments; automatic:
  *                   4 where one round of its items fills the thread block, else 2
+ * Test hooks of the direct cone's bounded waits (for failure-path tests):
+ *   "cone.test_wait_limit"  polls before a TMA-plane wait gives up (default 2^26)
+ *   "cone.test_skip_load"   k > 0: the load of the k-th staged plane of every
+ *                   CTA is not issued, so its wait runs out; the kernel waits
+ *                   for its other loads, stops, and flc_device_status then
+ *                   reports FLC_ERR_TIMEOUT (no fault, the context stays usable)
  * 0 restores the automatic choice.  flc_tune_get returns -1 for an unknown
  * name.  Process-wide; not synchronized with launches in flight. */
 FLC_API int flc_tune_set(const char* name, int64_t value);
@@ -144,9 +150,13 @@ FLC_API int flc_mlem(float* C, const float* atten, const float* em, const float*
  * buffers, a process whose device memory another framework has reserved).
  * No counterpart in the reference.  Problems whose flc_mlem_workspace_bytes
  * exceeds 32 MiB return FLC_ERR_UNSUPPORTED.  The first call on a device
- * looks up the array's address (make it before any stream capture); calls
- * that overlap in time share the array and race.  Runs the eager iteration
- * path (use_graph = 0). */
+ * looks up the array's address (make it before any stream capture); with
+ * lazy module loading, the CUDA default, that first call is also when the
+ * driver commits the 32 MiB, so make it at start-up, before another pool
+ * reserves the device's memory.  The address is kept per device for the
+ * primary context: do not call cudaDeviceReset between calls.  Calls that
+ * overlap in time share the array and race.  Runs the eager iteration path
+ * (use_graph = 0). */
 FLC_API int flc_mlem_static(float* C, const float* atten, const float* em, const float* theta,
                     const float* I, int64_t n_iter, double beta, double delta,
                     int64_t A, int64_t B, int64_t R, int64_t H, int64_t W, void* stream);

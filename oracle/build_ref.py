@@ -3,8 +3,9 @@ unmodified, into ``oracle/_ref/`` so the GPU tests can use it as a second
 checker and as a golden-vector generator.
 
 Test infrastructure only: nothing in the product imports this.  The sources
-are read from the reference checkout (``FL_REF_ROOT``, default
-``/root/reference``) and only the built ``.so`` lands in ``oracle/_ref``; the
+are read from the reference checkout (``ref_root()``: the ``FL_REF_ROOT``
+environment variable, else the read-only checkout this recipe was written
+against) and only the built ``.so`` lands in ``oracle/_ref``; the
 reference's own ``setup.py`` is not used.  Build flags: ``-O2`` as in the
 reference's ``setup.py:19-21`` plus an explicit sm_100a target.
 """
@@ -14,11 +15,26 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
 NAME = "ref_atten_cuda"
+# where the reference checkout is mounted read-only on the build machine; the
+# GPU machines have no checkout and use the prebuilt .so
+DEFAULT_REF_ROOT = "/root/reference"
+
+
+def ref_root(required=False):
+    """The reference checkout: FL_REF_ROOT if set, else DEFAULT_REF_ROOT.
+    Returns None (or raises, with required=True) when neither holds FL/."""
+    root = os.environ.get("FL_REF_ROOT") or DEFAULT_REF_ROOT
+    if os.path.isdir(os.path.join(root, "FL")):
+        return root
+    if required:
+        raise FileNotFoundError(
+            "reference checkout not found at %r: set FL_REF_ROOT to the FL_correction "
+            "checkout (the directory that holds FL/)" % root)
+    return None
 
 
 def build(verbose=False):
-    ref_root = os.environ.get("FL_REF_ROOT", "/root/reference")
-    src_dir = os.path.join(ref_root, "FL", "cuda_lib")
+    src_dir = os.path.join(ref_root(required=True), "FL", "cuda_lib")
     srcs = [os.path.join(src_dir, "atten_cuda.cpp"), os.path.join(src_dir, "atten_cuda_kernel.cu")]
     if not all(os.path.exists(s) for s in srcs):
         raise FileNotFoundError("reference sources not found under %s" % src_dir)

@@ -27,7 +27,10 @@ import warnings
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("FL_REF_ROOT", "/root/reference")
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+from oracle.build_ref import ref_root  # noqa: E402
+
+REF = ref_root(required=True)
 STUBBED = ("xraylib", "skimage", "matplotlib", "h5py", "pystackreg", "bm3d",
            "tomopy", "pyxas", "porespy")
 CUDA_NAMES = ("cal_atten_cuda", "forward_emission", "backward_emission",

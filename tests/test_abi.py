@@ -100,7 +100,8 @@ def test_cpu_tensors_fail_loudly():
 
 def test_tuning_knobs_round_trip():
     lib = _lib.load()
-    for name in (b"proj.cluster", b"proj.apc", b"cone.variant", b"atten.chunk", b"proj.bwd"):
+    for name in (b"proj.cluster", b"proj.apc", b"cone.variant", b"atten.chunk", b"proj.bwd",
+                 b"cone.test_wait_limit", b"cone.test_skip_load"):
         old = lib.flc_tune_get(name)
         assert old >= 0
         assert lib.flc_tune_set(name, 3) == 0

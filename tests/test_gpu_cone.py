@@ -200,3 +200,37 @@ def test_spectral_cone_benchmark_size():
         tune.set_knob("cone.variant", old)
     assert _lib.query("flc_device_status", 1) == 0
     assert rel_err(outs[0], outs[1]) < 2e-6
+
+
+def test_bounded_wait_runs_out_and_reports_timeout():
+    """The direct cone's bounded TMA waits: with the test hooks the first
+    staged plane's load is never issued and the wait gives up after a few
+    thousand polls.  The kernel waits for its other loads, stops, and leaves
+    FLC_ERR_TIMEOUT for flc_device_status; the context stays usable."""
+    lib = _lib.load()
+    rng = np.random.default_rng(5)
+    K, Z, X, Y = 1, 16, 16, 16
+    mask = generate_detector_mask(13.309, 13.309, X)
+    u, v = factor_mask(mask)
+    mu = (rng.random((K, Z, X, Y)) * 0.02).astype(np.float32)
+    x, U, V = T(mu), T(u), T(v)
+    out = torch.empty_like(x)
+
+    def run():
+        _lib.call("flc_cone_atten_separable", _lib.ptr(x), _lib.ptr(U), _lib.ptr(V),
+                  _lib.ptr(out), K, Z, X, Y, *mask.shape, 0, _lib.stream())
+        torch.cuda.synchronize()
+
+    assert lib.flc_device_status(1) == 0
+    try:
+        assert lib.flc_tune_set(b"cone.test_wait_limit", 4000) == 0
+        assert lib.flc_tune_set(b"cone.test_skip_load", 1) == 0
+        run()
+    finally:
+        lib.flc_tune_set(b"cone.test_skip_load", 0)
+        lib.flc_tune_set(b"cone.test_wait_limit", 0)
+    assert lib.flc_device_status(1) == 6            # FLC_ERR_TIMEOUT, then cleared
+    assert lib.flc_device_status(0) == 0
+    run()                                           # the same call works again
+    assert lib.flc_device_status(1) == 0
+    assert rel_err(out.cpu().numpy(), O.cone_ref(mu, mask.astype(np.float32))) < TOL_MAP

@@ -42,6 +42,7 @@ SIGNATURES = {
     "flc_atten_workspace_bytes": (_sz, [_i64, _i64, _i64, _i64, _i64, _i64, _i64]),
     "flc_atten_maps": (_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64,
                               _i64, _i64, _i64, _i64, _int, _int, _i64, _vp, _sz, _vp]),
+    "flc_atten_maps_ref": (_int, [_vp] * 8 + [_i64] * 11 + [_int, _int, _i64, _vp, _sz, _vp]),
     "flc_atten_stage": (_int, [_vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _i64,
                                _i64, _i64, _int, _int, _vp]),
     "flc_cone_atten_apply": (_int, [_vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _i64, _i64,

@@ -6,6 +6,7 @@ them from xraylib, FL/atten_util.py:14-39, which this package does not use).
 from copy import deepcopy
 
 import numpy as np
+import torch
 
 __all__ = ["extract_single_value_param", "extract_em_cs_elem", "update_dict_use_ref_at_angle",
            "get_atten_coef"]
@@ -41,11 +42,24 @@ def extract_em_cs_elem(param, elem, use_ref=False):
 
 
 def update_dict_use_ref_at_angle(dict_use_ref, current_angle):
-    """Copy of dict_use_ref; rotating reference volumes is not implemented
-    (FL/atten_util.py:79-88)."""
+    """Copy of dict_use_ref with every reference volume of 'ref_3D' rotated by
+    current_angle degrees (FL/atten_util.py:79-88).  The reference rotates with
+    scipy's ndimage.rotate (order 1, FL/image_util.py:165-203); here the
+    native grid_sample rotation runs (the fractions' rotation, which equals
+    it to ~1e-6 inside the volume).  numpy in, float32 numpy out, as rot3D
+    returns; a cuda tensor stays on its device."""
     d = deepcopy(dict_use_ref)
     if len(d) > 0 and d.get("use_ref", False):
-        raise NotImplementedError("reference-spectrum volumes are not implemented")
+        from .torch_image_util import torch_rotate_image_nd
+        th = float(current_angle) / 180.0 * np.pi
+        refs = d["ref_3D"]
+        for i in range(len(refs)):
+            r = refs[i]
+            if isinstance(r, torch.Tensor):
+                refs[i] = torch_rotate_image_nd(r.to(torch.float32), th)
+            else:
+                t = torch.tensor(np.nan_to_num(np.asarray(r, np.float32)), device="cuda")
+                refs[i] = torch_rotate_image_nd(t, th).cpu().numpy()
     return d
 
 

@@ -18,7 +18,7 @@ from .atten_util import extract_single_value_param
 from .cuda_lib.atten_cuda import forward_emission_batch
 from .detector_mask import factor_mask
 
-__all__ = ["atten_coefficients", "mask_factors", "atten_maps", "pick_chunk", "cal_xrf_atten_at_angles",
+__all__ = ["atten_coefficients", "ref_coefficients", "mask_factors", "atten_maps", "pick_chunk", "cal_xrf_atten_at_angles",
            "cal_xray_atten_at_angles", "cal_total_atten_at_angles", "cal_atten_at_angles",
            "re_projection_cuda"]
 
@@ -54,7 +54,7 @@ def mask_factors(detector_mask, device):
 
 
 def atten_maps(frac_4D, angle_list, coef_x, coef_f, mask_uv=None, incident="own", xrf=True,
-               out=None, chunk=0, workspace=None, cone_events=None, theta=None):
+               out=None, chunk=0, workspace=None, cone_events=None, theta=None, ref=None):
     """Attenuation (L, A, S, H, W) for fractions frac_4D (n_ch, S, H, W) on the
     device: incident term (mode 'own' | 'all' | 'none') times exp(-cone).
 
@@ -64,11 +64,20 @@ def atten_maps(frac_4D, angle_list, coef_x, coef_f, mask_uv=None, incident="own"
     per angle chunk and (start, end, volumes) CUDA events of every cone launch
     are appended to it.  theta: optional device tensor of the angles in
     radians (float32), used instead of converting angle_list (no host copy,
-    so the call can be captured in a CUDA graph)."""
+    so the call can be captured in a CUDA graph).
+    ref: optional (ref_3D, coef_ref, ref_ch) for a reference-spectrum incident
+    cross section of compound ref_ch (the XANES case of
+    FL/torch_functions.py:22-37): ref_3D (n_ref, S, H, W) raw reference
+    volumes in the unrotated frame (rotated with the fractions), coef_ref
+    (A, n_ref) the per-angle spectrum values cs[comp-x_ref{i+1}] * rho * pix
+    (see ref_coefficients)."""
     _lib.require_cuda("atten_maps", frac_4D)
     dev = frac_4D.device
     frac = frac_4D.contiguous()
     n_ch, S, H, W = frac.shape
+    if ref is not None:
+        return _atten_maps_ref(frac, angle_list, coef_x, coef_f, mask_uv, incident, xrf, out,
+                               chunk, workspace, cone_events, theta, ref)
     if theta is None:
         theta = torch.as_tensor(np.asarray(angle_list, dtype=np.float64) / 180.0 * np.pi,
                                 dtype=torch.float32, device=dev)
@@ -116,6 +125,61 @@ def atten_maps(frac_4D, angle_list, coef_x, coef_f, mask_uv=None, incident="own"
     return out
 
 
+def _atten_maps_ref(frac, angle_list, coef_x, coef_f, mask_uv, incident, xrf, out, chunk,
+                    workspace, cone_events, theta, ref):
+    """atten_maps with reference volumes appended to the fractions
+    (flc_atten_maps_ref)."""
+    if cone_events is not None:
+        raise ValueError("atten_maps: cone_events are not collected with reference volumes")
+    ref_3D, coef_ref, ref_ch = ref
+    dev = frac.device
+    n_ch, S, H, W = frac.shape
+    rv = torch.as_tensor(ref_3D, dtype=torch.float32, device=dev)
+    if rv.dim() != 4 or tuple(rv.shape[1:]) != (S, H, W):
+        raise ValueError("atten_maps: reference volumes must be (n_ref, S, H, W)")
+    n_ref = rv.shape[0]
+    allf = torch.cat([frac, rv]).contiguous()
+    if theta is None:
+        theta = torch.as_tensor(np.asarray(angle_list, dtype=np.float64) / 180.0 * np.pi,
+                                dtype=torch.float32, device=dev)
+    A = theta.numel()
+    cx = torch.as_tensor(coef_x, dtype=torch.float32, device=dev).contiguous()
+    cf = torch.as_tensor(coef_f, dtype=torch.float32, device=dev).contiguous()
+    cr = torch.as_tensor(coef_ref, dtype=torch.float32, device=dev).reshape(A, n_ref).contiguous()
+    L = cf.shape[1]
+    if out is None:
+        out = torch.empty((L, A, S, H, W), dtype=torch.float32, device=dev)
+    if xrf:
+        u, v, (Mz, Mx, My) = mask_uv
+    else:
+        u = v = None
+        Mz = Mx = My = 1
+    chunk = pick_chunk(S, H, W, A, L, chunk)
+    ws_bytes, _, _ = atten_workspace_bytes(n_ch + n_ref, S, H, W, A, L, chunk,
+                                           (Mz, Mx, My) if xrf else None)
+    ws = workspace if workspace is not None and workspace.numel() >= ws_bytes else _lib.workspace(ws_bytes, dev)
+    with torch.cuda.device(dev):
+        _lib.call("flc_atten_maps_ref", _lib.ptr(allf), _lib.ptr(theta), _lib.ptr(cx),
+                  _lib.ptr(cf), _lib.ptr(cr), _lib.ptr(u), _lib.ptr(v), _lib.ptr(out), n_ch, n_ref,
+                  int(ref_ch), S, H, W, A, L, Mz, Mx, My, INCIDENT_MODES[incident],
+                  0 if xrf else 1, chunk, _lib.ptr(ws), ws_bytes, _lib.stream())
+    return out
+
+
+def ref_coefficients(param, n_angle, ref_comp):
+    """(A, n_ref) float32 spectrum values cs['<ref_comp>-x_ref<i+1>'] * rho *
+    pix per angle (selected per angle like extract_single_value_param), and
+    the channel of ref_comp."""
+    cs = param["cs"]
+    n_ref = int(cs["n_ref"])
+    rho, pix = param["rho"][ref_comp], param["pix"]
+    out = np.zeros((n_angle, n_ref), np.float32)
+    for i in range(n_ref):
+        v = np.asarray(cs[f"{ref_comp}-x_ref{i + 1}"], np.float64).reshape(-1)
+        out[:, i] = (v if v.size > 1 else np.repeat(v, n_angle))[:n_angle] * rho * pix
+    return out, list(param["elem_compound"]).index(ref_comp)
+
+
 def atten_workspace_bytes(n_ch, S, H, W, A, L, chunk=0, mask_shape=None):
     """(total, pipeline, spectral-cone) workspace bytes of atten_maps for
     `chunk` angles per pass (0: the default chunk); the pipeline part holds
@@ -155,8 +219,8 @@ def cal_xrf_atten_at_angles(frac_4D, param, angle_list, detector_mask, detector_
     returns (L, A, S, H, W) on frac_4D's device."""
     if abs(detector_offset_angle) > 1e-2 * 180 / np.pi or position_det != "r":
         raise NotImplementedError("only detector_offset_angle=0, position_det='r' is implemented")
-    if len(dict_use_ref) > 0 and dict_use_ref.get("use_ref", False):
-        raise NotImplementedError("reference-spectrum volumes are not implemented")
+    # dict_use_ref does not enter the fluorescence mu (FL/torch_functions.py:55-81;
+    # FL/core.py:36-47 only selects per-angle parameters with it)
     cx, cf = atten_coefficients(param, len(angle_list), frac_4D.shape[0])
     maps = atten_maps(frac_4D, angle_list, cx, cf, mask_factors(detector_mask, frac_4D.device),
                       incident="none", xrf=True)
@@ -164,13 +228,24 @@ def cal_xrf_atten_at_angles(frac_4D, param, angle_list, detector_mask, detector_
     return maps
 
 
-def cal_xray_atten_at_angles(frac_4D, param, angle_list, dict_use_ref={}, fsave=None):
+def cal_xray_atten_at_angles(frac_4D, param, angle_list, dict_use_ref={}, fsave=None,
+                             apply_ref=False):
     """Incident-beam attenuation at every angle (FL/core.py:55-81): element i
-    uses channel i, as the reference writes atten_xray[i] for element i."""
-    if len(dict_use_ref) > 0 and dict_use_ref.get("use_ref", False):
-        raise NotImplementedError("reference-spectrum volumes are not implemented")
+    uses channel i, as the reference writes atten_xray[i] for element i.
+
+    The reference selects per-angle parameters with dict_use_ref but then
+    calls torch_xray_atten_3D with an empty dict (FL/core.py:76-79), so its
+    result does not depend on the reference volumes; that is the default here
+    too.  apply_ref=True applies them as torch_xray_atten_3D does when it is
+    given them (FL/torch_functions.py:22-37): the incident cross section of
+    dict_use_ref['ref_comp'] becomes the per-voxel mix of the reference
+    spectra, the reference volumes rotated with the fractions."""
     cx, cf = atten_coefficients(param, len(angle_list), frac_4D.shape[0])
-    maps = atten_maps(frac_4D, angle_list, cx, cf, None, incident="own", xrf=False)
+    ref = None
+    if apply_ref and len(dict_use_ref) > 0 and dict_use_ref.get("use_ref", False):
+        cr, ch = ref_coefficients(param, len(angle_list), dict_use_ref["ref_comp"])
+        ref = (dict_use_ref["ref_3D"], cr, ch)
+    maps = atten_maps(frac_4D, angle_list, cx, cf, None, incident="own", xrf=False, ref=ref)
     _save(fsave, "xray", param, maps)
     return maps
 

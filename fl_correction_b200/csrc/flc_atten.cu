@@ -78,6 +78,20 @@ constexpr int kRun = 8;
 struct StageCoef {
     float cx[kMaxCh];
     float cf[kMaxL][kMaxCh];
+    float cref[kMaxCh];
+};
+
+// Reference-spectrum incident cross section (FL/torch_functions.py:22-37 with
+// FL/cross_section_util.py:44-66): channels [n_ch, n_ch + n) of the rotated
+// fractions are raw reference volumes; the incident coefficient of channel
+// ch becomes, per voxel, sum_i coef[a][i] * max(ref_i / (sum_k ref_k +
+// 1e-12), 0) -- the reference fractions of cal_frac (FL/core.py:159-205)
+// with enable_scale off and no threshold mask -- times the spectrum value
+// cs[comp-x_ref{i+1}] * rho * pix in coef (A, n).  ch < 0: not used.
+struct RefSpec {
+    const float* coef;
+    int ch;
+    int n;
 };
 
 // Channel-interleaved copy of the fractions: frac4[s][h][w][q] holds channels
@@ -137,20 +151,23 @@ __global__ void atten_stage_kernel(const float* __restrict__ frac, const float4*
                                    const float* __restrict__ coef_f, float* __restrict__ out,
                                    float* __restrict__ mu_ref, int n_ch, int S, int H, int W,
                                    int L, int64_t out_a_stride, int64_t out_l_stride, int a_base,
-                                   int incident_mode, int write_mu, int out_a0) {
+                                   int incident_mode, int write_mu, int out_a0, RefSpec ref) {
     __shared__ StageCoef cf;
     const int s = blockIdx.x;
     const int al = blockIdx.y;
     const int a = a_base + al;
     const int w = threadIdx.x;
-    for (int t = threadIdx.x; t < kMaxCh * (kMaxL + 1); t += blockDim.x) {
+    for (int t = threadIdx.x; t < kMaxCh * (kMaxL + 2); t += blockDim.x) {
         int j = t % kMaxCh, i = t / kMaxCh;
-        if (i == kMaxL)
+        if (i == kMaxL + 1)
+            cf.cref[j] = j < ref.n ? ref.coef[(int64_t)a * ref.n + j] : 0.f;
+        else if (i == kMaxL)
             cf.cx[j] = j < n_ch ? coef_x[(int64_t)a * n_ch + j] : 0.f;
         else
             cf.cf[i][j] = (i < L && j < n_ch) ? coef_f[((int64_t)a * L + i) * n_ch + j] : 0.f;
     }
     __syncthreads();
+    const int n_tot = n_ch + ref.n;       // channels sampled (compounds, then references)
     if (w >= W) return;
     // the reference rounds math.cos / math.sin of the angle to an FP32 matrix
     const double th = (double)theta[a];
@@ -177,8 +194,19 @@ __global__ void atten_stage_kernel(const float* __restrict__ frac, const float4*
             } else {
 #pragma unroll
                 for (int j = 0; j < kMaxCh; ++j)
-                    fr[j] = j < n_ch ? rot_sample(frac + ((int64_t)j * S + s) * HW, H, W, g, h, w)
-                                     : 0.f;
+                    fr[j] = j < n_tot ? rot_sample(frac + ((int64_t)j * S + s) * HW, H, W, g, h, w)
+                                      : 0.f;
+            }
+            // the reference-spectrum coefficient of channel ref.ch at this voxel
+            float cxr = 0.f;
+            if (ref.ch >= 0) {
+                float tot = 1e-12f;
+#pragma unroll
+                for (int j = 0; j < kMaxCh; ++j)
+                    if (j >= n_ch && j < n_tot) tot += fr[j];
+#pragma unroll
+                for (int j = 0; j < kMaxCh; ++j)
+                    if (j >= n_ch && j < n_tot) cxr += cf.cref[j - n_ch] * fmaxf(fr[j] / tot, 0.f);
             }
             // incident term: write the exclusive product, then fold in this voxel
             if (incident_mode != 2) {
@@ -188,12 +216,12 @@ __global__ void atten_stage_kernel(const float* __restrict__ frac, const float4*
                 if (incident_mode == 0) {
 #pragma unroll
                     for (int i = 0; i < LM; ++i)
-                        if (i < L) prod[i] *= 1.f - fr[i] * cf.cx[i];
+                        if (i < L) prod[i] *= 1.f - fr[i] * (i == ref.ch ? cxr : cf.cx[i]);
                 } else {
                     float f = 1.f;
 #pragma unroll
                     for (int j = 0; j < kMaxCh; ++j)
-                        if (j < n_ch) f *= 1.f - fr[j] * cf.cx[j];
+                        if (j < n_ch) f *= 1.f - fr[j] * (j == ref.ch ? cxr : cf.cx[j]);
 #pragma unroll
                     for (int i = 0; i < LM; ++i) prod[i] *= f;
                 }
@@ -609,17 +637,17 @@ int frac_interleave_launch(const float* frac, float4* frac4, int64_t n_ch, int64
 
 // frac4: the channel-interleaved copy (frac_interleave_launch) or nullptr
 // for the planar frac.
-int atten_stage_launch(const float* frac, const float* theta, const float* coef_x,
-                       const float* coef_f, float* out, float* mu_ref, int n_ch, int S, int H,
-                       int W, int L, int64_t out_a_stride, int64_t out_l_stride, int a_base,
-                       int n_a, int incident_mode, int write_mu, cudaStream_t st, int out_a0,
-                       const float4* frac4) {
+int atten_stage_launch_ref(const float* frac, const float* theta, const float* coef_x,
+                           const float* coef_f, float* out, float* mu_ref, int n_ch, int S, int H,
+                           int W, int L, int64_t out_a_stride, int64_t out_l_stride, int a_base,
+                           int n_a, int incident_mode, int write_mu, cudaStream_t st, int out_a0,
+                           const float4* frac4, RefSpec ref) {
     const int threads = (W + 31) & ~31;
     using K = void (*)(const float*, const float4*, const float*, const float*, const float*,
                        float*, float*, int, int, int, int, int, int64_t, int64_t, int, int, int,
-                       int);
+                       int, RefSpec);
     K kern;
-    const int G = frac4 ? frac_groups(n_ch) : 0;
+    const int G = frac4 ? frac_groups(n_ch + ref.n) : 0;
     if (G == 1)
         kern = L <= 1 ? atten_stage_kernel<1, 1> : L <= 2 ? atten_stage_kernel<2, 1>
              : L <= 4 ? atten_stage_kernel<4, 1> : atten_stage_kernel<8, 1>;
@@ -631,30 +659,43 @@ int atten_stage_launch(const float* frac, const float* theta, const float* coef_
              : L <= 4 ? atten_stage_kernel<4, 0> : atten_stage_kernel<8, 0>;
     kern<<<dim3((unsigned)S, (unsigned)n_a), threads, 0, st>>>(
         frac, frac4, theta, coef_x, coef_f, out, mu_ref, n_ch, S, H, W, L, out_a_stride,
-        out_l_stride, a_base, incident_mode, write_mu, out_a0 < 0 ? a_base : out_a0);
+        out_l_stride, a_base, incident_mode, write_mu, out_a0 < 0 ? a_base : out_a0, ref);
     return check_launch("atten_stage_kernel");
+}
+
+int atten_stage_launch(const float* frac, const float* theta, const float* coef_x,
+                       const float* coef_f, float* out, float* mu_ref, int n_ch, int S, int H,
+                       int W, int L, int64_t out_a_stride, int64_t out_l_stride, int a_base,
+                       int n_a, int incident_mode, int write_mu, cudaStream_t st, int out_a0,
+                       const float4* frac4) {
+    return atten_stage_launch_ref(frac, theta, coef_x, coef_f, out, mu_ref, n_ch, S, H, W, L,
+                                  out_a_stride, out_l_stride, a_base, n_a, incident_mode,
+                                  write_mu, st, out_a0, frac4, RefSpec{nullptr, -1, 0});
 }
 
 int atten_maps_launch(const float* frac, const float* theta, const float* coef_x,
                       const float* coef_f, const float* u, const float* v, float* out,
                       int64_t n_ch, int64_t S, int64_t H, int64_t W, int64_t A, int64_t L,
                       int64_t Mz, int64_t Mx, int64_t My, int incident_mode, int xrf_mode,
-                      int64_t chunk, void* workspace, size_t ws_bytes, cudaStream_t st) {
+                      int64_t chunk, void* workspace, size_t ws_bytes, cudaStream_t st,
+                      RefSpec ref = RefSpec{nullptr, -1, 0}) {
     chunk = pick_chunk(S, H, W, A, L, chunk);
     float* mu_ref = (float*)workspace;
-    // the interleaved fractions follow the staged mu; the spectral cone's
-    // scratch is whatever the workspace holds past both
-    const size_t pipe_bytes = atten_ws_bytes(n_ch, S, H, W, A, L, chunk);
-    float4* frac4 = (float4*)((char*)workspace + (pipe_bytes - frac4_bytes(n_ch, S, H, W)));
+    // the interleaved fractions (compounds, then reference volumes) follow the
+    // staged mu; the spectral cone's scratch is whatever the workspace holds
+    // past both
+    const int64_t n_tot = n_ch + ref.n;
+    const size_t pipe_bytes = atten_ws_bytes(n_tot, S, H, W, A, L, chunk);
+    float4* frac4 = (float4*)((char*)workspace + (pipe_bytes - frac4_bytes(n_tot, S, H, W)));
     void* fft_ws = ws_bytes > pipe_bytes ? (char*)workspace + pipe_bytes : nullptr;
     const size_t fft_bytes = ws_bytes > pipe_bytes ? ws_bytes - pipe_bytes : 0;
-    FLC_TRY(frac_interleave_launch(frac, frac4, n_ch, S, H, W, st));
+    FLC_TRY(frac_interleave_launch(frac, frac4, n_tot, S, H, W, st));
     const int64_t out_a = S * H * W, out_l = A * S * H * W;
     for (int64_t a0 = 0; a0 < A; a0 += chunk) {
         int n_a = (int)(A - a0 < chunk ? A - a0 : chunk);
-        FLC_TRY(atten_stage_launch(frac, theta, coef_x, coef_f, out, mu_ref, (int)n_ch, (int)S,
-                                   (int)H, (int)W, (int)L, out_a, out_l, (int)a0, n_a,
-                                   incident_mode, xrf_mode == 0, st, -1, frac4));
+        FLC_TRY(atten_stage_launch_ref(frac, theta, coef_x, coef_f, out, mu_ref, (int)n_ch,
+                                       (int)S, (int)H, (int)W, (int)L, out_a, out_l, (int)a0, n_a,
+                                       incident_mode, xrf_mode == 0, st, -1, frac4, ref));
         if (xrf_mode != 0) continue;
         // reference frame of the cone: (Z=S, X=W, Y=H)
         FLC_TRY(cone_launch_ws(mu_ref, u, v, out, (int64_t)n_a * L, S, W, H, Mz, Mx, My, 2,
@@ -809,6 +850,46 @@ extern "C" int flc_atten_maps(const float* frac, const float* theta, const float
     return atten_maps_launch(frac, theta, coef_x, coef_f, u, v, out, n_ch, S, H, W, A, L, Mz, Mx,
                              My, incident_mode, xrf_mode, chunk, workspace, workspace_bytes,
                              as_stream(stream));
+}
+
+extern "C" int flc_atten_maps_ref(const float* frac, const float* theta, const float* coef_x,
+                                  const float* coef_f, const float* coef_ref, const float* u,
+                                  const float* v, float* out, int64_t n_ch, int64_t n_ref,
+                                  int64_t ref_ch, int64_t S, int64_t H, int64_t W, int64_t A,
+                                  int64_t L, int64_t Mz, int64_t Mx, int64_t My,
+                                  int incident_mode, int xrf_mode, int64_t chunk, void* workspace,
+                                  size_t workspace_bytes, void* stream) {
+    clear_error();
+    FLC_REQUIRE(frac && theta && coef_x && coef_f && out && workspace,
+                "flc_atten_maps_ref: null pointer argument");
+    FLC_REQUIRE(xrf_mode != 0 || (u && v), "flc_atten_maps_ref: mask factors required");
+    FLC_REQUIRE(n_ref >= 0 && n_ch >= 1 && n_ch + n_ref <= kMaxCh,
+                "flc_atten_maps_ref: 1 <= n_ch and n_ch + n_ref <= %d", kMaxCh);
+    FLC_REQUIRE(n_ref == 0 || (coef_ref && ref_ch >= 0 && ref_ch < n_ch),
+                "flc_atten_maps_ref: with references, coef_ref is required and 0 <= ref_ch < n_ch");
+    FLC_REQUIRE(L >= 1 && L <= kMaxL, "flc_atten_maps_ref: 1 <= L <= %d", kMaxL);
+    FLC_REQUIRE(S >= 1 && S <= 65535 && A >= 1 && A <= 65535,
+                "flc_atten_maps_ref: S, A in [1, 65535]");
+    FLC_REQUIRE(H == W && H >= 2 && W <= 1024,
+                "flc_atten_maps_ref: needs square slices H == W in [2, 1024]");
+    FLC_REQUIRE(incident_mode >= 0 && incident_mode <= 2 && (xrf_mode == 0 || xrf_mode == 1),
+                "flc_atten_maps_ref: bad mode");
+    FLC_REQUIRE(xrf_mode != 0 || (Mz >= 1 && Mx >= 1 && My >= 1),
+                "flc_atten_maps_ref: bad mask size");
+    if (((uintptr_t)workspace & 255) != 0) {
+        set_error("flc_atten_maps_ref: workspace must be 256-byte aligned");
+        return FLC_ERR_ALIGNMENT;
+    }
+    size_t need = atten_ws_bytes(n_ch + n_ref, S, H, W, A, L, chunk);
+    if (workspace_bytes < need) {
+        set_error("flc_atten_maps_ref: workspace of %zu bytes is smaller than the %zu required",
+                  workspace_bytes, need);
+        return FLC_ERR_WORKSPACE;
+    }
+    RefSpec ref{n_ref > 0 ? coef_ref : nullptr, n_ref > 0 ? (int)ref_ch : -1, (int)n_ref};
+    return atten_maps_launch(frac, theta, coef_x, coef_f, u, v, out, n_ch, S, H, W, A, L, Mz, Mx,
+                             My, incident_mode, xrf_mode, chunk, workspace, workspace_bytes,
+                             as_stream(stream), ref);
 }
 
 extern "C" int flc_atten_stage(const float* frac, const float* theta, const float* coef_x,

@@ -44,7 +44,9 @@ enum TuneKey {
     // FLC_ERR_TIMEOUT without faulting
     kTuneConeWaitLimit = 5,
     kTuneConeSkipLoad = 6,
-    kTuneCount = 7
+    kTuneProjLegacy = 7,    // 1: the earlier projector / fused-MLEM kernels instead of
+                            // the two lean kernels (for comparison)
+    kTuneCount = 8
 };
 int64_t tune(int key);
 
@@ -52,6 +54,8 @@ int64_t tune(int key);
 int sm_count();
 // Opt-in shared memory per block of the current device (cached per device).
 int max_smem_optin();
+// Shared memory per SM of the current device (cached per device).
+int smem_per_sm();
 
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 

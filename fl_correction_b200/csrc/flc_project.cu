@@ -766,6 +766,266 @@ mlem_iter_kernel(const float* __restrict__ atten, const float* __restrict__ em,
     cluster.sync();
 }
 
+// ===========================================================================
+// The lean projector kernels (default): forward (+ MLEM ratio) and backward
+// (+ sensitivity clamp or MLEM update), each sized so that three CTAs share
+// an SM -- one slice image in shared memory per CTA, no attenuation tile --
+// so that one CTA's barriers and shared-memory latencies are covered by the
+// other two.  An MLEM iteration is the two launches; the attenuation is read
+// by each (the bytes the reference's forward and backward calls read).
+// ===========================================================================
+constexpr int kT2 = 256;      // threads per CTA of the lean kernels
+constexpr int kFwdU = 8;      // attenuation loads issued together in the forward
+constexpr int kSegU = 8;      // ... and in a backward segment walk
+
+// Forward: grid (angle groups, B).  The CTA stages slice b of C (R images,
+// row pitch == 3 mod 32) and walks its angles.  Work item = (column w, part
+// p): the thread sums atten(h, w) * sum_r em_r bilerp(C_r) over the part's
+// rows; a warp's loads of atten run along w (coalesced) and kFwdU of them are
+// in flight before their samples are computed.  The parts of a column are
+// added in a fixed order (deterministic); the partial sums are double
+// buffered, so an angle costs one barrier.  I != nullptr: out = I / max(Pf,
+// 1e-6) (the MLEM ratio, atten_cuda.cpp:326-329), else out = Pf.
+template <int RC>
+__global__ void __launch_bounds__(kT2, 3)
+proj_fwd2_kernel(const float* __restrict__ atten, const float* __restrict__ C,
+                 const float* __restrict__ em, const float* __restrict__ theta,
+                 float* __restrict__ out, const float* __restrict__ I, int A, int B, int Rrt,
+                 int H, int W, int apc, int parts) {
+    extern __shared__ __align__(16) float smem[];
+    const int R = RC > 0 ? RC : Rrt;
+    const int b = blockIdx.y;
+    const int a0 = blockIdx.x * apc, a1 = min(A, a0 + apc);
+    const int pitch = slice_pitch(W);
+    const int img = H * pitch;
+    float* sC = smem;                      // [R][H][pitch]
+    float* spart = sC + R * img;           // [2][parts][W]
+    stage_slice(sC, C, R, B, b, H, W, pitch);
+    __syncthreads();
+    const int hper = (H + parts - 1) / parts;
+    const int nitems = parts * W;
+    for (int a = a0; a < a1; ++a) {
+        const Geo g = make_geo(theta[a], H, W);
+        const float* at = atten + ((int64_t)a * B + b) * H * W;
+        float* sp = spart + (a & 1) * parts * W;
+        const float em0 = __ldg(em + (int64_t)a * R);
+        for (int item = threadIdx.x; item < nitems; item += blockDim.x) {
+            const int part = item / W, w = item - part * W;
+            const int h0 = part * hper, n = min(H, h0 + hper) - h0;
+            if (n <= 0) {                      // a part past the last row
+                sp[part * W + w] = 0.f;
+                continue;
+            }
+            const float bx = col_bx(g, w), by = col_by(g, w);
+            const float* ap = at + (int64_t)h0 * W + w;
+            float acc = 0.f;
+            float hf = (float)h0 - g.cy;
+            // batch j of kFwdU rows is loaded while batch j - 1 is computed;
+            // rows past the part repeat its last row with weight 0
+            float cur[kFwdU], nxt[kFwdU];
+#pragma unroll
+            for (int k = 0; k < kFwdU; ++k) {
+                cur[k] = __ldg(ap + (int64_t)min(k, n - 1) * W);
+                if (k >= n) cur[k] = 0.f;
+            }
+            for (int j = 0; j < n; j += kFwdU) {
+#pragma unroll
+                for (int k = 0; k < kFwdU; ++k) {
+                    const int r = j + kFwdU + k;
+                    nxt[k] = __ldg(ap + (int64_t)min(r, n - 1) * W);
+                    if (r >= n) nxt[k] = 0.f;
+                }
+#pragma unroll
+                for (int k = 0; k < kFwdU; ++k) {
+                    const Smp s = sample_xy(g, fmaf(g.c, hf, bx), fmaf(g.s, hf, by));
+                    hf += 1.f;
+                    float v;
+                    if (RC == 1) {
+                        v = bilerp(sC, pitch, s);
+                    } else {
+                        v = 0.f;
+                        for (int r = 0; r < R; ++r)
+                            v = fmaf(__ldg(em + (int64_t)a * R + r), bilerp(sC + r * img, pitch, s), v);
+                    }
+                    acc = fmaf(cur[k], v, acc);
+                }
+#pragma unroll
+                for (int k = 0; k < kFwdU; ++k) cur[k] = nxt[k];
+            }
+            sp[part * W + w] = acc;
+        }
+        __syncthreads();
+        for (int w = threadIdx.x; w < W; w += blockDim.x) {
+            float s = 0.f;
+            for (int p = 0; p < parts; ++p) s += sp[p * W + w];
+            if (RC == 1) s *= em0;
+            const int64_t o = ((int64_t)a * B + b) * W + w;
+            if (I) s = I[o] / fmaxf(s, 1e-6f);
+            out[o] = s;
+        }
+        // the next angle writes the other partial buffer; the one after it
+        // writes this buffer again only past the next barrier
+    }
+}
+
+// The per-angle weights q[r][w] = ratio(a, b, w) * em(a, r) of the backward
+// (ratio == nullptr: ratio = 1, the sensitivity P^T 1).
+__device__ __forceinline__ void stage_q(float* sq, const float* __restrict__ ratio,
+                                        const float* __restrict__ em, int a, int b, int B, int R,
+                                        int W) {
+    for (int i = threadIdx.x; i < R * W; i += blockDim.x) {
+        const int r = i / W, w = i - r * W;
+        const float rq = ratio ? __ldg(ratio + ((int64_t)a * B + b) * W + w) : 1.f;
+        sq[i] = rq * __ldg(em + (int64_t)a * R + r);
+    }
+}
+
+// Splats samples h0 <= h < h1 of column w (one angle) into sacc: unclamped
+// samples with plain read-modify-writes (the caller's phases keep concurrent
+// footprints disjoint), clamped ones into the frame buffers.  The segment's
+// attenuation values are loaded kSegU at a time before any of them is used.
+template <int RC>
+__device__ __forceinline__ void bwd_segment(const float* __restrict__ at, const float* q,
+                                            float* sacc, float* srow, float* scol, int img,
+                                            int pitch, int R, const Geo& g, int H, int W, int w,
+                                            int h0, int h1, Corners& cs) {
+    const float bx = col_bx(g, w), by = col_by(g, w);
+    const float q0 = q[w];
+    const float* ap = at + (int64_t)h0 * W + w;
+    const int n = h1 - h0;
+    float hf = (float)h0 - g.cy;
+    for (int j = 0; j < n; j += kSegU) {
+        float av[kSegU];
+#pragma unroll
+        for (int k = 0; k < kSegU; ++k) av[k] = __ldg(ap + (int64_t)min(j + k, n - 1) * W);
+#pragma unroll
+        for (int k = 0; k < kSegU; ++k) {
+            if (j + k >= n) break;
+            const float x = fmaf(g.c, hf, bx), y = fmaf(g.s, hf, by);
+            hf += 1.f;
+            const float xc = fminf(fmaxf(x, 0.f), g.rmax), yc = fminf(fmaxf(y, 0.f), g.cmax);
+            float fx, fy;
+            const int i0 = ffloor(xc, fx), j0 = ffloor(yc, fy);
+            if (x == xc && y == yc) {
+                if (RC == 1) {
+                    const float v = av[k] * q0;
+                    const float ra = v * fx, rb = v - ra;     // row i0+1, row i0
+                    const float a1 = ra * fy, b1 = rb * fy;   // their column j0+1 parts
+                    float* p = sacc + i0 * pitch + j0;
+                    const float p0 = p[0], p1 = p[1], p2 = p[pitch], p3 = p[pitch + 1];
+                    p[0] = p0 + (rb - b1);
+                    p[1] = p1 + b1;
+                    p[pitch] = p2 + (ra - a1);
+                    p[pitch + 1] = p3 + a1;
+                } else {
+                    for (int r = 0; r < R; ++r) {
+                        const float v = av[k] * q[r * W + w];
+                        const float ra = v * fx, rb = v - ra;
+                        const float a1 = ra * fy, b1 = rb * fy;
+                        float* p = sacc + r * img + i0 * pitch + j0;
+                        p[0] += rb - b1;
+                        p[1] += b1;
+                        p[pitch] += ra - a1;
+                        p[pitch + 1] += a1;
+                    }
+                }
+            } else {
+                Foot f;
+                f.i0 = i0;
+                f.j0 = j0;
+                f.fx = fx;
+                f.fy = fy;
+                f.kind = (x < 0.f ? 1 : 0) | (x > g.rmax ? 2 : 0) | (y < 0.f ? 4 : 0) |
+                         (y > g.cmax ? 8 : 0);
+                if (RC == 1) {
+                    frame_add<false>(f, av[k] * q0, srow, scol, H, W, cs, 0);
+                } else {
+                    for (int r = 0; r < R; ++r)
+                        frame_add<false>(f, av[k] * q[r * W + w], srow, scol, H, W, cs, r);
+                }
+            }
+        }
+    }
+}
+
+// Backward with an epilogue: grid (G, B), cluster (G, 1, 1).  CTA g of slice b
+// splats angles [g*apc, (g+1)*apc) into its shared-memory image of the slice
+// in six phases per angle ((w mod 3) x (segment parity), column segments of
+// `seg` samples; see backward_angle_seg); the q weights of the next angle are
+// staged during the last phase.  The cluster then sums its G images over DSMEM
+// in rank order and applies the epilogue:
+//   mode 0: out = sum, or max(sum, clamp_min) when clamp_min > 0;
+//   mode 1: MLEM update out = max(Cin*sum / (sens + beta*huber(Cin)), 0)
+//           (atten_cuda.cpp:331-341), Cin and sens (R,B,H,W) in global memory.
+template <int RC>
+__global__ void __launch_bounds__(kT2, 3)
+proj_bwd2_kernel(const float* __restrict__ atten, const float* __restrict__ ratio,
+                 const float* __restrict__ em, const float* __restrict__ theta,
+                 float* __restrict__ out, const float* __restrict__ Cin,
+                 const float* __restrict__ sens, int A, int B, int Rrt, int H, int W, int apc,
+                 int seg, int ncopy, float clamp_min, int mode, float beta, float delta) {
+    extern __shared__ __align__(16) float smem[];
+    cg::cluster_group cluster = cg::this_cluster();
+    const int R = RC > 0 ? RC : Rrt;
+    const int b = blockIdx.y;
+    const int a0 = blockIdx.x * apc, a1 = min(A, a0 + apc);
+    const int pitch = slice_pitch(W);
+    const int img = H * pitch;
+    float* sacc = smem;                                     // [R][H][pitch]
+    float* sframe = sacc + R * img;                         // ncopy x [R][2][W + H]
+    float* srow = sframe + ((threadIdx.x >> 5) % ncopy) * 2 * R * (H + W);
+    float* scol = srow + 2 * R * W;
+    float* sq = sframe + frame_floats(R, H, W, ncopy);      // [2][R][W]
+    for (int i = threadIdx.x; i < R * img + frame_floats(R, H, W, ncopy); i += blockDim.x)
+        sacc[i] = 0.f;
+    if (a0 < a1) stage_q(sq + (a0 & 1) * R * W, ratio, em, a0, b, B, R, W);
+    __syncthreads();
+    Corners cs;
+    cs.zero();
+    const int nseg = (H + seg - 1) / seg;
+    for (int a = a0; a < a1; ++a) {
+        const Geo g = make_geo(theta[a], H, W);
+        const float* at = atten + ((int64_t)a * B + b) * H * W;
+        const float* q = sq + (a & 1) * R * W;
+        for (int ph = 0; ph < 6; ++ph) {
+            const int pw = ph >> 1, ps = ph & 1;
+            const int nw = (W - pw + 2) / 3, nsp = (nseg - ps + 1) / 2;
+            const int items = nw * nsp;
+            for (int it = threadIdx.x; it < items; it += blockDim.x) {
+                const int k = it / nw, cw = it - k * nw;
+                const int h0 = (ps + 2 * k) * seg;
+                bwd_segment<RC>(at, q, sacc, srow, scol, img, pitch, R, g, H, W, pw + 3 * cw, h0,
+                                min(H, h0 + seg), cs);
+            }
+            // the other q buffer was last read in the previous angle
+            if (ph == 5 && a + 1 < a1) stage_q(sq + ((a + 1) & 1) * R * W, ratio, em, a + 1, b, B, R, W);
+            __syncthreads();
+        }
+    }
+    fold_frame(cs, sacc, sframe, ncopy, img, pitch, R, H, W);
+    cluster.sync();
+    cluster_reduce(cluster, sacc, R, H, W, pitch, [&](int r, int h, int w, float s) {
+        const int64_t gi = (((int64_t)r * B + b) * H + h) * W + w;
+        if (mode == 0) {
+            out[gi] = clamp_min > 0.f ? fmaxf(s, clamp_min) : s;
+            return;
+        }
+        const float* ci = Cin + ((int64_t)r * B + b) * H * W;
+        const float cp = ci[h * W + w];
+        float den = sens[gi];
+        if (beta > 0.f) {
+            float hg = 0.f;
+            if (h > 0) { float d = cp - ci[(h - 1) * W + w]; hg += fabsf(d) <= delta ? d : copysignf(delta, d); }
+            if (h + 1 < H) { float d = cp - ci[(h + 1) * W + w]; hg += fabsf(d) <= delta ? d : copysignf(delta, d); }
+            if (w > 0) { float d = cp - ci[h * W + w - 1]; hg += fabsf(d) <= delta ? d : copysignf(delta, d); }
+            if (w + 1 < W) { float d = cp - ci[h * W + w + 1]; hg += fabsf(d) <= delta ? d : copysignf(delta, d); }
+            den = __fadd_rn(den, __fmul_rn(beta, hg));
+        }
+        out[gi] = fmaxf(__fmul_rn(cp, s) / den, 0.f);
+    });
+    cluster.sync();
+}
+
 // Backward for slices whose image does not fit in shared memory: one thread
 // per (angle, slice, column) walks the beam and adds into global memory with
 // atomics (the reference's own scheme, atten_cuda_kernel.cu:390-446); `out`
@@ -841,7 +1101,7 @@ int check_proj_sizes(int64_t A, int64_t B, int64_t R, int64_t H, int64_t W) {
 
 // Clusters of G CTAs of fn (kThreads threads, smem bytes each) that can be
 // resident at once on the current device; 0 if G is not launchable.  Cached.
-int active_clusters(const void* fn, int G, size_t smem) {
+int active_clusters(const void* fn, int G, size_t smem, int threads = kThreads) {
     struct Entry {
         const void* fn;
         int dev, G;
@@ -863,7 +1123,7 @@ int active_clusters(const void* fn, int G, size_t smem) {
         cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(G);
-        cfg.blockDim = dim3(kThreads);
+        cfg.blockDim = dim3(threads);
         cfg.dynamicSmemBytes = smem;
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -884,7 +1144,8 @@ int active_clusters(const void* fn, int G, size_t smem) {
 // waves * (angles per CTA + 2): the B clusters run in ceil(B / resident)
 // waves, and each CTA pays about two angles' worth of staging and reduction.
 // The "proj.cluster" knob forces G.
-Plan plan_cluster(const void* fn, int64_t A, int64_t B, size_t smem_per_cta) {
+Plan plan_cluster(const void* fn, int64_t A, int64_t B, size_t smem_per_cta,
+                  int threads = kThreads) {
     Plan p;
     p.smem = smem_per_cta;
     int gmax = kMaxCluster < A ? kMaxCluster : (int)A;
@@ -894,7 +1155,7 @@ Plan plan_cluster(const void* fn, int64_t A, int64_t B, size_t smem_per_cta) {
     } else {
         int64_t best = -1;
         for (int G = 1; G <= gmax; ++G) {
-            const int n = active_clusters(fn, G, smem_per_cta);
+            const int n = active_clusters(fn, G, smem_per_cta, threads);
             if (n < 1) continue;
             const int64_t cost = ceil_div(B, n) * (ceil_div(A, G) + 2);
             if (best < 0 || cost < best) {
@@ -908,12 +1169,13 @@ Plan plan_cluster(const void* fn, int64_t A, int64_t B, size_t smem_per_cta) {
     return p;
 }
 
-int launch_cluster(const void* fn, dim3 grid, int G, size_t smem, cudaStream_t st, void** args) {
+int launch_cluster(const void* fn, dim3 grid, int G, size_t smem, cudaStream_t st, void** args,
+                   int threads = kThreads) {
     FLC_TRY_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     FLC_TRY_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = grid;
-    cfg.blockDim = dim3(kThreads);
+    cfg.blockDim = dim3(threads);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
@@ -981,12 +1243,121 @@ int frame_copies(F smem_of) {
     return n;
 }
 
+// ---- lean kernels: sizes and launches ------------------------------------
+// Partial sums per column of the lean forward: about one item per thread.
+int fwd2_parts(int64_t H, int64_t W) {
+    int64_t p = kT2 / W;
+    if (p < 1) p = 1;
+    if (p > H) p = H;
+    return (int)p;
+}
+
+size_t fwd2_smem(int64_t R, int64_t H, int64_t W) {
+    return sizeof(float) * (R * H * slice_pitch((int)W) + 2 * fwd2_parts(H, W) * W);
+}
+
+size_t bwd2_smem(int64_t R, int64_t H, int64_t W, int ncopy) {
+    return sizeof(float) * (R * H * slice_pitch((int)W) + frame_floats((int)R, (int)H, (int)W, ncopy) +
+                            2 * R * W);
+}
+
+// Segment length of the lean backward: the shortest (>= 2) for which one
+// round of a phase's items fits its kT2 threads.
+int seg2_length(int64_t H, int64_t W) {
+    const int64_t nw = (W + 2) / 3;
+    int seg = 2;
+    while (seg < H && nw * (((H + seg - 1) / seg + 1) / 2) > kT2) ++seg;
+    return seg;
+}
+
+// Shared-memory budget per CTA for `per_sm` resident CTAs (1 KB of each CTA's
+// shared memory is reserved by the runtime), capped by the opt-in limit.
+size_t smem_budget(int per_sm) {
+    size_t b = (size_t)smem_per_sm() / (size_t)per_sm;
+    b = b > 1024 ? b - 1024 : 0;
+    return b < (size_t)max_smem_optin() ? b : (size_t)max_smem_optin();
+}
+
+// Frame copies of the lean backward: as many (up to kMaxFrameCopies) as keep
+// the CTAs per SM that the bare image allows.
+int bwd2_copies(int64_t R, int64_t H, int64_t W) {
+    int per_sm = 3;
+    while (per_sm > 1 && bwd2_smem(R, H, W, 1) > smem_budget(per_sm)) --per_sm;
+    int n = kMaxFrameCopies;
+    while (n > 1 && bwd2_smem(R, H, W, n) > smem_budget(per_sm)) n /= 2;
+    return n;
+}
+
+bool use_lean() { return tune(kTuneProjLegacy) == 0; }
+
 }  // namespace
+
+// Lean forward (+ ratio when I != nullptr); FLC_ERR_UNSUPPORTED (nothing
+// launched) when the slice does not fit in shared memory.
+int fwd2_launch(const float* atten, const float* C, const float* em, const float* theta,
+                float* out, const float* I, int64_t A, int64_t B, int64_t R, int64_t H, int64_t W,
+                cudaStream_t st) {
+    const size_t smem = fwd2_smem(R, H, W);
+    if (smem > (size_t)max_smem_optin()) return FLC_ERR_UNSUPPORTED;
+    const void* fn = R == 1 ? (const void*)proj_fwd2_kernel<1> : (const void*)proj_fwd2_kernel<0>;
+    FLC_TRY_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kT2, smem) != cudaSuccess ||
+        per_sm < 1)
+        per_sm = 1;
+    (void)cudaGetLastError();
+    // angle groups minimising waves x (angles per CTA + 1 for staging the slice)
+    const int64_t slots = (int64_t)sm_count() * per_sm;
+    int64_t best = -1, groups = 1;
+    for (int64_t gcount = 1; gcount <= A && gcount <= 64; ++gcount) {
+        const int64_t apc = ceil_div(A, gcount);
+        const int64_t cost = ceil_div(B * ceil_div(A, apc), slots) * (apc + 1);
+        if (best < 0 || cost < best) {
+            best = cost;
+            groups = gcount;
+        }
+    }
+    int apc = (int)ceil_div(A, groups);
+    if (int64_t t = tune(kTuneProjApc)) apc = (int)(t < A ? t : A);
+    groups = ceil_div(A, apc);
+    const int parts = fwd2_parts(H, W);
+    int iA = (int)A, iB = (int)B, iR = (int)R, iH = (int)H, iW = (int)W;
+    void* args[] = {(void*)&atten, (void*)&C, (void*)&em, (void*)&theta, (void*)&out, (void*)&I,
+                    &iA, &iB, &iR, &iH, &iW, &apc, (void*)&parts};
+    FLC_TRY_CUDA(cudaLaunchKernel(fn, dim3((unsigned)groups, (unsigned)B), dim3(kT2), args, smem, st));
+    count_launches(1);
+    return FLC_OK;
+}
+
+// Lean backward with its epilogue (mode 0: out = P^T ratio, clamped below by
+// clamp_min when > 0; mode 1: the MLEM update of Cin into out).
+// FLC_ERR_UNSUPPORTED (nothing launched) when the image does not fit.
+int bwd2_launch(const float* atten, const float* ratio, const float* em, const float* theta,
+                float* out, const float* Cin, const float* sens, int64_t A, int64_t B, int64_t R,
+                int64_t H, int64_t W, float clamp_min, int mode, float beta, float delta,
+                cudaStream_t st) {
+    if (bwd2_smem(R, H, W, 1) > (size_t)max_smem_optin()) return FLC_ERR_UNSUPPORTED;
+    const int ncopy = bwd2_copies(R, H, W);
+    const size_t smem = bwd2_smem(R, H, W, ncopy);
+    const void* fn = R == 1 ? (const void*)proj_bwd2_kernel<1> : (const void*)proj_bwd2_kernel<0>;
+    Plan p = plan_cluster(fn, A, B, smem, kT2);
+    int iA = (int)A, iB = (int)B, iR = (int)R, iH = (int)H, iW = (int)W, apc = p.apc;
+    int seg = seg2_length(H, W);
+    void* args[] = {(void*)&atten, (void*)&ratio, (void*)&em, (void*)&theta, (void*)&out,
+                    (void*)&Cin, (void*)&sens, &iA, &iB, &iR, &iH, &iW, &apc, &seg,
+                    (void*)&ncopy, &clamp_min, &mode, &beta, &delta};
+    return launch_cluster(fn, dim3(p.G, (unsigned)B), p.G, smem, st, args, kT2);
+}
 
 // Launches the backward projector (also used for the MLEM sensitivity).
 int bwd_emission_launch(const float* atten, const float* ratio, const float* em,
                         const float* theta, float* out, int64_t A, int64_t B, int64_t R,
                         int64_t H, int64_t W, float clamp_min, cudaStream_t st) {
+    if (use_lean()) {
+        const int r = bwd2_launch(atten, ratio, em, theta, out, nullptr, nullptr, A, B, R, H, W,
+                                  clamp_min, 0, 0.f, 0.f, st);
+        if (r != FLC_ERR_UNSUPPORTED) return r;
+    }
     const size_t cap = (size_t)max_smem_optin();
     int stage_tile = bwd_smem(R, H, W, true, 1) <= cap;
     if (!stage_tile && bwd_smem(R, H, W, false, 1) > cap) {
@@ -1018,6 +1389,10 @@ int bwd_emission_launch(const float* atten, const float* ratio, const float* em,
 int fwd_emission_launch(const float* atten, const float* C, const float* em, const float* theta,
                         float* Pf, const float* I, int64_t A, int64_t B, int64_t R, int64_t H,
                         int64_t W, cudaStream_t st) {
+    if (use_lean()) {
+        const int r = fwd2_launch(atten, C, em, theta, Pf, I, A, B, R, H, W, st);
+        if (r != FLC_ERR_UNSUPPORTED) return r;
+    }
     const size_t cap = (size_t)max_smem_optin();
     int stage_tile = 1, stage_c = 1;
     if (fwd_smem(R, H, W, true, true) > cap) stage_tile = 0;
@@ -1044,7 +1419,15 @@ int fwd_emission_launch(const float* atten, const float* C, const float* em, con
 int mlem_iter_launch(const float* atten, const float* em, const float* theta, const float* I,
                      const float* sens, const float* Cin, float* Cout, int64_t A, int64_t B,
                      int64_t R, int64_t H, int64_t W, float beta, float delta, cudaStream_t st,
-                     bool* fused) {
+                     bool* fused, float* ratio_ws) {
+    if (use_lean() && fwd2_smem(R, H, W) <= (size_t)max_smem_optin() &&
+        bwd2_smem(R, H, W, 1) <= (size_t)max_smem_optin()) {
+        // forward + ratio, then backward + update: two launches
+        *fused = true;
+        FLC_TRY(fwd2_launch(atten, Cin, em, theta, ratio_ws, I, A, B, R, H, W, st));
+        return bwd2_launch(atten, ratio_ws, em, theta, Cout, Cin, sens, A, B, R, H, W, 0.f, 1,
+                           beta, delta, st);
+    }
     *fused = mlem_smem(R, H, W, 1) <= (size_t)max_smem_optin();
     if (!*fused) return FLC_OK;
     int ncopy = frame_copies([&](int n) { return mlem_smem(R, H, W, n); });
@@ -1062,6 +1445,12 @@ int mlem_iter_launch(const float* atten, const float* em, const float* theta, co
 // Computes (and caches) the launch plan of the fused iteration, so that a
 // later stream capture makes no occupancy queries.
 void mlem_iter_prepare(int64_t A, int64_t B, int64_t R, int64_t H, int64_t W) {
+    if (use_lean() && bwd2_smem(R, H, W, 1) <= (size_t)max_smem_optin()) {
+        const size_t smem = bwd2_smem(R, H, W, bwd2_copies(R, H, W));
+        const void* fn = R == 1 ? (const void*)proj_bwd2_kernel<1> : (const void*)proj_bwd2_kernel<0>;
+        (void)plan_cluster(fn, A, B, smem, kT2);
+        return;
+    }
     if (mlem_smem(R, H, W, 1) > (size_t)max_smem_optin()) return;
     const size_t smem = mlem_smem(R, H, W, frame_copies([&](int n) { return mlem_smem(R, H, W, n); }));
     const void* fn = R == 1 ? (const void*)mlem_iter_kernel<1> : (const void*)mlem_iter_kernel<0>;

@@ -24,6 +24,7 @@ std::atomic<uint64_t> g_launches{0};
 thread_local char g_err[1024] = {0};
 int g_sms[64] = {0};
 int g_smem[64] = {0};
+int g_smem_sm[64] = {0};
 std::mutex g_mu;
 }  // namespace
 
@@ -53,13 +54,16 @@ static void query_device(int dev) {
     v = 0;
     cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     g_smem[dev] = v > 0 ? v : 48 * 1024;
+    v = 0;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    g_smem_sm[dev] = v > 0 ? v : g_smem[dev];
 }
 
 namespace {
 std::atomic<int64_t> g_tune[kTuneCount];
 const char* const kTuneNames[kTuneCount] = {"proj.cluster", "proj.apc", "cone.variant",
                                             "atten.chunk", "proj.bwd", "cone.test_wait_limit",
-                                            "cone.test_skip_load"};
+                                            "cone.test_skip_load", "proj.legacy"};
 }  // namespace
 
 int64_t tune(int key) { return (key >= 0 && key < kTuneCount) ? g_tune[key].load() : 0; }
@@ -75,6 +79,13 @@ int sm_count() {
     cudaGetDevice(&dev);
     query_device(dev);
     return (dev >= 0 && dev < 64) ? g_sms[dev] : 148;
+}
+
+int smem_per_sm() {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    query_device(dev);
+    return (dev >= 0 && dev < 64) ? g_smem_sm[dev] : 228 * 1024;
 }
 
 int max_smem_optin() {
@@ -94,7 +105,7 @@ int fwd_emission_launch(const float* atten, const float* C, const float* em, con
 int mlem_iter_launch(const float* atten, const float* em, const float* theta, const float* I,
                      const float* sens, const float* Cin, float* Cout, int64_t A, int64_t B,
                      int64_t R, int64_t H, int64_t W, float beta, float delta, cudaStream_t st,
-                     bool* fused);
+                     bool* fused, float* ratio_ws);
 void mlem_iter_prepare(int64_t A, int64_t B, int64_t R, int64_t H, int64_t W);
 
 namespace {
@@ -154,7 +165,7 @@ int mlem_step(const float* atten, const float* em, const float* theta, const flo
               int64_t H, int64_t W, float beta, float delta, cudaStream_t st) {
     bool fused = false;
     FLC_TRY(mlem_iter_launch(atten, em, theta, I, m.sens, Cin, Cout, A, B, R, H, W, beta, delta,
-                             st, &fused));
+                             st, &fused, m.ratio));
     if (fused) return FLC_OK;
     FLC_TRY(fwd_emission_launch(atten, Cin, em, theta, m.ratio, I, A, B, R, H, W, st));
     FLC_TRY(bwd_emission_launch(atten, m.ratio, em, theta, m.back, A, B, R, H, W, 0.f, st));

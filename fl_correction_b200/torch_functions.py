@@ -14,7 +14,8 @@ from .torch_image_util import torch_rotate_image_nd, torch_rot90_4D
 from .detector_mask import factor_mask
 
 __all__ = ["torch_extract_3D_mu_xray", "torch_extract_3D_mu_xrf", "torch_xray_atten_3D",
-           "torch_xrf_atten_3D", "torch_3D_forward_projection", "coef_xray", "coef_xrf"]
+           "torch_xrf_atten_3D", "torch_3D_forward_projection", "coef_xray", "coef_xrf",
+           "compose_cs_incident_xray_with_reference"]
 
 
 def coef_xray(param_angle_energy, n_ch=None):
@@ -36,14 +37,51 @@ def coef_xrf(param_angle_energy):
     return [[float(cs[f"{c}-{e}"]) * rho[c] * pix for c in comps] for e in elems]
 
 
+def compose_cs_incident_xray_with_reference(ref_3D, ref_cs, ref_comp):
+    """Per-voxel incident cross section sum_i spec_i * frac_i of the reference
+    volumes ref_3D (n_ref, ...) (FL/cross_section_util.py:44-66), with
+    frac_i = max(ref_i / (sum_k ref_k + 1e-12), 0), the fractions of
+    FL.core.cal_frac(ref_3D, scale_range=[], enable_scale=False)
+    (FL/core.py:159-205) without its Otsu-threshold mask: the reference masks
+    with skimage's threshold_multiotsu and falls back to no mask when the
+    threshold fails, which is the case this build reproduces.  FP64 on the
+    device of ref_3D (numpy input: cuda)."""
+    n_ref = int(ref_cs["n_ref"])
+    if len(ref_3D) != n_ref:
+        raise AssertionError("number of references and number of 3D stack in 'ref_3D' does not match")
+    dev = ref_3D.device if isinstance(ref_3D, torch.Tensor) else torch.device("cuda")
+    ref = torch.as_tensor(np.asarray(ref_3D) if not isinstance(ref_3D, torch.Tensor) else ref_3D,
+                          dtype=torch.float64, device=dev)
+    tot = ref.sum(dim=0) + 1e-12
+    fr = torch.nan_to_num(ref / tot, nan=0.0, posinf=0.0, neginf=0.0).clamp_(min=0.0)
+    spec = [float(np.asarray(ref_cs[f"{ref_comp}-x_ref{i + 1}"]).reshape(-1)[0]) for i in range(n_ref)]
+    cs = torch.zeros_like(tot)
+    for i in range(n_ref):
+        cs += spec[i] * fr[i]
+    return cs
+
+
 def torch_extract_3D_mu_xray(frac_4D, param_angle_energy, dict_use_ref_rotate={}):
     """mu_x[j] = frac[j] * cs[comp_j-x] * rho_j * pix; channels without a
-    compound stay 1 (FL/torch_functions.py:8-52)."""
-    if len(dict_use_ref_rotate) > 0 and dict_use_ref_rotate.get("use_ref", False):
-        raise NotImplementedError("reference-spectrum cross sections are not implemented")
+    compound stay 1 (FL/torch_functions.py:8-52).  With dict_use_ref_rotate
+    ({'use_ref': True, 'ref_3D': (n_ref, S, H, W) already rotated,
+    'ref_comp': compound}) the cross section of ref_comp is the per-voxel
+    volume of compose_cs_incident_xray_with_reference (:22-37)."""
+    use_ref = len(dict_use_ref_rotate) > 0 and dict_use_ref_rotate.get("use_ref", False)
+    ref_comp = dict_use_ref_rotate.get("ref_comp") if use_ref else None
+    if use_ref and ref_comp is None:
+        raise AssertionError("need to provide 'ref_comp', e.g, 'LiNiO2'")
     mu_x = torch.ones_like(frac_4D)
+    comps = param_angle_energy["cs"]["elem_compound"]
     for j, cf in enumerate(coef_xray(param_angle_energy)):
-        mu_x[j] = frac_4D[j] * torch.tensor(cf, dtype=frac_4D.dtype, device=frac_4D.device)
+        if use_ref and comps[j] == ref_comp:
+            cs3 = compose_cs_incident_xray_with_reference(dict_use_ref_rotate["ref_3D"],
+                                                          param_angle_energy["cs"], ref_comp)
+            coef = (cs3.to(frac_4D.device) * (param_angle_energy["rho"][ref_comp] *
+                                              param_angle_energy["pix"])).to(frac_4D.dtype)
+            mu_x[j] = frac_4D[j] * coef
+        else:
+            mu_x[j] = frac_4D[j] * torch.tensor(cf, dtype=frac_4D.dtype, device=frac_4D.device)
     return mu_x
 
 

@@ -193,6 +193,23 @@ FLC_API int flc_atten_maps(const float* frac, const float* theta, const float* c
                    int64_t Mz, int64_t Mx, int64_t My, int incident_mode, int xrf_mode,
                    int64_t chunk, void* workspace, size_t workspace_bytes, void* stream);
 
+/* flc_atten_maps with a reference-spectrum incident cross section (the
+ * XANES case of FL/torch_functions.py:22-37, FL/cross_section_util.py:44-66):
+ * frac holds n_ch compound fractions followed by n_ref raw reference volumes
+ * (n_ch + n_ref channels, all rotated with the same grid_sample rotation);
+ * coef_x (A, n_ch) and coef_f (A, L, n_ch) cover the compounds only.  The
+ * incident coefficient of compound ref_ch is, per voxel, sum_i coef_ref[a][i] *
+ * max(ref_i / (sum_k ref_k + 1e-12), 0), with coef_ref (A, n_ref) the spectrum
+ * values cs[comp-x_ref{i+1}] * rho * pix per angle.  n_ref = 0 is
+ * flc_atten_maps.  Workspace: flc_atten_workspace_bytes(n_ch + n_ref, ...). */
+FLC_API int flc_atten_maps_ref(const float* frac, const float* theta, const float* coef_x,
+                               const float* coef_f, const float* coef_ref, const float* u,
+                               const float* v, float* out, int64_t n_ch, int64_t n_ref,
+                               int64_t ref_ch, int64_t S, int64_t H, int64_t W, int64_t A,
+                               int64_t L, int64_t Mz, int64_t Mx, int64_t My, int incident_mode,
+                               int xrf_mode, int64_t chunk, void* workspace,
+                               size_t workspace_bytes, void* stream);
+
 /* The two stages of flc_atten_maps, for callers that schedule angle chunks
  * themselves.  flc_atten_stage writes the incident term of angles
  * [a0, a0+n_a) into out (L, A, S, H, W) and, if write_mu, the fluorescence mu

@@ -206,6 +206,48 @@ def main():
     out["cone_mu"] = mu_c
     out["cone_out"] = cone_conv3d(mu_c, mask).numpy()
 
+    # ---- reference-spectrum incident cross section (XANES) ---------------
+    # FL/torch_functions.py:22-37 -> FL/cross_section_util.py:44-66, which
+    # calls cal_frac without importing it: the FL.core function it names is
+    # put into that module's namespace.  skimage is stubbed, so cal_frac's
+    # Otsu mask falls back to 1 (FL/core.py:177-179).
+    import FL.core as core
+    import FL.cross_section_util as csu
+    csu.cal_frac = core.cal_frac
+    rng2 = np.random.default_rng(20240612)
+    n_angle = 5
+    pr = make_param(3, rng2, energy_len=n_angle)
+    comps = pr["elem_compound"]
+    ref_comp = comps[1]
+    pr["cs"]["n_ref"] = 2
+    for i in range(2):
+        pr["cs"][f"{ref_comp}-x_ref{i + 1}"] = rng2.uniform(30.0, 160.0, n_angle)
+    pr["pix"] = 8e-4
+    fr = (rng2.random((3, 6, 16, 16)) * 0.8).astype(np.float32)
+    fr[:, :, 3:11, 5:12] += 0.4
+    ref3 = rng2.uniform(0.1, 1.0, (2, 6, 16, 16)).astype(np.float32)
+    ref3[0, :, 2:8, 4:14] *= 4.0
+    out["xref_frac"] = fr
+    out["xref_ref3d"] = ref3
+    a_id = 3
+    ang = np.linspace(0.0, 180.0, n_angle, endpoint=False)
+    meta["xref"] = {"ref_comp": ref_comp, "angle_id": a_id, "angles_deg": ang.tolist(),
+                    "param": {"cs": {k: (np.asarray(v).tolist() if k not in
+                                         ("elem_type", "elem_compound") else v)
+                                     for k, v in pr["cs"].items()},
+                              "rho": pr["rho"], "pix": pr["pix"], "elem_type": pr["elem_type"],
+                              "elem_compound": pr["elem_compound"],
+                              "em_cs": {k: np.asarray(v).tolist() for k, v in pr["em_cs"].items()}}}
+    d_ref = {"use_ref": True, "ref_3D": ref3, "ref_comp": ref_comp}
+    d_rot = au.update_dict_use_ref_at_angle(d_ref, ang[a_id])
+    p_a = au.extract_single_value_param(pr, a_id, d_rot)
+    fr_rot = tiu.torch_rotate_image_nd(torch.tensor(fr), torch.tensor(ang[a_id] / 180.0 * np.pi,
+                                                                      dtype=torch.float64))
+    out["xref_atten_x"] = tf.torch_xray_atten_3D(fr_rot, p_a, d_rot)
+    out["xref_ref3d_rot"] = np.asarray(d_rot["ref_3D"], np.float32)
+    out["xref_mu_x"] = tf.torch_extract_3D_mu_xray(fr_rot, p_a, d_rot).numpy()
+    meta["xref"]["selected_x_ref"] = [float(p_a["cs"][f"{ref_comp}-x_ref{i + 1}"]) for i in range(2)]
+
     np.savez_compressed(os.path.join(HERE, "ref_cpu.npz"), **out)
     with open(os.path.join(HERE, "ref_cpu.json"), "w") as f:
         json.dump(meta, f, indent=1)

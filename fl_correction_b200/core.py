@@ -217,10 +217,22 @@ def cal_xrf_atten_at_angles(frac_4D, param, angle_list, detector_mask, detector_
                             position_det="r", dict_use_ref={}, fsave=None):
     """exp(-cone(mu_f)) at every angle for every element (FL/core.py:19-52):
     returns (L, A, S, H, W) on frac_4D's device."""
-    if abs(detector_offset_angle) > 1e-2 * 180 / np.pi or position_det != "r":
-        raise NotImplementedError("only detector_offset_angle=0, position_det='r' is implemented")
     # dict_use_ref does not enter the fluorescence mu (FL/torch_functions.py:55-81;
     # FL/core.py:36-47 only selects per-angle parameters with it)
+    if abs(detector_offset_angle) > 1e-2 * 180 / np.pi or position_det != "r":
+        # the per-angle path of the reference, on the native kernels
+        # (offset semantics: torch_functions.torch_xrf_atten_3D)
+        from .torch_functions import torch_xrf_atten_3D
+        from .torch_image_util import torch_rotate_image_nd
+        maps = []
+        for a, ang in enumerate(angle_list):
+            fr = torch_rotate_image_nd(frac_4D, float(ang) / 180.0 * np.pi)
+            p = extract_single_value_param(param, a)
+            att = torch_xrf_atten_3D(fr, p, detector_mask, detector_offset_angle, position_det)
+            maps.append(torch.as_tensor(att[:len(param["elem_type"])], device=frac_4D.device))
+        maps = torch.stack(maps, dim=1).contiguous()
+        _save(fsave, "fl", param, maps)
+        return maps
     cx, cf = atten_coefficients(param, len(angle_list), frac_4D.shape[0])
     maps = atten_maps(frac_4D, angle_list, cx, cf, mask_factors(detector_mask, frac_4D.device),
                       incident="none", xrf=True)

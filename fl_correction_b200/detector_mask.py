@@ -17,7 +17,8 @@ import os
 
 import numpy as np
 
-__all__ = ["generate_detector_mask", "prep_detector_mask3D", "load_mask3D", "factor_mask"]
+__all__ = ["generate_detector_mask", "prep_detector_mask3D", "load_mask3D", "factor_mask",
+           "detector_mask_device"]
 
 
 def _profile(n_cells, depth, tan_a, cos_a, apex):
@@ -124,3 +125,29 @@ def load_mask3D(fn="mask3D.npz"):
         raise FileNotFoundError(fn)
     with np.load(fn) as z:
         return {k: z[k] for k in z.files}
+
+
+def detector_mask_device(alfa0, theta0, leng0, device="cuda", dense=False):
+    """The cone mask generated on the device (flc_detector_mask): returns
+    (u, v, (Mz, Mx, My)) -- the FP32 rank-one factors of every depth plane,
+    the form atten_maps and the cone kernels take (core.mask_factors gives the
+    same tuple from a host mask) -- and, with dense=True, also the FP64 mask
+    (Mz, Mx, My) that generate_detector_mask returns, as a device tensor."""
+    import ctypes
+
+    import torch
+
+    from . import _lib
+    Mz, Mx, My, nb = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64(), ctypes.c_size_t()
+    _lib.call("flc_detector_mask_shape", float(alfa0), float(theta0), int(leng0),
+              ctypes.byref(Mz), ctypes.byref(Mx), ctypes.byref(My), ctypes.byref(nb))
+    shape = (Mz.value, Mx.value, My.value)
+    dev = torch.device(device)
+    u = torch.empty((shape[1], shape[0]), dtype=torch.float32, device=dev)
+    v = torch.empty((shape[1], shape[2]), dtype=torch.float32, device=dev)
+    d = torch.empty(shape, dtype=torch.float64, device=dev) if dense else None
+    scratch = torch.empty(max(1, nb.value // 8), dtype=torch.float64, device=dev)
+    with torch.cuda.device(dev):
+        _lib.call("flc_detector_mask", float(alfa0), float(theta0), int(leng0), _lib.ptr(u),
+                  _lib.ptr(v), _lib.ptr(d), _lib.ptr(scratch), nb.value, _lib.stream())
+    return (u, v, shape, d) if dense else (u, v, shape)

@@ -15,7 +15,7 @@ from .detector_mask import factor_mask
 
 __all__ = ["torch_extract_3D_mu_xray", "torch_extract_3D_mu_xrf", "torch_xray_atten_3D",
            "torch_xrf_atten_3D", "torch_3D_forward_projection", "coef_xray", "coef_xrf",
-           "compose_cs_incident_xray_with_reference"]
+           "compose_cs_incident_xray_with_reference", "offset_canvas"]
 
 
 def coef_xray(param_angle_energy, n_ch=None):
@@ -110,23 +110,59 @@ def torch_xray_atten_3D(frac_4D, param_angle_energy, dict_use_ref_rotate={}, fla
     return out
 
 
+def offset_canvas(H, W, phi):
+    """Side of the square canvas that holds an H x W slice rotated by phi
+    radians: the reference's _rotated_hw size (FL/torch_image_util.py:5-10),
+    raised by one where needed so that the padding on each side is a whole
+    number of pixels (the rotation centre then stays on the slice centre)."""
+    c, s = abs(np.cos(phi)), abs(np.sin(phi))
+    n = max(int(H * c + W * s + 0.5), int(W * c + H * s + 0.5), H, W)
+    if (n - H) % 2:
+        n += 1
+    return n
+
+
+def _path_sum(mu, mask, position_det):
+    """Cone path sum toward a detector on the right / left of the slice:
+    rot90, cal_atten_cuda, rot90 back (FL/torch_functions.py:142-171)."""
+    if position_det == "r":
+        mu90 = torch_rot90_4D(mu, ax=0, mode="clock")
+    elif position_det == "l":
+        mu90 = torch_rot90_4D(mu, ax=0, mode="c-clock")
+    else:
+        raise ValueError("position_det must be 'r' or 'l'")
+    res = cal_atten_cuda(mu90.to(torch.float32).contiguous(), mask)
+    return torch_rot90_4D(res, ax=0, mode="c-clock" if position_det == "r" else "clock")
+
+
 def torch_xrf_atten_3D(frac_4D, param_angle_energy, detector_mask, detector_offset_angle=0,
                        position_det="r"):
     """Fluorescence attenuation exp(-cone(mu_f)) toward a detector on the
-    right ('r') or left ('l') (FL/torch_functions.py:110-176).  The
-    detector-offset branch of the reference (:134-166) is not implemented."""
-    if abs(detector_offset_angle / 180.0 * np.pi) > 1e-2:
-        raise NotImplementedError("detector_offset_angle != 0 is not implemented")
+    right ('r') or left ('l') (FL/torch_functions.py:110-176).
+
+    detector_offset_angle (degrees, the detector at 90 - offset degrees to the
+    beam) rotates mu_f counter-clockwise by the offset about the slice centre
+    onto a zero-padded square canvas (offset_canvas) at the same pixel size,
+    takes the cone path sum there, rotates the path sum back by -offset and
+    crops the slice's own window.  The reference's branch (:134-166) differs:
+    its expanded-canvas rotation (enable_crop=False) also magnifies the slice
+    by the canvas ratio, because affine_grid maps normalised output
+    coordinates onto normalised input coordinates; it rotates mu a second time
+    by the offset after rot90 (:146); and its column crop start divides by
+    -0.5 (:161), so the crop keeps the first W columns.  Those steps are not
+    reproduced."""
+    phi = float(np.float32(detector_offset_angle / 180.0 * np.pi))
     mu_xrf = torch_extract_3D_mu_xrf(frac_4D, param_angle_energy)
-    if position_det == "r":
-        mu90 = torch_rot90_4D(mu_xrf, ax=0, mode="clock")
-    elif position_det == "l":
-        mu90 = torch_rot90_4D(mu_xrf, ax=0, mode="c-clock")
-    else:
-        raise ValueError("position_det must be 'r' or 'l'")
     mask = torch.as_tensor(np.asarray(detector_mask), dtype=torch.float32, device=frac_4D.device)
-    res = cal_atten_cuda(mu90.to(torch.float32).contiguous(), mask)
-    res = torch_rot90_4D(res, ax=0, mode="c-clock" if position_det == "r" else "clock")
+    if abs(phi) <= 1e-2:
+        res = _path_sum(mu_xrf, mask, position_det)
+    else:
+        H, W = mu_xrf.shape[-2:]
+        n = offset_canvas(H, W, phi)
+        pr, pc = (n - H) // 2, (n - W) // 2
+        mu_c = torch.nn.functional.pad(mu_xrf, (pc, n - W - pc, pr, n - H - pr))
+        res_c = _path_sum(torch_rotate_image_nd(mu_c, phi), mask, position_det)
+        res = torch_rotate_image_nd(res_c.contiguous(), -phi)[..., pr:pr + H, pc:pc + W]
     return torch.exp(-res).cpu().numpy()
 
 

@@ -287,6 +287,23 @@ FLC_API int flc_xrf_project_adjoint(const float* frac, const float* theta, const
                                     int64_t Mx, int64_t My, int incident_mode, int64_t chunk,
                                     void* workspace, size_t workspace_bytes, void* stream);
 
+/* ---------------------------------------------------------------------
+ * Detector cone mask on the device (FL/detector_mask.py:22-151,
+ * generate_detector_mask with g_mask and g_radial_mask_approximate).
+ * alfa0, theta0: full horizontal / vertical cone angles in degrees; leng0:
+ * depth in voxels.  flc_detector_mask_shape gives the mask extents (Mz, Mx =
+ * leng0, My) and the FP64 scratch the generator needs.  flc_detector_mask
+ * writes the rank-one factors of every depth plane, u (Mx, Mz) and v (Mx, My)
+ * as FP32 (mask[dz][d][dy] = u[d][dz] * v[d][dy], the input of
+ * flc_cone_atten_separable and flc_atten_maps), and, when dense != NULL, the
+ * FP64 mask (Mz, Mx, My) the reference returns.  No counterpart entry point
+ * in the reference (it builds the mask on the host with numba).
+ * --------------------------------------------------------------------- */
+FLC_API int flc_detector_mask_shape(double alfa0, double theta0, int64_t leng0, int64_t* Mz,
+                                    int64_t* Mx, int64_t* My, size_t* scratch_bytes);
+FLC_API int flc_detector_mask(double alfa0, double theta0, int64_t leng0, float* u, float* v,
+                              double* dense, void* scratch, size_t scratch_bytes, void* stream);
+
 /* Rotation with torch grid_sample semantics (bilinear, zero padding,
  * align_corners=False, same-size output): out (N, H, W) from x (N, H, W).
  * cos_t/sin_t are the FP32 matrix entries.  Replaces torch_rotate_image_nd

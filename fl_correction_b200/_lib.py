@@ -45,6 +45,9 @@ SIGNATURES = {
     "flc_detector_mask_shape": (_int, [_f64, _f64, _i64, ctypes.POINTER(_i64), ctypes.POINTER(_i64),
                                        ctypes.POINTER(_i64), ctypes.POINTER(_sz)]),
     "flc_detector_mask": (_int, [_f64, _f64, _i64, _vp, _vp, _vp, _vp, _sz, _vp]),
+    "flc_cal_frac_workspace_bytes": (_sz, [_i64, _i64]),
+    "flc_cal_frac": (_int, [_vp, _vp, _vp, _vp, _i64, _i64, _int, _f64, _f64, _int, _f64, _vp, _sz,
+                            _vp]),
     "flc_atten_maps_ref": (_int, [_vp] * 8 + [_i64] * 11 + [_int, _int, _i64, _vp, _sz, _vp]),
     "flc_atten_stage": (_int, [_vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _i64,
                                _i64, _i64, _int, _int, _vp]),

@@ -18,7 +18,7 @@ from .atten_util import extract_single_value_param
 from .cuda_lib.atten_cuda import forward_emission_batch
 from .detector_mask import factor_mask
 
-__all__ = ["atten_coefficients", "ref_coefficients", "mask_factors", "atten_maps", "pick_chunk", "cal_xrf_atten_at_angles",
+__all__ = ["cal_frac", "atten_coefficients", "ref_coefficients", "mask_factors", "atten_maps", "pick_chunk", "cal_xrf_atten_at_angles",
            "cal_xray_atten_at_angles", "cal_total_atten_at_angles", "cal_atten_at_angles",
            "re_projection_cuda"]
 
@@ -317,3 +317,44 @@ def re_projection_cuda(img3D, angle_list, param=None, rho_compound=1, atten_coef
     theta = torch.tensor(np.asarray(angle_list) / 180.0 * np.pi, dtype=torch.float, device=device)
     em_t = torch.tensor(np.asarray(em), dtype=torch.float, device=device)
     return forward_emission_batch(at.contiguous(), C.contiguous(), em_t, theta).cpu().numpy()
+
+
+def cal_frac(*args, scale_range=[0.02, 0.98], enable_scale=True, scale_limit=0.95, img_mask=None,
+             out=None):
+    """Fractions from concentration volumes, FL/core.py:159-205, on the device
+    (flc_cal_frac): img (n, ...) -- one array/tensor, or several with the same
+    shape -- summed over n; each channel divided by the sum (NaN, inf and
+    negatives set to 0), clamped to its [scale_range] quantiles of positive
+    values where it has more than 100, and scaled by sum / (its
+    scale_limit-quantile) when enable_scale.  img_mask: the threshold mask
+    (None: 1, the reference's value when its multi-Otsu threshold fails, as it
+    does without scikit-image).  Returns {'frac', 'img_sum', 'img_mask'} with
+    device tensors (float32)."""
+    if len(args) == 1:
+        img = args[0]
+    else:
+        img = torch.stack([torch.as_tensor(a) for a in args])
+    img = torch.as_tensor(img if isinstance(img, torch.Tensor) else np.asarray(img, np.float32),
+                          dtype=torch.float32)
+    if not img.is_cuda:
+        img = img.cuda()
+    if img.dim() == 2:
+        img = img[None]
+    img = img.contiguous()
+    n = img.shape[0]
+    N = img[0].numel()
+    dev = img.device
+    mask = None
+    if img_mask is not None:
+        mask = torch.as_tensor(img_mask, dtype=torch.float32, device=dev).expand(img.shape[1:]).contiguous()
+    frac = out if out is not None else torch.empty_like(img)
+    isum = torch.empty(img.shape[1:], dtype=torch.float32, device=dev)
+    nb = int(_lib.query("flc_cal_frac_workspace_bytes", n, N))
+    ws = _lib.workspace(nb, dev)
+    use = 1 if len(scale_range) else 0
+    r0, r1 = (float(scale_range[0]), float(scale_range[1])) if use else (0.0, 1.0)
+    with torch.cuda.device(dev):
+        _lib.call("flc_cal_frac", _lib.ptr(img), _lib.ptr(mask), _lib.ptr(frac), _lib.ptr(isum), n, N,
+                  use, r0, r1, 1 if enable_scale else 0, float(scale_limit), _lib.ptr(ws), nb,
+                  _lib.stream())
+    return {"frac": frac, "img_sum": isum, "img_mask": mask if mask is not None else 1}

@@ -14,7 +14,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .core import atten_coefficients, atten_maps, atten_workspace_bytes, mask_factors
+from .core import atten_coefficients, atten_maps, atten_workspace_bytes, cal_frac, mask_factors
 from .detector_mask import generate_detector_mask
 
 __all__ = ["CorrectedMLEM"]
@@ -31,12 +31,28 @@ class CorrectedMLEM:
     fixed_frac     (n_ch - L, S, N, N) fractions of the non-element compounds.
     incident       'own' (element i's incident term uses compound i, as
                    FL/core.py:80-81 does), 'all' (legacy product) or 'none'.
+    feedback       how the estimate enters mu at each rebuild: 'bounded'
+                   (default) clips to [0, 1] and scales voxels whose
+                   elements' total exceeds 1 down to 1; 'cal_frac' runs the
+                   reference's cal_frac on the device (FL/core.py:159-205, as
+                   FL/example/demo.py:249-265 feeds the estimate back: per
+                   element fraction of the total clamped to its
+                   [scale_range] quantiles, times total / its scale_limit
+                   quantile; threshold mask 1).  'bounded' keeps cal_frac's
+                   non-negativity and replaces its quantile clamp and
+                   percentile scaling by the mass-fraction bound.
     """
 
     def __init__(self, param, angles_deg, mask, shape, fixed_frac=None, incident="own",
-                 beta=0.0, delta=0.01, device="cuda", chunk=0, bound_frac=True):
+                 beta=0.0, delta=0.01, device="cuda", chunk=0, bound_frac=True,
+                 feedback="bounded", cal_frac_args=None):
         self.device = torch.device(device)
         self.bound_frac = bound_frac
+        if feedback not in ("bounded", "cal_frac"):
+            raise ValueError("feedback must be 'bounded' or 'cal_frac'")
+        self.feedback = feedback
+        self.cal_frac_args = dict(scale_range=[0.02, 0.98], enable_scale=True, scale_limit=0.95)
+        self.cal_frac_args.update(cal_frac_args or {})
         self.param = param
         self.L = len(param["elem_type"])
         self.n_ch = len(param["elem_compound"])
@@ -75,16 +91,20 @@ class CorrectedMLEM:
     def recompute_attenuation(self, C, cone_events=None):
         """atten[l, a] from concentrations C (L, S, H, W) on the device.
 
-        The estimate enters mu as mass fractions: clipped to [0, 1] and, where
-        the elements' total exceeds 1, scaled down to a total of 1 (with
-        bound_frac, the default).  The reference likewise feeds back bounded
-        fractions, not raw MLEM values (cal_frac, FL/core.py:159-205).
-        Without a bound, voxels that MLEM overshoots raise mu, which lowers
-        the modelled signal there, which raises them further: the outer loop
+        With feedback 'bounded' the estimate enters mu as mass fractions:
+        clipped to [0, 1] and, where the elements' total exceeds 1, scaled
+        down to a total of 1 (with bound_frac, the default); with 'cal_frac'
+        as the reference's cal_frac makes them (FL/core.py:159-205).  Either
+        way bounded fractions, not raw MLEM values, are fed back: without a
+        bound, voxels that MLEM overshoots raise mu, which lowers the
+        modelled signal there, which raises them further, and the outer loop
         diverges on absorbing samples."""
         f = self.frac[:self.L]
-        f.copy_(C)
-        if self.bound_frac:
+        if self.feedback == "cal_frac":
+            cal_frac(C.contiguous(), out=f, **self.cal_frac_args)
+        else:
+            f.copy_(C)
+        if self.feedback == "bounded" and self.bound_frac:
             f.clamp_(0.0, 1.0)
             tot = f.sum(dim=0, keepdim=True).clamp_(min=1.0)
             f.div_(tot)

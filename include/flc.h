@@ -304,6 +304,27 @@ FLC_API int flc_detector_mask_shape(double alfa0, double theta0, int64_t leng0, 
 FLC_API int flc_detector_mask(double alfa0, double theta0, int64_t leng0, float* u, float* v,
                               double* dense, void* scratch, size_t scratch_bytes, void* stream);
 
+/* ---------------------------------------------------------------------
+ * cal_frac on the device (FL/core.py:159-205): frac (n_ch, N) from
+ * concentrations img (n_ch, N), N voxels per channel.
+ *   img_sum = (sum_i img_i + 1e-12) * mask      (mask NULL: 1)
+ *   tmp_i   = img_i / img_sum, NaN / inf / negative -> 0
+ *   use_range: where tmp_i has more than 100 positive values it is clamped
+ *     to its int(l*r0)-th and (int(l*r1)-1)-th smallest positive values
+ *   enable_scale: frac_i = tmp_i * mask * img_sum / p, p the
+ *     int(l*scale_limit)-th smallest positive img_sum; else tmp_i * mask
+ * img_sum (optional, N) receives the masked sum.  The order statistics are
+ * exact (radix select on the FP32 bit patterns).  The reference's mask is a
+ * multi-Otsu threshold that falls back to 1 without scikit-image; the caller
+ * passes a mask or NULL.  Workspace: flc_cal_frac_workspace_bytes.  n_ch <= 8.
+ * No counterpart entry point in the reference (numpy on the host).
+ * --------------------------------------------------------------------- */
+FLC_API size_t flc_cal_frac_workspace_bytes(int64_t n_ch, int64_t N);
+FLC_API int flc_cal_frac(const float* img, const float* mask, float* frac, float* img_sum,
+                         int64_t n_ch, int64_t N, int use_range, double r0, double r1,
+                         int enable_scale, double scale_limit, void* workspace,
+                         size_t workspace_bytes, void* stream);
+
 /* Rotation with torch grid_sample semantics (bilinear, zero padding,
  * align_corners=False, same-size output): out (N, H, W) from x (N, H, W).
  * cos_t/sin_t are the FP32 matrix entries.  Replaces torch_rotate_image_nd

@@ -324,3 +324,30 @@ def xrf_project_adjoint(frac, theta, cx, cf, mask, em, gPf, incident="own"):
         dfr = dmux * cx[a][:, None, None, None] + np.einsum("ij,ishw->jshw", cf[a].astype(np.float64), dmuf)
         dC += rotate_adjoint(dfr[:L], th[a])
     return dC
+
+
+def cal_frac(img, scale_range=(0.02, 0.98), enable_scale=True, scale_limit=0.95):
+    """cal_frac, FL/core.py:159-205, with the threshold mask at its fallback
+    value 1 (FL/core.py:177-179; the mask needs scikit-image): FP32 sums and
+    ratios as numpy computes them on FP32 volumes.  Returns frac (float32)."""
+    img = np.asarray(img, np.float32)
+    s = np.sum(img, axis=0) + np.float32(1e-12)
+    ss = np.sort(s[s > 0], axis=None)
+    ratio = np.float32(1.0)
+    if enable_scale and ss.size:
+        ratio = s / ss[int(ss.size * scale_limit)]
+    out = np.zeros(img.shape, np.float32)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        for i in range(img.shape[0]):
+            t = img[i] / s
+            t[~np.isfinite(t)] = 0
+            t[t < 0] = 0
+            if len(scale_range):
+                ts = np.sort(t[t > 0])
+                n = ts.size
+                if n > 100:
+                    ts = ts[int(n * scale_range[0]):int(n * scale_range[1])]
+                    t[t >= ts[-1]] = ts[-1]
+                    t[t <= ts[0]] = ts[0]
+            out[i] = t * ratio
+    return out

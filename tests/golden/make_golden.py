@@ -248,6 +248,24 @@ def main():
     out["xref_mu_x"] = tf.torch_extract_3D_mu_xray(fr_rot, p_a, d_rot).numpy()
     meta["xref"]["selected_x_ref"] = [float(p_a["cs"][f"{ref_comp}-x_ref{i + 1}"]) for i in range(2)]
 
+    # ---- cal_frac (FL/core.py:159-205) -----------------------------------
+    # skimage is stubbed, so adaptive_threshold fails and cal_frac falls back
+    # to mask = 1 (FL/core.py:177-179), the case flc_cal_frac reproduces
+    rng3 = np.random.default_rng(20240613)
+    cimg = (rng3.random((3, 6, 20, 20)) * 1.5).astype(np.float32)
+    cimg[:, :, :3, :] = 0.0                    # empty rows: zero sums
+    cimg[1, 2:4, 5:9, 5:9] = -0.2              # negatives (rm_abnormal)
+    cimg[2, :, 10:, 12:] *= 6.0                # a bright corner for the clamps
+    out["calfrac_img"] = cimg
+    r = core.cal_frac(cimg, scale_range=[0.02, 0.98], enable_scale=True, scale_limit=0.95)
+    out["calfrac_default"] = r["frac"]
+    out["calfrac_default_sum"] = r["img_sum"]
+    meta["calfrac_pix_max"] = float(r["pix_max"])
+    r = core.cal_frac(cimg, scale_range=[], enable_scale=False)
+    out["calfrac_plain"] = r["frac"]
+    r = core.cal_frac(cimg, scale_range=[0.1, 0.7], enable_scale=True, scale_limit=0.5)
+    out["calfrac_other"] = r["frac"]
+
     np.savez_compressed(os.path.join(HERE, "ref_cpu.npz"), **out)
     with open(os.path.join(HERE, "ref_cpu.json"), "w") as f:
         json.dump(meta, f, indent=1)

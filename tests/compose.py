@@ -85,8 +85,19 @@ def oracle_atten(frac, theta, cx, cf, mask, z_range=None):
     return out
 
 
+def feedback_fractions(C, feedback, cal_frac_args=None):
+    """The fractions fed back at a rebuild (numpy): 'bounded' as
+    bounded_fractions, 'cal_frac' as the reference's cal_frac (the oracle's
+    restatement, FL/core.py:159-205, threshold mask 1)."""
+    if feedback == "cal_frac":
+        kw = dict(scale_range=[0.02, 0.98], enable_scale=True, scale_limit=0.95)
+        kw.update(cal_frac_args or {})
+        return O.cal_frac(np.asarray(C, np.float32), **kw).astype(np.float64)
+    return bounded_fractions(C)
+
+
 def oracle_corrected_mlem(param, angles_deg, mask, I, fixed_frac, n_iter, recompute_every,
-                          C0=None, beta=0.0, delta=0.01, z_range=None):
+                          C0=None, beta=0.0, delta=0.01, z_range=None, feedback="bounded"):
     """Corrected MLEM in FP64 (host).  I (L, A, S, W); fixed_frac (n_ch-L, S,
     H, W) fractions of the non-element compounds.  With z_range=(z0, z1) the
     result is valid on those slices only: the inputs must then hold the slab
@@ -105,7 +116,9 @@ def oracle_corrected_mlem(param, angles_deg, mask, I, fixed_frac, n_iter, recomp
     done, k_done = 0, 0
     while done < n_iter:
         k = min(recompute_every, n_iter - done)
-        frac = np.concatenate([bounded_fractions(C), np.asarray(fixed_frac, np.float64)])
+        if feedback != "bounded" and z_range is not None:
+            raise ValueError("cal_frac's order statistics couple all slices: no slab form")
+        frac = np.concatenate([feedback_fractions(C, feedback), np.asarray(fixed_frac, np.float64)])
         zr = None
         if z_range is not None:
             # rebuild on the slices later rebuilds still need
@@ -179,7 +192,7 @@ def reference_atten(ref, frac, theta64, cx, cf, mask):
 
 
 def reference_corrected_mlem(ref, param, angles_deg, mask, I, fixed_frac, n_iter,
-                             recompute_every, C0=None, beta=0.0, delta=0.01):
+                             recompute_every, C0=None, beta=0.0, delta=0.01, feedback="bounded"):
     """Corrected MLEM through the reference's kernels (FP32, GPU).  I (L, A,
     S, W) device tensor; fixed_frac (n_ch-L, S, H, W) device tensor."""
     import torch
@@ -197,8 +210,12 @@ def reference_corrected_mlem(ref, param, angles_deg, mask, I, fixed_frac, n_iter
     done = 0
     while done < n_iter:
         k = min(recompute_every, n_iter - done)
-        f = C.clamp(0.0, 1.0)
-        f = f / f.sum(dim=0, keepdim=True).clamp(min=1.0)
+        if feedback == "cal_frac":
+            f = torch.tensor(feedback_fractions(C.cpu().numpy(), feedback), dtype=torch.float32,
+                             device=dev)
+        else:
+            f = C.clamp(0.0, 1.0)
+            f = f / f.sum(dim=0, keepdim=True).clamp(min=1.0)
         frac = torch.cat([f, fixed_frac]).contiguous()
         att = reference_atten(ref, frac, th64, cx, cf, mask)
         for l in range(L):

@@ -65,3 +65,28 @@ def test_cfg0_corrected_mlem_vs_reference_kernels(cfg0):
     e = compose.relative_errors(C.cpu().numpy(), Cr.cpu().numpy())
     print("cfg0 vs reference", e)
     assert rel_err(C.cpu().numpy(), Cr.cpu().numpy()) < TOL_MLEM
+
+
+def test_cal_frac_feedback_vs_reference_kernels():
+    """The corrected loop with the reference's own feedback step (cal_frac,
+    FL/example/demo.py:249-265) on a smaller workload of the same kind."""
+    if not os.path.exists(REF_SO):
+        pytest.skip("reference extension not built (python oracle/build_ref.py)")
+    from oracle.build_ref import load_built
+    refext = load_built()
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(3)
+    N, A = 40, 36
+    conc = phantoms.ellipsoid_grains(N, rng)[None]
+    angles = np.linspace(0, 180, A, endpoint=False)
+    param = phantoms.xrf_params(["Fe"], A, 12.0, 1.6e-4)
+    mask = generate_detector_mask(13.309, 13.309, N)
+    solver = CorrectedMLEM(param, angles, mask, (N, N, N), device=dev, feedback="cal_frac")
+    truth = torch.from_numpy(conc).to(dev)
+    solver.recompute_attenuation(truth)
+    I = solver.project(truth).contiguous()
+    C = solver.run(I, n_iter=10, recompute_every=5)
+    Cr = compose.reference_corrected_mlem(refext, param, angles, mask, I,
+                                          torch.ones((1, N, N, N), device=dev), 10, 5,
+                                          feedback="cal_frac")
+    assert rel_err(C.cpu().numpy(), Cr.cpu().numpy()) < TOL_MLEM

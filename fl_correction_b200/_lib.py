@@ -48,6 +48,9 @@ SIGNATURES = {
     "flc_cal_frac_workspace_bytes": (_sz, [_i64, _i64]),
     "flc_cal_frac": (_int, [_vp, _vp, _vp, _vp, _i64, _i64, _int, _f64, _f64, _int, _f64, _vp, _sz,
                             _vp]),
+    "flc_mlem_multi_workspace_bytes": (_sz, [_i64, _vp, _vp, _i64, _i64, _i64]),
+    "flc_mlem_multi": (_int, [_i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _f64,
+                              _f64, _vp, _sz, _vp]),
     "flc_atten_maps_ref": (_int, [_vp] * 8 + [_i64] * 11 + [_int, _int, _i64, _vp, _sz, _vp]),
     "flc_atten_stage": (_int, [_vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _i64,
                                _i64, _i64, _int, _int, _vp]),
@@ -147,3 +150,36 @@ def workspace(nbytes, device):
     buf = torch.empty(n, dtype=torch.uint8, device=device)
     off = (-buf.data_ptr()) % 256
     return buf[off:off + max(int(nbytes), 1)]
+
+
+def ptr_array(tensors):
+    """Host array of the device pointers of `tensors` (for the entry points
+    that take one pointer per problem)."""
+    arr = (ctypes.c_void_p * len(tensors))(*[t.data_ptr() for t in tensors])
+    return ctypes.cast(arr, ctypes.c_void_p), arr
+
+
+def i64_array(values):
+    arr = (ctypes.c_int64 * len(values))(*[int(v) for v in values])
+    return ctypes.cast(arr, ctypes.c_void_p), arr
+
+
+def mlem_multi(Cs, attens, ems, thetas, Is, n_iter, beta, delta, ws=None):
+    """flc_mlem_multi over the problems i: C (R, B, H, W) in place, atten
+    (A, B, H, W), em (A, R), theta (A,), I (A, B, W).  Returns the workspace
+    `ws` (reusable for calls of the same shapes)."""
+    P = len(Cs)
+    R, _, H, W = Cs[0].shape
+    A = [a.shape[0] for a in attens]
+    B = [a.shape[1] for a in attens]
+    pa, ka = i64_array(A)
+    pb, kb = i64_array(B)
+    nb = query("flc_mlem_multi_workspace_bytes", P, pa, pb, R, H, W)
+    if ws is None or ws.numel() < nb:
+        ws = workspace(nb, Cs[0].device)
+    keep = [ptr_array(x) for x in (Cs, attens, ems, thetas, Is)]
+    with torch.cuda.device(Cs[0].device):
+        call("flc_mlem_multi", P, *[k[0] for k in keep], pa, pb, R, H, W, int(n_iter),
+             float(beta), float(delta), ptr(ws), nb, stream())
+    del keep, ka, kb
+    return ws

@@ -778,14 +778,83 @@ constexpr int kT2 = 256;      // threads per CTA of the lean kernels
 constexpr int kFwdU = 8;      // attenuation loads issued together in the forward
 constexpr int kSegU = 8;      // ... and in a backward segment walk
 
+// Partial column sums of one (angle, slice) for the lean kernels: work item =
+// (column w, part p); the thread sums atten(h, w) * sum_r em_r bilerp(C_r)
+// over the part's rows of column w into sp[p][w].  A warp's loads of atten
+// run along w (coalesced); batch j of kFwdU rows is loaded while batch j - 1
+// is computed.  em_a: the angle's R emission values (RC == 1: unused, the
+// caller scales the column sums).
+template <int RC>
+__device__ __forceinline__ void fwd_angle2(const float* __restrict__ at, const float* sC, int img,
+                                           int pitch, const float* __restrict__ em_a, int R,
+                                           const Geo& g, int H, int W, int parts, float* sp) {
+    const int hper = (H + parts - 1) / parts;
+    const int nitems = parts * W;
+    for (int item = threadIdx.x; item < nitems; item += blockDim.x) {
+        const int part = item / W, w = item - part * W;
+        const int h0 = part * hper, n = min(H, h0 + hper) - h0;
+        if (n <= 0) {                      // a part past the last row
+            sp[part * W + w] = 0.f;
+            continue;
+        }
+        const float bx = col_bx(g, w), by = col_by(g, w);
+        const float* ap = at + (int64_t)h0 * W + w;
+        float acc = 0.f;
+        float hf = (float)h0 - g.cy;
+        // rows past the part repeat its last row with weight 0
+        float cur[kFwdU], nxt[kFwdU];
+#pragma unroll
+        for (int k = 0; k < kFwdU; ++k) {
+            cur[k] = __ldg(ap + (int64_t)min(k, n - 1) * W);
+            if (k >= n) cur[k] = 0.f;
+        }
+        for (int j = 0; j < n; j += kFwdU) {
+#pragma unroll
+            for (int k = 0; k < kFwdU; ++k) {
+                const int r = j + kFwdU + k;
+                nxt[k] = __ldg(ap + (int64_t)min(r, n - 1) * W);
+                if (r >= n) nxt[k] = 0.f;
+            }
+#pragma unroll
+            for (int k = 0; k < kFwdU; ++k) {
+                const Smp s = sample_xy(g, fmaf(g.c, hf, bx), fmaf(g.s, hf, by));
+                hf += 1.f;
+                float v;
+                if (RC == 1) {
+                    v = bilerp(sC, pitch, s);
+                } else {
+                    v = 0.f;
+                    for (int r = 0; r < R; ++r)
+                        v = fmaf(__ldg(em_a + r), bilerp(sC + r * img, pitch, s), v);
+                }
+                acc = fmaf(cur[k], v, acc);
+            }
+#pragma unroll
+            for (int k = 0; k < kFwdU; ++k) cur[k] = nxt[k];
+        }
+        sp[part * W + w] = acc;
+    }
+}
+
+// Column sums of the partials (fixed order) -> Pf, or the MLEM ratio
+// I / max(Pf, 1e-6) when I != nullptr (atten_cuda.cpp:326-329).
+__device__ __forceinline__ void fwd_finish(const float* sp, int parts, int W, float scale,
+                                           const float* __restrict__ I, float* __restrict__ out,
+                                           int64_t row) {
+    for (int w = threadIdx.x; w < W; w += blockDim.x) {
+        float s = 0.f;
+        for (int p = 0; p < parts; ++p) s += sp[p * W + w];
+        s *= scale;
+        const int64_t o = row * W + w;
+        if (I) s = I[o] / fmaxf(s, 1e-6f);
+        out[o] = s;
+    }
+}
+
 // Forward: grid (angle groups, B).  The CTA stages slice b of C (R images,
-// row pitch == 3 mod 32) and walks its angles.  Work item = (column w, part
-// p): the thread sums atten(h, w) * sum_r em_r bilerp(C_r) over the part's
-// rows; a warp's loads of atten run along w (coalesced) and kFwdU of them are
-// in flight before their samples are computed.  The parts of a column are
-// added in a fixed order (deterministic); the partial sums are double
-// buffered, so an angle costs one barrier.  I != nullptr: out = I / max(Pf,
-// 1e-6) (the MLEM ratio, atten_cuda.cpp:326-329), else out = Pf.
+// row pitch == 3 mod 32) and walks its angles (fwd_angle2).  The partial sums
+// are double buffered, so an angle costs one barrier.  I != nullptr: out =
+// I / max(Pf, 1e-6) (the MLEM ratio), else out = Pf.
 template <int RC>
 __global__ void __launch_bounds__(kT2, 3)
 proj_fwd2_kernel(const float* __restrict__ atten, const float* __restrict__ C,
@@ -802,67 +871,14 @@ proj_fwd2_kernel(const float* __restrict__ atten, const float* __restrict__ C,
     float* spart = sC + R * img;           // [2][parts][W]
     stage_slice(sC, C, R, B, b, H, W, pitch);
     __syncthreads();
-    const int hper = (H + parts - 1) / parts;
-    const int nitems = parts * W;
     for (int a = a0; a < a1; ++a) {
         const Geo g = make_geo(theta[a], H, W);
-        const float* at = atten + ((int64_t)a * B + b) * H * W;
         float* sp = spart + (a & 1) * parts * W;
-        const float em0 = __ldg(em + (int64_t)a * R);
-        for (int item = threadIdx.x; item < nitems; item += blockDim.x) {
-            const int part = item / W, w = item - part * W;
-            const int h0 = part * hper, n = min(H, h0 + hper) - h0;
-            if (n <= 0) {                      // a part past the last row
-                sp[part * W + w] = 0.f;
-                continue;
-            }
-            const float bx = col_bx(g, w), by = col_by(g, w);
-            const float* ap = at + (int64_t)h0 * W + w;
-            float acc = 0.f;
-            float hf = (float)h0 - g.cy;
-            // batch j of kFwdU rows is loaded while batch j - 1 is computed;
-            // rows past the part repeat its last row with weight 0
-            float cur[kFwdU], nxt[kFwdU];
-#pragma unroll
-            for (int k = 0; k < kFwdU; ++k) {
-                cur[k] = __ldg(ap + (int64_t)min(k, n - 1) * W);
-                if (k >= n) cur[k] = 0.f;
-            }
-            for (int j = 0; j < n; j += kFwdU) {
-#pragma unroll
-                for (int k = 0; k < kFwdU; ++k) {
-                    const int r = j + kFwdU + k;
-                    nxt[k] = __ldg(ap + (int64_t)min(r, n - 1) * W);
-                    if (r >= n) nxt[k] = 0.f;
-                }
-#pragma unroll
-                for (int k = 0; k < kFwdU; ++k) {
-                    const Smp s = sample_xy(g, fmaf(g.c, hf, bx), fmaf(g.s, hf, by));
-                    hf += 1.f;
-                    float v;
-                    if (RC == 1) {
-                        v = bilerp(sC, pitch, s);
-                    } else {
-                        v = 0.f;
-                        for (int r = 0; r < R; ++r)
-                            v = fmaf(__ldg(em + (int64_t)a * R + r), bilerp(sC + r * img, pitch, s), v);
-                    }
-                    acc = fmaf(cur[k], v, acc);
-                }
-#pragma unroll
-                for (int k = 0; k < kFwdU; ++k) cur[k] = nxt[k];
-            }
-            sp[part * W + w] = acc;
-        }
+        fwd_angle2<RC>(atten + ((int64_t)a * B + b) * H * W, sC, img, pitch, em + (int64_t)a * R,
+                       R, g, H, W, parts, sp);
         __syncthreads();
-        for (int w = threadIdx.x; w < W; w += blockDim.x) {
-            float s = 0.f;
-            for (int p = 0; p < parts; ++p) s += sp[p * W + w];
-            if (RC == 1) s *= em0;
-            const int64_t o = ((int64_t)a * B + b) * W + w;
-            if (I) s = I[o] / fmaxf(s, 1e-6f);
-            out[o] = s;
-        }
+        fwd_finish(sp, parts, W, RC == 1 ? __ldg(em + (int64_t)a * R) : 1.f, I, out,
+                   (int64_t)a * B + b);
         // the next angle writes the other partial buffer; the one after it
         // writes this buffer again only past the next barrier
     }
@@ -948,36 +964,23 @@ __device__ __forceinline__ void bwd_segment(const float* __restrict__ at, const 
     }
 }
 
-// Backward with an epilogue: grid (G, B), cluster (G, 1, 1).  CTA g of slice b
-// splats angles [g*apc, (g+1)*apc) into its shared-memory image of the slice
-// in six phases per angle ((w mod 3) x (segment parity), column segments of
-// `seg` samples; see backward_angle_seg); the q weights of the next angle are
-// staged during the last phase.  The cluster then sums its G images over DSMEM
-// in rank order and applies the epilogue:
-//   mode 0: out = sum, or max(sum, clamp_min) when clamp_min > 0;
-//   mode 1: MLEM update out = max(Cin*sum / (sens + beta*huber(Cin)), 0)
-//           (atten_cuda.cpp:331-341), Cin and sens (R,B,H,W) in global memory.
+// Splats angles [a0, a1) of slice b into this CTA's shared-memory image of
+// the slice (zeroed first) in six phases per angle ((w mod 3) x (segment
+// parity), column segments of `seg` samples; see backward_angle_seg), with
+// the clamped samples in the frame buffers, which are folded into the image
+// at the end.  q = ratio * em of each angle is staged during the previous
+// angle's last phase (ratio == nullptr: 1).
 template <int RC>
-__global__ void __launch_bounds__(kT2, 3)
-proj_bwd2_kernel(const float* __restrict__ atten, const float* __restrict__ ratio,
-                 const float* __restrict__ em, const float* __restrict__ theta,
-                 float* __restrict__ out, const float* __restrict__ Cin,
-                 const float* __restrict__ sens, int A, int B, int Rrt, int H, int W, int apc,
-                 int seg, int ncopy, float clamp_min, int mode, float beta, float delta) {
-    extern __shared__ __align__(16) float smem[];
-    cg::cluster_group cluster = cg::this_cluster();
-    const int R = RC > 0 ? RC : Rrt;
-    const int b = blockIdx.y;
-    const int a0 = blockIdx.x * apc, a1 = min(A, a0 + apc);
+__device__ void bwd_splat_angles(const float* __restrict__ atten, const float* __restrict__ ratio,
+                                 const float* __restrict__ em, const float* __restrict__ theta,
+                                 float* sacc, float* sframe, float* sq, int ncopy, int a0, int a1,
+                                 int b, int B, int R, int H, int W, int seg) {
     const int pitch = slice_pitch(W);
     const int img = H * pitch;
-    float* sacc = smem;                                     // [R][H][pitch]
-    float* sframe = sacc + R * img;                         // ncopy x [R][2][W + H]
     float* srow = sframe + ((threadIdx.x >> 5) % ncopy) * 2 * R * (H + W);
     float* scol = srow + 2 * R * W;
-    float* sq = sframe + frame_floats(R, H, W, ncopy);      // [2][R][W]
-    for (int i = threadIdx.x; i < R * img + frame_floats(R, H, W, ncopy); i += blockDim.x)
-        sacc[i] = 0.f;
+    for (int i = threadIdx.x; i < R * img; i += blockDim.x) sacc[i] = 0.f;
+    for (int i = threadIdx.x; i < frame_floats(R, H, W, ncopy); i += blockDim.x) sframe[i] = 0.f;
     if (a0 < a1) stage_q(sq + (a0 & 1) * R * W, ratio, em, a0, b, B, R, W);
     __syncthreads();
     Corners cs;
@@ -1003,27 +1006,158 @@ proj_bwd2_kernel(const float* __restrict__ atten, const float* __restrict__ rati
         }
     }
     fold_frame(cs, sacc, sframe, ncopy, img, pitch, R, H, W);
+}
+
+// Epilogue of a reduced back-projection pixel s of (r, b, h, w):
+//   mode 0: out = s, or max(s, clamp_min) when clamp_min > 0;
+//   mode 1: MLEM update out = max(Cin*s / (sens + beta*huber(Cin)), 0)
+//           (atten_cuda.cpp:331-341), Cin and sens (R,B,H,W) in global memory.
+__device__ __forceinline__ void bwd_epilogue(int mode, float* __restrict__ out,
+                                             const float* __restrict__ Cin,
+                                             const float* __restrict__ sens, float clamp_min,
+                                             float beta, float delta, int r, int b, int B, int H,
+                                             int W, int h, int w, float s) {
+    const int64_t gi = (((int64_t)r * B + b) * H + h) * W + w;
+    if (mode == 0) {
+        out[gi] = clamp_min > 0.f ? fmaxf(s, clamp_min) : s;
+        return;
+    }
+    const float* ci = Cin + ((int64_t)r * B + b) * H * W;
+    const float cp = ci[h * W + w];
+    float den = sens[gi];
+    if (beta > 0.f) {
+        float hg = 0.f;
+        if (h > 0) { float d = cp - ci[(h - 1) * W + w]; hg += fabsf(d) <= delta ? d : copysignf(delta, d); }
+        if (h + 1 < H) { float d = cp - ci[(h + 1) * W + w]; hg += fabsf(d) <= delta ? d : copysignf(delta, d); }
+        if (w > 0) { float d = cp - ci[h * W + w - 1]; hg += fabsf(d) <= delta ? d : copysignf(delta, d); }
+        if (w + 1 < W) { float d = cp - ci[h * W + w + 1]; hg += fabsf(d) <= delta ? d : copysignf(delta, d); }
+        den = __fadd_rn(den, __fmul_rn(beta, hg));
+    }
+    out[gi] = fmaxf(__fmul_rn(cp, s) / den, 0.f);
+}
+
+// Backward with an epilogue: grid (G, B), cluster (G, 1, 1).  CTA g of slice b
+// splats angles [g*apc, (g+1)*apc) (bwd_splat_angles); the cluster then sums
+// its G images over DSMEM in rank order and applies bwd_epilogue.
+template <int RC>
+__global__ void __launch_bounds__(kT2, 3)
+proj_bwd2_kernel(const float* __restrict__ atten, const float* __restrict__ ratio,
+                 const float* __restrict__ em, const float* __restrict__ theta,
+                 float* __restrict__ out, const float* __restrict__ Cin,
+                 const float* __restrict__ sens, int A, int B, int Rrt, int H, int W, int apc,
+                 int seg, int ncopy, float clamp_min, int mode, float beta, float delta) {
+    extern __shared__ __align__(16) float smem[];
+    cg::cluster_group cluster = cg::this_cluster();
+    const int R = RC > 0 ? RC : Rrt;
+    const int b = blockIdx.y;
+    const int a0 = blockIdx.x * apc, a1 = min(A, a0 + apc);
+    const int pitch = slice_pitch(W);
+    float* sacc = smem;                                     // [R][H][pitch]
+    float* sframe = sacc + R * H * pitch;                   // ncopy x [R][2][W + H]
+    float* sq = sframe + frame_floats(R, H, W, ncopy);      // [2][R][W]
+    bwd_splat_angles<RC>(atten, ratio, em, theta, sacc, sframe, sq, ncopy, a0, a1, b, B, R, H, W,
+                         seg);
     cluster.sync();
     cluster_reduce(cluster, sacc, R, H, W, pitch, [&](int r, int h, int w, float s) {
-        const int64_t gi = (((int64_t)r * B + b) * H + h) * W + w;
-        if (mode == 0) {
-            out[gi] = clamp_min > 0.f ? fmaxf(s, clamp_min) : s;
-            return;
-        }
-        const float* ci = Cin + ((int64_t)r * B + b) * H * W;
-        const float cp = ci[h * W + w];
-        float den = sens[gi];
-        if (beta > 0.f) {
-            float hg = 0.f;
-            if (h > 0) { float d = cp - ci[(h - 1) * W + w]; hg += fabsf(d) <= delta ? d : copysignf(delta, d); }
-            if (h + 1 < H) { float d = cp - ci[(h + 1) * W + w]; hg += fabsf(d) <= delta ? d : copysignf(delta, d); }
-            if (w > 0) { float d = cp - ci[h * W + w - 1]; hg += fabsf(d) <= delta ? d : copysignf(delta, d); }
-            if (w + 1 < W) { float d = cp - ci[h * W + w + 1]; hg += fabsf(d) <= delta ? d : copysignf(delta, d); }
-            den = __fadd_rn(den, __fmul_rn(beta, hg));
-        }
-        out[gi] = fmaxf(__fmul_rn(cp, s) / den, 0.f);
+        bwd_epilogue(mode, out, Cin, sens, clamp_min, beta, delta, r, b, B, H, W, h, w, s);
     });
     cluster.sync();
+}
+
+// ---------------------------------------------------------------------------
+// Persistent MLEM over several problems (a problem: one element's -- or one
+// volume's -- C, atten, em, theta, I; all with the same R, H, W).  Work item =
+// (problem, slice); the clusters of G CTAs take items from a device counter
+// (largest angle counts first, as the host orders the problems) until none
+// is left.  Per item, CTA g of the cluster takes the angles [g*apc, ...):
+//   mode 0 (iteration): the forward of its angles with the slice of Cin in
+//     shared memory, the ratio I / max(Pf, 1e-6) written to the problem's
+//     ratio buffer; then the backward of the same angles (the image region is
+//     reused as the accumulator), the cluster reduction and the update into
+//     Cout (bwd_epilogue mode 1);
+//   mode 1 (sensitivity): the backward of ratio = 1, max(P^T 1, 1e-6) into sens.
+// One launch thus covers an MLEM iteration of every problem, so that small
+// problems fill the GPU beside large ones and no launch leaves a tail per
+// problem.
+// ---------------------------------------------------------------------------
+constexpr int kMaxProbs = 32;
+
+struct MlemProb {
+    const float* atten;
+    const float* em;
+    const float* theta;
+    const float* I;
+    float* sens;
+    const float* Cin;
+    float* Cout;
+    float* ratio;
+    int A, B;
+};
+
+struct MlemQueue {
+    MlemProb p[kMaxProbs];
+    int start[kMaxProbs + 1];   // item offsets: problem i owns items [start[i], start[i+1])
+    int n_prob;
+};
+
+template <int RC>
+__global__ void __launch_bounds__(kT2, 3)
+mlem_queue_kernel(const MlemQueue* __restrict__ queue, int* __restrict__ counter, int Rrt, int H,
+                  int W, int seg, int ncopy, int parts, int mode, float beta, float delta) {
+    extern __shared__ __align__(16) float smem[];
+    __shared__ int s_item;
+    cg::cluster_group cluster = cg::this_cluster();
+    const int R = RC > 0 ? RC : Rrt;
+    const int G = (int)cluster.num_blocks();
+    const int rank = (int)cluster.block_rank();
+    const int pitch = slice_pitch(W);
+    const int img = H * pitch;
+    float* simg = smem;                                     // C (forward) / accumulator
+    float* sframe = simg + R * img;                         // frames; partial sums (forward)
+    float* sq = sframe + frame_floats(R, H, W, ncopy);      // [2][R][W]
+    const int n_items = queue->start[queue->n_prob];
+    for (;;) {
+        if (rank == 0 && threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+        cluster.sync();
+        const int item = *cluster.map_shared_rank(&s_item, 0);
+        cluster.sync();   // every CTA has read the item before rank 0 takes the next
+        if (item >= n_items) break;
+        int pi = 0;
+        while (queue->start[pi + 1] <= item) ++pi;
+        const MlemProb P = queue->p[pi];
+        const int b = item - queue->start[pi];
+        const int apc = (P.A + G - 1) / G;
+        const int a0 = rank * apc, a1 = min(P.A, a0 + apc);
+        if (mode == 0) {
+            stage_slice(simg, P.Cin, R, P.B, b, H, W, pitch);
+            __syncthreads();
+            for (int a = a0; a < a1; ++a) {
+                const Geo g = make_geo(P.theta[a], H, W);
+                float* sp = sframe + (a & 1) * parts * W;
+                fwd_angle2<RC>(P.atten + ((int64_t)a * P.B + b) * H * W, simg, img, pitch,
+                               P.em + (int64_t)a * R, R, g, H, W, parts, sp);
+                __syncthreads();
+                fwd_finish(sp, parts, W, RC == 1 ? __ldg(P.em + (int64_t)a * R) : 1.f, P.I,
+                           P.ratio, (int64_t)a * P.B + b);
+            }
+            __syncthreads();   // the image and partials are reused below
+        }
+        bwd_splat_angles<RC>(P.atten, mode == 0 ? P.ratio : nullptr, P.em, P.theta, simg, sframe,
+                             sq, ncopy, a0, a1, b, P.B, R, H, W, seg);
+        cluster.sync();
+        cluster_reduce(cluster, simg, R, H, W, pitch, [&](int r, int h, int w, float s) {
+            if (mode == 0)
+                bwd_epilogue(1, P.Cout, P.Cin, P.sens, 0.f, beta, delta, r, b, P.B, H, W, h, w, s);
+            else
+                bwd_epilogue(0, P.sens, nullptr, nullptr, 1e-6f, 0.f, 0.f, r, b, P.B, H, W, h, w, s);
+        });
+        cluster.sync();   // remote images read before the next item overwrites them
+    }
+}
+
+// Copies the problem table (passed by value: no host copy, capture-safe).
+__global__ void mlem_queue_init_kernel(MlemQueue q, MlemQueue* __restrict__ dst) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) *dst = q;
 }
 
 // Backward for slices whose image does not fit in shared memory: one thread
@@ -1487,6 +1621,164 @@ extern "C" int flc_bwd_emission(const float* atten, const float* ratio, const fl
     FLC_REQUIRE(atten && ratio && em && theta && out, "flc_bwd_emission: null pointer argument");
     FLC_TRY(check_proj_sizes(A, B, R, H, W));
     return bwd_emission_launch(atten, ratio, em, theta, out, A, B, R, H, W, 0.f, as_stream(stream));
+}
+
+// ---------------------------------------------------------------------------
+// flc_mlem_multi: MLEM of P problems of the same R, H, W with the persistent
+// queue kernel -- one launch per iteration for all of them.
+// ---------------------------------------------------------------------------
+namespace flc {
+namespace {
+
+size_t al256(size_t n) { return (n + 255) & ~(size_t)255; }
+
+size_t multi_frame_floats(int64_t R, int64_t H, int64_t W, int ncopy) {
+    const size_t f = (size_t)frame_floats((int)R, (int)H, (int)W, ncopy);
+    const size_t pt = (size_t)2 * fwd2_parts(H, W) * W;   // forward partials share the region
+    return f > pt ? f : pt;
+}
+
+size_t multi_smem(int64_t R, int64_t H, int64_t W, int ncopy) {
+    return sizeof(float) * ((size_t)R * H * slice_pitch((int)W) + multi_frame_floats(R, H, W, ncopy) +
+                            2 * (size_t)R * W);
+}
+
+size_t multi_layout(int64_t P, const int64_t* A, const int64_t* B, int64_t R, int64_t H, int64_t W,
+                    size_t* prob_off) {
+    size_t off = 2 * al256(sizeof(MlemQueue)) + 256;   // two tables, the counter
+    for (int64_t i = 0; i < P; ++i) {
+        if (prob_off) prob_off[i] = off;
+        const size_t nC = al256(sizeof(float) * (size_t)(R * B[i] * H * W));
+        off += 2 * nC + al256(sizeof(float) * (size_t)(A[i] * B[i] * W));
+    }
+    return off;
+}
+
+}  // namespace
+}  // namespace flc
+
+extern "C" size_t flc_mlem_multi_workspace_bytes(int64_t P, const int64_t* A, const int64_t* B,
+                                                 int64_t R, int64_t H, int64_t W) {
+    if (P < 1 || P > kMaxProbs || !A || !B || R < 1 || H < 1 || W < 1) return 0;
+    for (int64_t i = 0; i < P; ++i)
+        if (A[i] < 1 || B[i] < 1) return 0;
+    return multi_layout(P, A, B, R, H, W, nullptr);
+}
+
+extern "C" int flc_mlem_multi(int64_t P, float* const* C, const float* const* atten,
+                              const float* const* em, const float* const* theta,
+                              const float* const* I, const int64_t* A, const int64_t* B, int64_t R,
+                              int64_t H, int64_t W, int64_t n_iter, double beta, double delta,
+                              void* workspace, size_t workspace_bytes, void* stream) {
+    clear_error();
+    FLC_REQUIRE(P >= 1 && P <= kMaxProbs, "flc_mlem_multi: 1 <= P <= %d problems", kMaxProbs);
+    FLC_REQUIRE(C && atten && em && theta && I && A && B && workspace,
+                "flc_mlem_multi: null pointer argument");
+    int64_t items = 0;
+    for (int64_t i = 0; i < P; ++i) {
+        FLC_REQUIRE(C[i] && atten[i] && em[i] && theta[i] && I[i],
+                    "flc_mlem_multi: null pointer for problem %lld", (long long)i);
+        FLC_TRY(check_proj_sizes(A[i], B[i], R, H, W));
+        items += B[i];
+    }
+    FLC_REQUIRE(n_iter >= 0 && items < (1LL << 30), "flc_mlem_multi: invalid sizes");
+    if (((uintptr_t)workspace & 255) != 0) {
+        set_error("flc_mlem_multi: workspace must be 256-byte aligned");
+        return FLC_ERR_ALIGNMENT;
+    }
+    size_t prob_off[kMaxProbs];
+    const size_t need = multi_layout(P, A, B, R, H, W, prob_off);
+    if (workspace_bytes < need) {
+        set_error("flc_mlem_multi: workspace of %zu bytes is smaller than the %zu required",
+                  workspace_bytes, need);
+        return FLC_ERR_WORKSPACE;
+    }
+    const int ncopy_base = 1;
+    if (multi_smem(R, H, W, ncopy_base) > (size_t)max_smem_optin()) {
+        set_error("flc_mlem_multi: a %lld x %lld slice does not fit in shared memory",
+                  (long long)H, (long long)W);
+        return FLC_ERR_UNSUPPORTED;
+    }
+    cudaStream_t st = as_stream(stream);
+    char* ws = (char*)workspace;
+    MlemQueue* q_even = (MlemQueue*)ws;
+    MlemQueue* q_odd = (MlemQueue*)(ws + al256(sizeof(MlemQueue)));
+    int* counter = (int*)(ws + 2 * al256(sizeof(MlemQueue)));
+    // problems in decreasing angle count: the long items are taken first
+    int order[kMaxProbs];
+    for (int i = 0; i < P; ++i) order[i] = i;
+    for (int i = 1; i < P; ++i)
+        for (int j = i; j > 0 && A[order[j]] > A[order[j - 1]]; --j) std::swap(order[j], order[j - 1]);
+    MlemQueue te = {}, to = {};
+    te.n_prob = to.n_prob = (int)P;
+    int64_t amax = 1;
+    for (int k = 0; k < P; ++k) {
+        const int i = order[k];
+        char* base = ws + prob_off[i];
+        const size_t nC = al256(sizeof(float) * (size_t)(R * B[i] * H * W));
+        float* sens = (float*)base;
+        float* alt = (float*)(base + nC);
+        float* ratio = (float*)(base + 2 * nC);
+        te.p[k] = MlemProb{atten[i], em[i], theta[i], I[i], sens, C[i], alt, ratio, (int)A[i], (int)B[i]};
+        to.p[k] = MlemProb{atten[i], em[i], theta[i], I[i], sens, alt, C[i], ratio, (int)A[i], (int)B[i]};
+        te.start[k + 1] = to.start[k + 1] = te.start[k] + (int)B[i];
+        amax = A[i] > amax ? A[i] : amax;
+    }
+    mlem_queue_init_kernel<<<1, 32, 0, st>>>(te, q_even);
+    FLC_TRY(check_launch("mlem_queue_init_kernel"));
+    mlem_queue_init_kernel<<<1, 32, 0, st>>>(to, q_odd);
+    FLC_TRY(check_launch("mlem_queue_init_kernel"));
+    // launch shape: frame copies that keep the CTAs per SM, cluster size by
+    // waves x (angles per CTA + 2) over the items, persistent grid
+    int per_sm = 3;
+    while (per_sm > 1 && multi_smem(R, H, W, 1) > smem_budget(per_sm)) --per_sm;
+    int ncopy = kMaxFrameCopies;
+    while (ncopy > 1 && multi_smem(R, H, W, ncopy) > smem_budget(per_sm)) ncopy /= 2;
+    const size_t smem = multi_smem(R, H, W, ncopy);
+    const void* fn = R == 1 ? (const void*)mlem_queue_kernel<1> : (const void*)mlem_queue_kernel<0>;
+    int bestG = 1, nclu = 1;
+    int64_t best = -1;
+    const int gmax = (int)(amax < kMaxCluster ? amax : kMaxCluster);
+    if (int64_t t = tune(kTuneProjCluster)) {
+        bestG = (int)(t < gmax ? t : gmax);
+        nclu = active_clusters(fn, bestG, smem, kT2);
+    } else {
+        for (int G = 1; G <= gmax; ++G) {
+            const int n = active_clusters(fn, G, smem, kT2);
+            if (n < 1) continue;
+            const int64_t cost = ceil_div(items, n) * (ceil_div(amax, G) + 2);
+            if (best < 0 || cost < best) {
+                best = cost;
+                bestG = G;
+                nclu = n;
+            }
+        }
+    }
+    if (nclu < 1) {
+        set_error("flc_mlem_multi: the queue kernel cannot be made resident");
+        return FLC_ERR_UNSUPPORTED;
+    }
+    if (nclu > items) nclu = (int)items;
+    const int seg = seg2_length(H, W), parts = fwd2_parts(H, W);
+    int iR = (int)R, iH = (int)H, iW = (int)W;
+    float fb = (float)beta, fd = (float)delta;
+    auto launch = [&](const MlemQueue* q, int mode) -> int {
+        FLC_TRY_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), st));
+        void* args[] = {(void*)&q, (void*)&counter, &iR, &iH, &iW, (void*)&seg, &ncopy,
+                        (void*)&parts, &mode, &fb, &fd};
+        return launch_cluster(fn, dim3((unsigned)(nclu * bestG)), bestG, smem, st, args, kT2);
+    };
+    FLC_TRY(launch(q_even, 1));                       // sensitivities
+    for (int64_t it = 0; it < n_iter; ++it) FLC_TRY(launch((it & 1) ? q_odd : q_even, 0));
+    if (n_iter & 1) {
+        for (int64_t i = 0; i < P; ++i) {
+            const size_t nC = al256(sizeof(float) * (size_t)(R * B[i] * H * W));
+            FLC_TRY_CUDA(cudaMemcpyAsync(C[i], ws + prob_off[i] + nC,
+                                         sizeof(float) * (size_t)(R * B[i] * H * W),
+                                         cudaMemcpyDeviceToDevice, st));
+        }
+    }
+    return FLC_OK;
 }
 
 extern "C" int flc_huber_grad(const float* C, float* grad, int64_t RB, int64_t H, int64_t W,

@@ -45,8 +45,12 @@ class CorrectedMLEM:
 
     def __init__(self, param, angles_deg, mask, shape, fixed_frac=None, incident="own",
                  beta=0.0, delta=0.01, device="cuda", chunk=0, bound_frac=True,
-                 feedback="bounded", cal_frac_args=None):
+                 feedback="bounded", cal_frac_args=None, multi=False):
         self.device = torch.device(device)
+        # multi: the MLEM iterations of all elements in one persistent launch
+        # each (flc_mlem_multi) instead of one flc_mlem call per element
+        self.multi = multi
+        self._ws_multi = None
         self.bound_frac = bound_frac
         if feedback not in ("bounded", "cal_frac"):
             raise ValueError("feedback must be 'bounded' or 'cal_frac'")
@@ -118,6 +122,18 @@ class CorrectedMLEM:
         (L, S, H, W) is updated in place.  mlem_events: optional list receiving
         (start, end) CUDA events around each element's iterations."""
         S, H, W = self.shape
+        if self.multi and use_graph == 0:
+            if mlem_events is not None:
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+            self._ws_multi = _lib.mlem_multi(
+                [C[l:l + 1] for l in range(self.L)], [self.atten[l] for l in range(self.L)],
+                [self.em[l] for l in range(self.L)], [self.theta] * self.L,
+                [I[l] for l in range(self.L)], n_iter, self.beta, self.delta, self._ws_multi)
+            if mlem_events is not None:
+                e1.record()
+                mlem_events.append((e0, e1, int(n_iter) * self.L))
+            return C
         with torch.cuda.device(self.device):
             for l in range(self.L):
                 if mlem_events is not None:

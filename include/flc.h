@@ -161,6 +161,27 @@ FLC_API int flc_mlem_static(float* C, const float* atten, const float* em, const
                     const float* I, int64_t n_iter, double beta, double delta,
                     int64_t A, int64_t B, int64_t R, int64_t H, int64_t W, void* stream);
 
+/* MLEM of P independent problems at once (P <= 32; for instance the elements
+ * of one volume, or several volumes of one slice size): problem i has C[i]
+ * (R, B[i], H, W), atten[i] (A[i], B[i], H, W), em[i] (A[i], R), theta[i]
+ * (A[i]) and I[i] (A[i], B[i], W), all device pointers held in host arrays
+ * of length P; R, H, W are shared.  Each C[i] is updated in place by n_iter
+ * iterations of flc_mlem.  One persistent launch per iteration covers every
+ * problem: clusters of CTAs take (problem, slice) items from a device
+ * counter, largest angle counts first, and for each item run the forward of
+ * their angles, the backward of the same angles and the update.  Workspace:
+ * flc_mlem_multi_workspace_bytes (256-byte aligned).  Issues no host copies
+ * (the problem table travels as a kernel argument).  No counterpart in the
+ * reference, which runs mlem_cuda_batch once per element
+ * (FL/torch_recon.py:50-99, FL/example/demo.py:177-232). */
+FLC_API size_t flc_mlem_multi_workspace_bytes(int64_t P, const int64_t* A, const int64_t* B,
+                                              int64_t R, int64_t H, int64_t W);
+FLC_API int flc_mlem_multi(int64_t P, float* const* C, const float* const* atten,
+                           const float* const* em, const float* const* theta,
+                           const float* const* I, const int64_t* A, const int64_t* B, int64_t R,
+                           int64_t H, int64_t W, int64_t n_iter, double beta, double delta,
+                           void* workspace, size_t workspace_bytes, void* stream);
+
 /* ---------------------------------------------------------------------
  * Per-angle attenuation maps (rotation + mu assembly + incident scan +
  * fluorescence cone + product), the path of FL.core.cal_xrf_atten_at_angles,

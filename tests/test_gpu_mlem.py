@@ -90,3 +90,45 @@ def test_huber_api():
     g = torch.empty((2, 3, 17, 19), device="cuda")
     AC.huber_grad_batch(T(C), g, 0.05)
     assert rel_err(g.cpu().numpy(), O.huber_grad(C, 0.05)) < 1e-6
+
+
+@pytest.mark.parametrize("shapes,beta", [([(12, 4, 32), (30, 3, 32), (7, 5, 32)], 1e-3),
+                                         ([(24, 16, 64), (24, 16, 64), (24, 16, 64)], 0.0),
+                                         ([(9, 2, 20)], 1e-3)])
+def test_mlem_multi_matches_per_problem(shapes, beta):
+    """flc_mlem_multi (one persistent launch per iteration for all problems)
+    against flc_mlem per problem and the oracle."""
+    rng = np.random.default_rng(len(shapes) + int(beta * 1e3))
+    Cs, ats, ems, ths, Is, refs = [], [], [], [], [], []
+    for (A, B, N) in shapes:
+        atten, C, em, th, I = _problem(rng, A, B, 1, N, N)
+        Cs.append(T(np.ones_like(C)))
+        ats.append(T(atten)); ems.append(T(em)); ths.append(T(th)); Is.append(T(I))
+        refs.append(O.mlem(np.ones_like(C), atten, em, th, I, 7, beta, 0.01))
+    singles = [AC.mlem_cuda_batch(c.clone(), a, e, t, i, 7, beta, 0.01)
+               for c, a, e, t, i in zip(Cs, ats, ems, ths, Is)]
+    _lib.mlem_multi(Cs, ats, ems, ths, Is, 7, beta, 0.01)
+    for c, s1, ref in zip(Cs, singles, refs):
+        assert rel_err(c.cpu().numpy(), s1.cpu().numpy()) < 1e-5
+        assert rel_err(c.cpu().numpy(), ref) < TOL_MLEM
+
+
+def test_corrected_mlem_multi_equals_per_element():
+    from fl_correction_b200 import phantoms
+    from fl_correction_b200.detector_mask import generate_detector_mask
+    from fl_correction_b200.recon import CorrectedMLEM
+    rng = np.random.default_rng(8)
+    N, A = 32, 24
+    conc = phantoms.voronoi_grains(N, rng, 2, n_seeds=12)
+    conc = (conc * 0.4).astype(np.float32)
+    angles = np.linspace(0, 180, A, endpoint=False)
+    param = phantoms.xrf_params(["Fe", "Ni"], A, 14.0, 4e-4)
+    mask = generate_detector_mask(13.309, 13.309, N)
+    outs = []
+    for multi in (False, True):
+        s = CorrectedMLEM(param, angles, mask, (N, N, N), multi=multi)
+        truth = torch.from_numpy(conc).cuda()
+        s.recompute_attenuation(truth)
+        I = s.project(truth).contiguous()
+        outs.append(s.run(I, n_iter=6, recompute_every=3).cpu().numpy())
+    assert rel_err(outs[1], outs[0]) < 1e-5

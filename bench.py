@@ -53,8 +53,11 @@ def parse():
                    help="skip timing the reference's own CUDA kernels on this GPU")
     p.add_argument("--adam-steps", type=int, default=0,
                    help="configurations 2/4: Adam steps timed (default 200 / 3)")
-    p.add_argument("--case", default=None, choices=["cone", "cone_direct", "mlem", "fwd", "bwd", "stage"],
+    p.add_argument("--case", default=None, choices=["cone", "cone_direct", "mlem", "fwd", "bwd", "stage",
+                                                    "mlem_multi"],
                    help="run one kernel on a profiling-sized case instead of the benchmark")
+    p.add_argument("--case-slices", type=int, default=16,
+                   help="slices of 128^2 in the projector / MLEM cases (128: the benchmark's shape)")
     return p.parse_args()
 
 
@@ -830,6 +833,19 @@ def run_case(args):
             _lib.call("flc_cone_atten_apply_ws", _lib.ptr(mu), _lib.ptr(u), _lib.ptr(v),
                       _lib.ptr(atten), n_a, L, N, N, N, A, 0, *mask.shape, _lib.ptr(ws), nb,
                       _lib.stream())
+    elif args.case == "mlem_multi":
+        # one persistent MLEM iteration over 3 elements (the benchmark's MLEM shape
+        # with --case-slices 128)
+        A, B = 120, args.case_slices
+        ats = [torch.rand((A, B, N, N), device=dev, generator=g) for _ in range(3)]
+        em = torch.full((A, 1), 0.02, device=dev)
+        th = torch.linspace(0, math.pi, A + 1, device=dev)[:-1].contiguous()
+        Cs = [torch.ones((1, B, N, N), device=dev) for _ in range(3)]
+        Is = [AC.forward_emission_batch(a, c * 0.7, em, th) for a, c in zip(ats, Cs)]
+        box = {}
+        def once():
+            box["ws"] = _lib.mlem_multi(Cs, ats, [em] * 3, [th] * 3, Is, 1, 0.0, 0.01,
+                                        box.get("ws"))
     elif args.case == "mlem":
         A, B = 24, 16
         atten = torch.rand((A, B, N, N), device=dev, generator=g)
@@ -855,7 +871,7 @@ def run_case(args):
                       _lib.ptr(cf), _lib.ptr(atten), _lib.ptr(ws), n_ch, N, N, N, A, L, 0, n_a,
                       0, 1, _lib.ptr(ws4), nb, _lib.stream())
     elif args.case in ("fwd", "bwd"):
-        A, B = 120, 16
+        A, B = 120, args.case_slices
         atten = torch.rand((A, B, N, N), device=dev, generator=g)
         em = torch.full((A, 1), 0.02, device=dev)
         th = torch.linspace(0, math.pi, A + 1, device=dev)[:-1].contiguous()

@@ -66,6 +66,7 @@ SIGNATURES = {
     "flc_xrf_project_adjoint": (_int, [_vp] * 11 + [_i64] * 9 + [_int, _i64, _vp, _sz, _vp]),
     "flc_rotate": (_int, [_vp, _vp, _i64, _i64, _i64, _f32, _f32, _vp]),
     "flc_incident_scan": (_int, [_vp, _vp, _i64, _i64, _i64, _vp]),
+    "flc_rotate_ex": (_int, [_vp, _vp, _i64, _i64, _i64, _f32, _f32, _int, _vp]),
 }
 
 _LIB = None

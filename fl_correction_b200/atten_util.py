@@ -43,23 +43,21 @@ def extract_em_cs_elem(param, elem, use_ref=False):
 
 def update_dict_use_ref_at_angle(dict_use_ref, current_angle):
     """Copy of dict_use_ref with every reference volume of 'ref_3D' rotated by
-    current_angle degrees (FL/atten_util.py:79-88).  The reference rotates with
-    scipy's ndimage.rotate (order 1, FL/image_util.py:165-203); here the
-    native grid_sample rotation runs (the fractions' rotation, which equals
-    it to ~1e-6 inside the volume).  numpy in, float32 numpy out, as rot3D
-    returns; a cuda tensor stays on its device."""
+    current_angle degrees (FL/atten_util.py:79-88), as the reference's rot3D
+    does (scipy.ndimage.rotate, order 1, zero outside the slice;
+    torch_image_util.rot3D_scipy on the device).  numpy in, float32 numpy
+    out, as rot3D returns; a cuda tensor stays on its device."""
     d = deepcopy(dict_use_ref)
     if len(d) > 0 and d.get("use_ref", False):
-        from .torch_image_util import torch_rotate_image_nd
-        th = float(current_angle) / 180.0 * np.pi
+        from .torch_image_util import rot3D_scipy
         refs = d["ref_3D"]
         for i in range(len(refs)):
             r = refs[i]
             if isinstance(r, torch.Tensor):
-                refs[i] = torch_rotate_image_nd(r.to(torch.float32), th)
+                refs[i] = rot3D_scipy(r, current_angle)
             else:
-                t = torch.tensor(np.nan_to_num(np.asarray(r, np.float32)), device="cuda")
-                refs[i] = torch_rotate_image_nd(t, th).cpu().numpy()
+                t = torch.tensor(np.asarray(r, np.float32), device="cuda")
+                refs[i] = rot3D_scipy(t, current_angle).cpu().numpy()
     return d
 
 

@@ -35,13 +35,14 @@ namespace {
 // RotGeom / rot_sample live in flc_geom.cuh, shared with the adjoint kernels.
 
 __global__ void rotate_kernel(const float* __restrict__ x, float* __restrict__ out, int64_t N,
-                              int H, int W, RotGeom g) {
+                              int H, int W, RotGeom g, int scipy_mode) {
     int w = blockIdx.x * blockDim.x + threadIdx.x;
     int h = blockIdx.y;
     if (w >= W) return;
     for (int64_t n = blockIdx.z; n < N; n += gridDim.z) {
         const float* img = x + n * H * W;
-        out[(n * H + h) * W + w] = rot_sample(img, H, W, g, h, w);
+        out[(n * H + h) * W + w] = scipy_mode ? rot_sample_scipy(img, H, W, g, h, w)
+                                              : rot_sample(img, H, W, g, h, w);
     }
 }
 
@@ -117,7 +118,8 @@ __global__ void frac_interleave_kernel(const float* __restrict__ frac, float4* _
 // once: the same taps, weights and operations per channel.
 template <int G>
 __device__ __forceinline__ void rot_sample_all(const float4* __restrict__ img, int H, int W,
-                                               const RotGeom& g, int h, int w, float (&fr)[kMaxCh]) {
+                                               const RotGeom& g, int h, int w, float (&fr)[kMaxCh],
+                                               int scipy_from = kMaxCh) {
     const RotTap t = rot_tap(g, h, w);
     const int x0 = t.x0, y0 = t.y0;
     const bool xin0 = x0 >= 0 && x0 < W, xin1 = x0 + 1 >= 0 && x0 + 1 < W;
@@ -140,6 +142,12 @@ __device__ __forceinline__ void rot_sample_all(const float4* __restrict__ img, i
     }
 #pragma unroll
     for (int j = 4 * G; j < kMaxCh; ++j) fr[j] = 0.f;
+    // channels from scipy_from on take the reference's scipy rotation rule
+    if (!t.inside) {
+#pragma unroll
+        for (int j = 0; j < kMaxCh; ++j)
+            if (j >= scipy_from) fr[j] = 0.f;
+    }
 }
 
 // LM: lines held in registers (>= L).  G > 0: the rotation reads the
@@ -189,12 +197,15 @@ __global__ void atten_stage_kernel(const float* __restrict__ frac, const float4*
             if (r >= n) break;
             const int h = H - 1 - (y0 + r);
             float fr[kMaxCh];
+            // the reference volumes rotate as the reference's rot3D does
+            // (FL/atten_util.py:79-88): scipy's boundary rule
             if constexpr (G > 0) {
-                rot_sample_all<G>(frac4 + (int64_t)s * HW * G, H, W, g, h, w, fr);
+                rot_sample_all<G>(frac4 + (int64_t)s * HW * G, H, W, g, h, w, fr, n_ch);
             } else {
 #pragma unroll
                 for (int j = 0; j < kMaxCh; ++j)
-                    fr[j] = j < n_tot ? rot_sample(frac + ((int64_t)j * S + s) * HW, H, W, g, h, w)
+                    fr[j] = j < n_ch ? rot_sample(frac + ((int64_t)j * S + s) * HW, H, W, g, h, w)
+                          : j < n_tot ? rot_sample_scipy(frac + ((int64_t)j * S + s) * HW, H, W, g, h, w)
                                       : 0.f;
             }
             // the reference-spectrum coefficient of channel ref.ch at this voxel
@@ -588,10 +599,10 @@ bool factor_mask(const std::vector<float>& m, int64_t Mz, int64_t Mx, int64_t My
 }  // namespace
 
 int rotate_launch(const float* x, float* out, int64_t N, int64_t H, int64_t W, float c, float s,
-                  cudaStream_t st) {
+                  cudaStream_t st, int scipy_mode = 0) {
     RotGeom g = rot_geom(c, s, (int)H, (int)W);
     dim3 grid((unsigned)ceil_div(W, 128), (unsigned)H, (unsigned)(N < 65535 ? N : 65535));
-    rotate_kernel<<<grid, 128, 0, st>>>(x, out, N, (int)H, (int)W, g);
+    rotate_kernel<<<grid, 128, 0, st>>>(x, out, N, (int)H, (int)W, g, scipy_mode);
     return check_launch("rotate_kernel");
 }
 
@@ -714,6 +725,15 @@ extern "C" int flc_rotate(const float* x, float* out, int64_t N, int64_t H, int6
     FLC_REQUIRE(x && out, "flc_rotate: null pointer argument");
     FLC_REQUIRE(N >= 1 && H >= 1 && W >= 1, "flc_rotate: sizes must be positive");
     return rotate_launch(x, out, N, H, W, cos_t, sin_t, as_stream(stream));
+}
+
+extern "C" int flc_rotate_ex(const float* x, float* out, int64_t N, int64_t H, int64_t W,
+                             float cos_t, float sin_t, int mode, void* stream) {
+    clear_error();
+    FLC_REQUIRE(x && out, "flc_rotate_ex: null pointer argument");
+    FLC_REQUIRE(N >= 1 && H >= 1 && W >= 1, "flc_rotate_ex: sizes must be positive");
+    FLC_REQUIRE(mode == 0 || mode == 1, "flc_rotate_ex: mode must be 0 or 1");
+    return rotate_launch(x, out, N, H, W, cos_t, sin_t, as_stream(stream), mode);
 }
 
 extern "C" int flc_incident_scan(const float* mu, float* out, int64_t N, int64_t H, int64_t W,

@@ -102,6 +102,7 @@ __host__ __device__ inline RotGeom rot_geom(float c, float s, int H, int W) {
 struct RotTap {
     int x0, y0;
     float tx, ty;
+    bool inside;   // the sample point lies in [0, W-1] x [0, H-1]
 };
 
 __device__ __forceinline__ RotTap rot_tap(const RotGeom& g, int h, int w) {
@@ -114,6 +115,7 @@ __device__ __forceinline__ RotTap rot_tap(const RotGeom& g, int h, int w) {
     t.y0 = (int)fy;
     t.tx = ix - fx;
     t.ty = iy - fy;
+    t.inside = ix >= 0.f && ix <= 2.f * g.cx && iy >= 0.f && iy <= 2.f * g.cy;
     return t;
 }
 
@@ -134,6 +136,16 @@ __device__ __forceinline__ float rot_sample_tap(const float* __restrict__ img, i
 __device__ __forceinline__ float rot_sample(const float* __restrict__ img, int H, int W,
                                             const RotGeom& g, int h, int w) {
     return rot_sample_tap(img, H, W, rot_tap(g, h, w));
+}
+
+// scipy.ndimage.rotate(order=1, reshape=False, mode='constant') -- the
+// reference's rot3D (FL/image_util.py:165-203): the same sample point and
+// bilinear weights as rot_sample inside [0, W-1] x [0, H-1], zero outside
+// (no interpolation against the padding within one pixel of the border).
+__device__ __forceinline__ float rot_sample_scipy(const float* __restrict__ img, int H, int W,
+                                                  const RotGeom& g, int h, int w) {
+    const RotTap t = rot_tap(g, h, w);
+    return t.inside ? rot_sample_tap(img, H, W, t) : 0.f;
 }
 
 // Adjoint of rot_sample_tap: spreads v over the in-image taps (global atomics).

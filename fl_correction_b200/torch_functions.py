@@ -112,11 +112,13 @@ def torch_xray_atten_3D(frac_4D, param_angle_energy, dict_use_ref_rotate={}, fla
 
 def offset_canvas(H, W, phi):
     """Side of the square canvas that holds an H x W slice rotated by phi
-    radians: the reference's _rotated_hw size (FL/torch_image_util.py:5-10),
+    radians: the reference's _rotated_hw size (FL/torch_image_util.py:5-10)
+    plus one pixel on each side -- so that no sample of the slice's window,
+    rotated there and back, reaches the zero padding of the canvas edge --
     raised by one where needed so that the padding on each side is a whole
     number of pixels (the rotation centre then stays on the slice centre)."""
     c, s = abs(np.cos(phi)), abs(np.sin(phi))
-    n = max(int(H * c + W * s + 0.5), int(W * c + H * s + 0.5), H, W)
+    n = max(int(H * c + W * s + 0.5), int(W * c + H * s + 0.5), H, W) + 2
     if (n - H) % 2:
         n += 1
     return n

@@ -11,7 +11,7 @@ import torch
 
 from . import _lib
 
-__all__ = ["torch_rotate_image_nd", "torch_rot90_3D", "torch_rot90_4D"]
+__all__ = ["torch_rotate_image_nd", "torch_rot90_3D", "torch_rot90_4D", "rot3D_scipy"]
 
 
 def _angle(theta):
@@ -42,6 +42,28 @@ def torch_rotate_image_nd(x, theta, enable_crop=True, align_corners=False, mode=
     with torch.cuda.device(x.device):
         _lib.call("flc_rotate", _lib.ptr(xc), _lib.ptr(out), xc.numel() // (H * W), H, W, c, s,
                   _lib.stream())
+    return out
+
+
+def rot3D_scipy(x, deg):
+    """The reference's rot3D (FL/image_util.py:165-203; scipy.ndimage.rotate,
+    order 1, reshape=False, mode='constant') of a CUDA tensor (..., H, W) by
+    `deg` degrees counter-clockwise: grid_sample's sample points and weights,
+    zero where the sample falls outside the slice (flc_rotate_ex, mode 1).
+    NaN and inf become 0 first, as rot3D's rm_nan does; 0 degrees returns
+    the cleaned input."""
+    _lib.require_cuda("rot3D_scipy", x)
+    xc = torch.nan_to_num(x.to(torch.float32), nan=0.0, posinf=0.0, neginf=0.0).contiguous()
+    if float(deg) == 0.0:
+        return xc
+    th = float(deg) / 180.0 * math.pi
+    c = float(torch.tensor(math.cos(th), dtype=torch.float32))
+    s = float(torch.tensor(math.sin(th), dtype=torch.float32))
+    H, W = xc.shape[-2:]
+    out = torch.empty_like(xc)
+    with torch.cuda.device(x.device):
+        _lib.call("flc_rotate_ex", _lib.ptr(xc), _lib.ptr(out), xc.numel() // (H * W), H, W, c, s,
+                  1, _lib.stream())
     return out
 
 

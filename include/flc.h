@@ -219,6 +219,8 @@ FLC_API int flc_atten_maps(const float* frac, const float* theta, const float* c
  * frac holds n_ch compound fractions followed by n_ref raw reference volumes
  * (n_ch + n_ref channels, all rotated with the same grid_sample rotation);
  * coef_x (A, n_ch) and coef_f (A, L, n_ch) cover the compounds only.  The
+ * The reference volumes rotate with the reference's scipy boundary rule (see
+ * flc_rotate_ex, mode 1), the fractions with grid_sample's.  The
  * incident coefficient of compound ref_ch is, per voxel, sum_i coef_ref[a][i] *
  * max(ref_i / (sum_k ref_k + 1e-12), 0), with coef_ref (A, n_ref) the spectrum
  * values cs[comp-x_ref{i+1}] * rho * pix per angle.  n_ref = 0 is
@@ -352,6 +354,16 @@ FLC_API int flc_cal_frac(const float* img, const float* mask, float* frac, float
  * (FL/torch_image_util.py:13-114, enable_crop=True). */
 FLC_API int flc_rotate(const float* x, float* out, int64_t N, int64_t H, int64_t W,
                float cos_t, float sin_t, void* stream);
+
+/* flc_rotate with a choice of boundary rule: mode 0 is flc_rotate
+ * (grid_sample, zero padding: within one pixel of the border the sample
+ * interpolates against the padding); mode 1 is scipy.ndimage.rotate with
+ * order=1, reshape=False, mode='constant' -- the reference's rot3D
+ * (FL/image_util.py:165-203), which rotates the reference-spectrum volumes
+ * (FL/atten_util.py:79-88): the same sample points and weights, but zero for
+ * every sample outside [0, W-1] x [0, H-1]. */
+FLC_API int flc_rotate_ex(const float* x, float* out, int64_t N, int64_t H, int64_t W,
+                          float cos_t, float sin_t, int mode, void* stream);
 
 /* Incident attenuation: out[n,h,w] = prod_{h'>h} (1 - mu[n,h',w]), out[n,H-1,w] = 1.
  * Replaces the flip/cumprod/flip of torch_xray_atten_3D (FL/torch_functions.py:95-102). */

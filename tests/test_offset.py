@@ -24,7 +24,7 @@ def test_canvas_holds_the_rotated_slice_with_whole_padding(H, deg):
     phi = deg / 180 * math.pi
     n = offset_canvas(H, H, phi)
     assert n >= max(_rotated_hw(H, H, phi)) and n >= H
-    assert (n - H) % 2 == 0 and n - max(_rotated_hw(H, H, phi)) <= 1
+    assert (n - H) % 2 == 0 and 2 <= n - max(max(_rotated_hw(H, H, phi)), H) <= 3
 
 
 def _oracle_offset(frac, cf, mask, phi):
@@ -70,5 +70,5 @@ def test_small_offset_approaches_the_plain_path():
     mask = generate_detector_mask(13.309, 13.309, 24)
     plain = torch_xrf_atten_3D(frac, p, mask)
     near = torch_xrf_atten_3D(frac, p, mask, detector_offset_angle=0.6)    # just above 1e-2 rad
-    # a 0.6 degree turn moves the far corner of a 24-pixel slice by ~0.25 pixel
+    # a 0.6 degree turn moves the far corner of a 24-pixel slice by ~0.2 pixel
     assert rel_err(near, plain) < 0.05

@@ -67,6 +67,9 @@ SIGNATURES = {
     "flc_rotate": (_int, [_vp, _vp, _i64, _i64, _i64, _f32, _f32, _vp]),
     "flc_incident_scan": (_int, [_vp, _vp, _i64, _i64, _i64, _vp]),
     "flc_rotate_ex": (_int, [_vp, _vp, _i64, _i64, _i64, _f32, _f32, _int, _vp]),
+    "flc_xray_atten_ref2d_workspace_bytes": (_sz, []),
+    "flc_xray_atten_ref2d": (_int, [_vp, _vp, _vp, _vp, _vp, _f32, _vp, _i64, _i64, _i64, _i64,
+                                    _int, _vp, _sz, _vp]),
 }
 
 _LIB = None

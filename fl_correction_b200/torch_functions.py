@@ -15,7 +15,8 @@ from .detector_mask import factor_mask
 
 __all__ = ["torch_extract_3D_mu_xray", "torch_extract_3D_mu_xrf", "torch_xray_atten_3D",
            "torch_xrf_atten_3D", "torch_3D_forward_projection", "coef_xray", "coef_xrf",
-           "compose_cs_incident_xray_with_reference", "offset_canvas"]
+           "compose_cs_incident_xray_with_reference", "offset_canvas",
+           "torch_2D_xray_atten_with_ref", "torch_2D_xray_atten_with_ref_vectorize"]
 
 
 def coef_xray(param_angle_energy, n_ch=None):
@@ -183,3 +184,42 @@ def torch_3D_forward_projection(C, angle_list, em_cs, atten, mode="batch"):
     for i in range(n_sli):
         prj[:, i] = forward_emission(at[:, i].contiguous(), C[:, i].contiguous(), em, theta).cpu().numpy()
     return prj
+
+
+def _xray_atten_with_ref(C, C_other, theta, cs_ref, rho, pix, variant):
+    dev = _lib.require_cuda("torch_2D_xray_atten_with_ref", C, dtype=None)
+    f32 = dict(dtype=torch.float32, device=dev)
+    n_ref, H, W = C.shape
+    th = torch.as_tensor(theta, **f32).reshape(-1).contiguous()
+    A = th.numel()
+    cs = torch.as_tensor(cs_ref, **f32).reshape(A, n_ref).contiguous()
+    rh = torch.as_tensor(rho, **f32).expand(H, W).contiguous()
+    Co = torch.as_tensor(C_other, **f32).expand(H, W).contiguous()
+    Cc = C.detach().to(**f32).contiguous()
+    out = torch.empty((A, H, W), **f32)
+    nb = _lib.query("flc_xray_atten_ref2d_workspace_bytes")
+    ws = _lib.workspace(nb, dev)
+    _lib.call("flc_xray_atten_ref2d", _lib.ptr(Cc), _lib.ptr(Co), _lib.ptr(th), _lib.ptr(cs),
+              _lib.ptr(rh), float(pix), _lib.ptr(out), n_ref, A, H, W, variant, _lib.ptr(ws), nb,
+              _lib.stream(dev))
+    return out.to(C.dtype)
+
+
+def torch_2D_xray_atten_with_ref(C, C_other, theta_list, cs_ref, rho, pix):
+    """Incident X-ray attenuation (n_angle, H, W) of one slice from reference
+    volumes C (n_ref, H, W) (FL/torch_functions.py:181-215): C scaled by
+    1 / (max(sum_j C_j + C_other) + 1e-9), rotated by theta_list (radians,
+    grid_sample with align_corners=False), mu = sum_j cs_ref[a, j] * frac_j *
+    rho * pix with rho (H, W) unrotated, and the exclusive product of
+    max(1 - mu, 1e-6) over the rows below, last row 1.  One native call
+    (flc_xray_atten_ref2d, variant 0); the result is not differentiable."""
+    return _xray_atten_with_ref(C, C_other, theta_list, cs_ref, rho, pix, 0)
+
+
+def torch_2D_xray_atten_with_ref_vectorize(C, C_other, theta, cs_ref, rho, pix):
+    """FL/torch_functions.py:247-330 with its own numbers: scale 1 / (max +
+    1e-8), rotation with align_corners=True, mu clipped at 0, floor 1e-8, and
+    the reference's shifted cumulative product, which includes row h itself
+    for h < H-1 (last row 1).  flc_xray_atten_ref2d, variant 1; the result
+    is not differentiable."""
+    return _xray_atten_with_ref(C, C_other, theta, cs_ref, rho, pix, 1)

@@ -217,10 +217,10 @@ FLC_API int flc_atten_maps(const float* frac, const float* theta, const float* c
 /* flc_atten_maps with a reference-spectrum incident cross section (the
  * XANES case of FL/torch_functions.py:22-37, FL/cross_section_util.py:44-66):
  * frac holds n_ch compound fractions followed by n_ref raw reference volumes
- * (n_ch + n_ref channels, all rotated with the same grid_sample rotation);
- * coef_x (A, n_ch) and coef_f (A, L, n_ch) cover the compounds only.  The
- * The reference volumes rotate with the reference's scipy boundary rule (see
- * flc_rotate_ex, mode 1), the fractions with grid_sample's.  The
+ * (n_ch + n_ref channels); coef_x (A, n_ch) and coef_f (A, L, n_ch) cover the
+ * compounds only.  All channels rotate about the same centre with the same
+ * sample points; the reference volumes take the reference's scipy boundary
+ * rule (see flc_rotate_ex, mode 1), the fractions grid_sample's.  The
  * incident coefficient of compound ref_ch is, per voxel, sum_i coef_ref[a][i] *
  * max(ref_i / (sum_k ref_k + 1e-12), 0), with coef_ref (A, n_ref) the spectrum
  * values cs[comp-x_ref{i+1}] * rho * pix per angle.  n_ref = 0 is
@@ -347,6 +347,26 @@ FLC_API int flc_cal_frac(const float* img, const float* mask, float* frac, float
                          int64_t n_ch, int64_t N, int use_range, double r0, double r1,
                          int enable_scale, double scale_limit, void* workspace,
                          size_t workspace_bytes, void* stream);
+
+/* Incident X-ray attenuation of one slice from reference-spectrum volumes,
+ * replacing torch_2D_xray_atten_with_ref (variant 0, FL/torch_functions.py:
+ * 181-215) and torch_2D_xray_atten_with_ref_vectorize (variant 1, :247-330).
+ * C (n_ref, H, W) reference volumes, C_other (H, W), theta (A,) radians,
+ * cs_ref (A, n_ref), rho (H, W) (applied unrotated), pix; out (A, H, W), all
+ * device FP32.  With frac = C / (max_p(sum_j C_j + C_other) + eps) rotated to
+ * each angle and mu = (sum_j cs_ref[a][j] frac_j) rho pix, f = max(1 - mu, fl):
+ *   variant 0: eps 1e-9, grid_sample rotation with align_corners=False,
+ *              fl 1e-6, out[h] = prod_{h' > h} f[h'], out[H-1] = 1;
+ *   variant 1: eps 1e-8, align_corners=True, mu clipped at 0, fl 1e-8,
+ *              out[h] = prod_{h' >= h} f[h'] for h < H-1, out[H-1] = 1
+ *              (the reference's shifted cumulative product includes row h).
+ * H, W >= 2.  Workspace: flc_xray_atten_ref2d_workspace_bytes() bytes of
+ * device memory (the normaliser). */
+FLC_API size_t flc_xray_atten_ref2d_workspace_bytes(void);
+FLC_API int flc_xray_atten_ref2d(const float* C, const float* C_other, const float* theta,
+                                 const float* cs_ref, const float* rho, float pix, float* out,
+                                 int64_t n_ref, int64_t A, int64_t H, int64_t W, int variant,
+                                 void* workspace, size_t workspace_bytes, void* stream);
 
 /* Rotation with torch grid_sample semantics (bilinear, zero padding,
  * align_corners=False, same-size output): out (N, H, W) from x (N, H, W).

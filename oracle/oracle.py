@@ -351,3 +351,68 @@ def cal_frac(img, scale_range=(0.02, 0.98), enable_scale=True, scale_limit=0.95)
                     t[t <= ts[0]] = ts[0]
             out[i] = t * ratio
     return out
+
+
+def _rotate_aspect(x, c, s, sxw, syh):
+    """Bilinear rotation of (..., H, W) about the centre with grid_sample's
+    zero-padded taps: out(h, w) samples x at ix = c dw - s dh sxw + cx,
+    iy = s dw syh + c dh + cy (dw = w - cx, dh = h - cy)."""
+    x = np.asarray(x, np.float64)
+    H, W = x.shape[-2:]
+    cx, cy = (W - 1) / 2.0, (H - 1) / 2.0
+    dh, dw = np.meshgrid(np.arange(H) - cy, np.arange(W) - cx, indexing="ij")
+    ix = c * dw - s * dh * sxw + cx
+    iy = s * dw * syh + c * dh + cy
+    x0, y0 = np.floor(ix).astype(np.int64), np.floor(iy).astype(np.int64)
+    tx, ty = ix - x0, iy - y0
+    out = np.zeros(x.shape)
+    for dy, wy in ((0, 1 - ty), (1, ty)):
+        for dx, wx in ((0, 1 - tx), (1, tx)):
+            yy, xx = y0 + dy, x0 + dx
+            ok = (yy >= 0) & (yy < H) & (xx >= 0) & (xx < W)
+            v = x[..., np.clip(yy, 0, H - 1), np.clip(xx, 0, W - 1)]
+            out += np.where(ok, v, 0.0) * wy * wx
+    return out
+
+
+def xray_atten_ref2d(C, C_other, theta, cs_ref, rho, pix, variant=0):
+    """torch_2D_xray_atten_with_ref (variant 0, FL/torch_functions.py:181-215)
+    and torch_2D_xray_atten_with_ref_vectorize (variant 1, :247-330) in FP64:
+    C (n_ref, H, W), C_other (H, W), theta (A,) radians, cs_ref (A, n_ref),
+    rho (H, W) -> (A, H, W).  Variant 0: scale eps 1e-9, align_corners=False
+    rotation (aspect W/H), floor 1e-6, exclusive product of the rows below;
+    variant 1: eps 1e-8, align_corners=True (aspect (W-1)/(H-1)), mu clipped
+    at 0, floor 1e-8, product including row h for h < H-1; last row 1."""
+    C = np.asarray(C, np.float64)
+    n_ref, H, W = C.shape
+    th = np.asarray(theta, np.float32).reshape(-1)
+    cs = np.asarray(cs_ref, np.float64).reshape(len(th), n_ref)
+    rho = np.broadcast_to(np.asarray(rho, np.float64), (H, W))
+    eps = 1e-8 if variant == 1 else 1e-9
+    frac = C / ((C.sum(axis=0) + np.asarray(C_other, np.float64)).max() + eps)
+    if variant == 1:
+        sxw, syh = (W - 1) / (H - 1), (H - 1) / (W - 1)
+    else:
+        sxw, syh = W / H, H / W
+    out = np.ones((len(th), H, W))
+    for a, t in enumerate(th):
+        if variant == 1:
+            c, s = float(np.cos(t)), float(np.sin(t))
+        else:
+            c, s = fp32_cos_sin(t)
+        fr = _rotate_aspect(frac, c, s, sxw, syh)
+        mu = np.einsum("j,jhw->hw", cs[a], fr) * rho * pix
+        if variant == 1:
+            mu = np.maximum(mu, 0.0)
+        f = np.maximum(1.0 - mu, 1e-8 if variant == 1 else 1e-6)
+        p = np.ones(W)
+        for h in range(H - 1, -1, -1):
+            if variant == 1:
+                p = p * f[h]
+                if h < H - 1:
+                    out[a, h] = p
+            else:
+                if h < H - 1:
+                    out[a, h] = p
+                p = p * f[h]
+    return out

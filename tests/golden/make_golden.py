@@ -266,6 +266,27 @@ def main():
     r = core.cal_frac(cimg, scale_range=[0.1, 0.7], enable_scale=True, scale_limit=0.5)
     out["calfrac_other"] = r["frac"]
 
+    # ---- torch_2D_xray_atten_with_ref[_vectorize] (FL/torch_functions.py:181,247)
+    # a non-square slice (the aspect terms of both rotations), negative
+    # entries (the relu of the vectorised form) and mu above 1 (the floors)
+    import torch
+    rng4 = np.random.default_rng(20240614)
+    H2, W2, n_ref2 = 20, 26, 3
+    xc = rng4.random((n_ref2, H2, W2)).astype(np.float32)
+    xc[1, 4:7, 3:9] = -0.6
+    xo = (rng4.random((H2, W2)) * 0.5).astype(np.float32)
+    xth = np.array([0.0, 0.4, 1.3, 2.5, -0.7], np.float32)
+    xcs = (rng4.random((len(xth), n_ref2)) * 3.0).astype(np.float32)
+    xcs[2, 0] = 60.0                           # one angle past the floors
+    xrho = (1.0 + rng4.random((H2, W2)) * 4.0).astype(np.float32)
+    xpix = 0.05
+    for k, v in (("C", xc), ("C_other", xo), ("theta", xth), ("cs_ref", xcs), ("rho", xrho)):
+        out["xray2d_" + k] = v
+    meta["xray2d_pix"] = xpix
+    targs = [torch.from_numpy(a) for a in (xc, xo, xth, xcs, xrho)] + [xpix]
+    out["xray2d_out"] = tf.torch_2D_xray_atten_with_ref(*targs).numpy()
+    out["xray2d_vec_out"] = tf.torch_2D_xray_atten_with_ref_vectorize(*targs).numpy()
+
     np.savez_compressed(os.path.join(HERE, "ref_cpu.npz"), **out)
     with open(os.path.join(HERE, "ref_cpu.json"), "w") as f:
         json.dump(meta, f, indent=1)

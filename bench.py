@@ -54,7 +54,7 @@ def parse():
     p.add_argument("--adam-steps", type=int, default=0,
                    help="configurations 2/4: Adam steps timed (default 200 / 3)")
     p.add_argument("--case", default=None, choices=["cone", "cone_direct", "mlem", "fwd", "bwd", "stage",
-                                                    "mlem_multi"],
+                                                    "mlem_multi", "bwd_large"],
                    help="run one kernel on a profiling-sized case instead of the benchmark")
     p.add_argument("--case-slices", type=int, default=16,
                    help="slices of 128^2 in the projector / MLEM cases (128: the benchmark's shape)")
@@ -788,6 +788,22 @@ def run_batch(args, device):
     torch.cuda.synchronize()
     t_loop, t_graph = e[0].elapsed_time(e[1]), e[2].elapsed_time(e[3])
     err = max(float((o - r).abs().max() / r.abs().max()) for o, r in zip(out, loop))
+    graph_out = [c.clone() for c in out]
+    # the persistent form: one launch per MLEM iteration for all 16 volumes'
+    # (volume, element) problems, the schedule replayed as a CUDA graph
+    b.capture_persistent()
+    for _ in range(max(1, args.warmup)):
+        b.run_persistent()
+    torch.cuda.synchronize()
+    ep = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    ep[0].record()
+    for _ in range(args.steps):
+        pout = b.run_persistent()
+    ep[1].record()
+    torch.cuda.synchronize()
+    t_pers = ep[0].elapsed_time(ep[1])
+    err_p = max(float((o - r).abs().max() / r.abs().max()) for o, r in zip(pout, loop))
+    del graph_out
     vol_iters = len(ws) * n_iter * args.steps
     return {
         "metric": "batched corrected MLEM: volume-iterations/s (16 uneven volumes)",
@@ -800,6 +816,13 @@ def run_batch(args, device):
                        "ms_per_step": round(t_loop / args.steps, 2)},
         "speedup_vs_plain_loop": round(t_loop / t_graph, 3),
         "max_rel_err_vs_plain_loop": err,
+        "persistent": {"value": round(vol_iters / (t_pers * 1e-3), 3),
+                       "ms_per_step": round(t_pers / args.steps, 2),
+                       "speedup_vs_plain_loop": round(t_loop / t_pers, 3),
+                       "max_rel_err_vs_plain_loop": err_p,
+                       "form": "one flc_mlem_multi_sizes launch per MLEM iteration over all "
+                               "(volume, element) problems; attenuation rebuilt per volume; "
+                               "the schedule replayed as one CUDA graph"},
         # a replay runs the kernels the eager loop launches (the graph was
         # captured from the same schedule); the host-side counter does not see
         # graph replays, so the loop's count stands for them
@@ -813,7 +836,8 @@ def run_case(args):
     benchmark size (2 angles x 3 lines of 128^3), spectral form (cone_direct:
     the direct separable kernel); mlem: one fused MLEM
     iteration (plus the sensitivity pass) at 24 angles x 16 slices of 128^2;
-    fwd / bwd: the projector at 120 angles x 16 slices of 128^2."""
+    fwd / bwd: the projector at 120 angles x 16 slices of 128^2; bwd_large:
+    the backward at 180 angles x --case-slices slices of 256^2."""
     import torch
     from fl_correction_b200 import _lib
     from fl_correction_b200.cuda_lib import atten_cuda as AC
@@ -870,6 +894,15 @@ def run_case(args):
             _lib.call("flc_atten_stage_ws", _lib.ptr(frac), _lib.ptr(th), _lib.ptr(cx),
                       _lib.ptr(cf), _lib.ptr(atten), _lib.ptr(ws), n_ch, N, N, N, A, L, 0, n_a,
                       0, 1, _lib.ptr(ws4), nb, _lib.stream())
+    elif args.case == "bwd_large":
+        # the row-band backward: 180 angles x --case-slices slices of 256^2
+        N, A, B = 256, 180, args.case_slices
+        atten = torch.rand((A, B, N, N), device=dev, generator=g)
+        em = torch.full((A, 1), 0.02, device=dev)
+        th = torch.linspace(0, math.pi, A + 1, device=dev)[:-1].contiguous()
+        r = torch.rand((A, B, N), device=dev, generator=g)
+        def once():
+            AC.backward_emission_batch(atten, r, em, th)
     elif args.case in ("fwd", "bwd"):
         A, B = 120, args.case_slices
         atten = torch.rand((A, B, N, N), device=dev, generator=g)

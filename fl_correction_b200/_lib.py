@@ -51,6 +51,9 @@ SIGNATURES = {
     "flc_mlem_multi_workspace_bytes": (_sz, [_i64, _vp, _vp, _i64, _i64, _i64]),
     "flc_mlem_multi": (_int, [_i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _f64,
                               _f64, _vp, _sz, _vp]),
+    "flc_mlem_multi_sizes_workspace_bytes": (_sz, [_i64, _vp, _vp, _i64, _vp, _vp]),
+    "flc_mlem_multi_sizes": (_int, [_i64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _i64, _vp, _vp, _i64,
+                                    _f64, _f64, _vp, _sz, _vp]),
     "flc_atten_maps_ref": (_int, [_vp] * 8 + [_i64] * 11 + [_int, _int, _i64, _vp, _sz, _vp]),
     "flc_atten_stage": (_int, [_vp, _vp, _vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _i64,
                                _i64, _i64, _int, _int, _vp]),
@@ -169,21 +172,28 @@ def i64_array(values):
 
 
 def mlem_multi(Cs, attens, ems, thetas, Is, n_iter, beta, delta, ws=None):
-    """flc_mlem_multi over the problems i: C (R, B, H, W) in place, atten
-    (A, B, H, W), em (A, R), theta (A,), I (A, B, W).  Returns the workspace
-    `ws` (reusable for calls of the same shapes)."""
+    """flc_mlem_multi_sizes over the problems i: C (R, B, H, W) in place,
+    atten (A, B, H, W), em (A, R), theta (A,), I (A, B, W); R shared, the
+    other sizes per problem.  Returns the workspace `ws` (reusable for calls
+    of the same shapes)."""
     P = len(Cs)
-    R, _, H, W = Cs[0].shape
+    R = Cs[0].shape[0]
+    if any(c.shape[0] != R for c in Cs):
+        raise ValueError("mlem_multi: every problem must have the same number of references")
     A = [a.shape[0] for a in attens]
     B = [a.shape[1] for a in attens]
+    H = [a.shape[2] for a in attens]
+    W = [a.shape[3] for a in attens]
     pa, ka = i64_array(A)
     pb, kb = i64_array(B)
-    nb = query("flc_mlem_multi_workspace_bytes", P, pa, pb, R, H, W)
+    ph, kh = i64_array(H)
+    pw, kw = i64_array(W)
+    nb = query("flc_mlem_multi_sizes_workspace_bytes", P, pa, pb, R, ph, pw)
     if ws is None or ws.numel() < nb:
         ws = workspace(nb, Cs[0].device)
     keep = [ptr_array(x) for x in (Cs, attens, ems, thetas, Is)]
     with torch.cuda.device(Cs[0].device):
-        call("flc_mlem_multi", P, *[k[0] for k in keep], pa, pb, R, H, W, int(n_iter),
+        call("flc_mlem_multi_sizes", P, *[k[0] for k in keep], pa, pb, R, ph, pw, int(n_iter),
              float(beta), float(delta), ptr(ws), nb, stream())
-    del keep, ka, kb
+    del keep, ka, kb, kh, kw
     return ws

@@ -15,13 +15,19 @@ detector distances -- becomes one job:
   small volumes run side by side instead of leaving most SMs idle;
 * `run()` replays that one graph.
 
+`run_persistent()` is the other batched form: between attenuation rebuilds,
+the MLEM iterations of every (volume, element) pair run as ONE persistent
+launch per iteration (flc_mlem_multi_sizes: clusters take (problem, slice)
+items of all volumes from a device work queue), optionally replayed as a
+CUDA graph of the whole schedule (`capture_persistent`).
+
 `run_loop()` is the plain single-volume path for comparison: the same
 problems one after another, default launch shapes, no graph.
 """
 import numpy as np
 import torch
 
-from . import tune
+from . import _lib, tune
 from .detector_mask import generate_detector_mask
 from .recon import CorrectedMLEM
 
@@ -146,6 +152,55 @@ class BatchedMLEM:
             self.capture()
         self.graph.replay()
         return self.C
+
+    # -- the persistent multi-problem path -----------------------------------
+    def _multi_args(self):
+        Cs, ats, ems, ths, Is = [], [], [], [], []
+        for s, C, I in zip(self.solvers, self.C, self.I):
+            for l in range(s.L):
+                Cs.append(C[l:l + 1])
+                ats.append(s.atten[l])
+                ems.append(s.em[l])
+                ths.append(s.theta)
+                Is.append(I[l])
+        return Cs, ats, ems, ths, Is
+
+    def _issue_persistent(self):
+        betas = {(s.beta, s.delta) for s in self.solvers}
+        if len(betas) != 1:
+            raise ValueError("run_persistent: every volume must use the same beta and delta")
+        beta, delta = betas.pop()
+        for C in self.C:
+            C.fill_(1.0)
+        args = self._multi_args()
+        done = 0
+        while done < self.n_iter:
+            kk = min(self.k, self.n_iter - done)
+            for s, C in zip(self.solvers, self.C):
+                s.recompute_attenuation(C)
+            self._ws_multi = _lib.mlem_multi(*args, kk, beta, delta, getattr(self, "_ws_multi", None))
+            done += kk
+
+    def run_persistent(self):
+        """The schedule with one persistent MLEM launch per iteration for all
+        (volume, element) problems; replays the captured graph when
+        `capture_persistent` has run.  Returns the C list."""
+        if getattr(self, "graph_persistent", None) is not None:
+            self.graph_persistent.replay()
+        else:
+            self._issue_persistent()
+        return self.C
+
+    def capture_persistent(self):
+        """Record the persistent schedule into one CUDA graph (one eager run
+        first, so that the workspace and every launch plan exist)."""
+        self._issue_persistent()
+        torch.cuda.synchronize(self.device)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=torch.cuda.Stream(self.device)):
+            self._issue_persistent()
+        self.graph_persistent = g
+        return g
 
 
 def problems_from_workloads(workloads, device="cuda"):

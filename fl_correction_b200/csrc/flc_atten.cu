@@ -209,15 +209,17 @@ __global__ void atten_stage_kernel(const float* __restrict__ frac, const float4*
                                       : 0.f;
             }
             // the reference-spectrum coefficient of channel ref.ch at this voxel
+            // (the rotated reference volumes clipped below at 0, as rot3D
+            // clips them)
             float cxr = 0.f;
             if (ref.ch >= 0) {
                 float tot = 1e-12f;
 #pragma unroll
                 for (int j = 0; j < kMaxCh; ++j)
-                    if (j >= n_ch && j < n_tot) tot += fr[j];
+                    if (j >= n_ch && j < n_tot) tot += fmaxf(fr[j], 0.f);
 #pragma unroll
                 for (int j = 0; j < kMaxCh; ++j)
-                    if (j >= n_ch && j < n_tot) cxr += cf.cref[j - n_ch] * fmaxf(fr[j] / tot, 0.f);
+                    if (j >= n_ch && j < n_tot) cxr += cf.cref[j - n_ch] * (fmaxf(fr[j], 0.f) / tot);
             }
             // incident term: write the exclusive product, then fold in this voxel
             if (incident_mode != 2) {

@@ -46,7 +46,9 @@ enum TuneKey {
     kTuneConeSkipLoad = 6,
     kTuneProjLegacy = 7,    // 1: the earlier projector / fused-MLEM kernels instead of
                             // the two lean kernels (for comparison)
-    kTuneCount = 8
+    kTuneProjBand = 8,      // 1: the band backward at every slice size (it runs by
+                            // itself only where the lean kernel's image does not fit)
+    kTuneCount = 9
 };
 int64_t tune(int key);
 

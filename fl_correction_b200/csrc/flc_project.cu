@@ -5,7 +5,7 @@
 // FL/cuda_lib/atten_cuda.cpp:82-345.  The reference scatters with one global
 // atomicAdd per sample (forward) and four per sample per reference
 // (backward).  Here one CTA owns one slice b and a group of angles:
-//  * the slice of C is staged once in shared memory (row pitch == 3 mod 32,
+//  * the slice of C is staged once in shared memory (row pitch == 9 mod 32,
 //    which spreads the rotated bilinear taps of a warp over the banks);
 //  * per angle the atten tile (H x W, contiguous) is copied into shared memory
 //    with coalesced 128-bit loads, issued one angle ahead into registers so
@@ -46,10 +46,11 @@ constexpr int kMaxCluster = 8;
 constexpr int kMaxR = 8;
 constexpr int kTileRegs = 8;   // float4 per thread prefetched for the next tile
 
-// Row pitch (floats) of a staged slice: >= W and == 3 (mod 32).
+// Row pitch (floats) of a staged slice: >= W and == 9 (mod 32) (of the odd
+// residues measured, 1, 3 and 9, the fastest for the column-segment kernels).
 __host__ __device__ inline int slice_pitch(int W) {
     int p = W;
-    while ((p & 31) != 3) ++p;
+    while ((p & 31) != 9) ++p;
     return p;
 }
 
@@ -801,6 +802,7 @@ __device__ __forceinline__ void fwd_angle2(const float* __restrict__ at, const f
         const float* ap = at + (int64_t)h0 * W + w;
         float acc = 0.f;
         float hf = (float)h0 - g.cy;
+
         // rows past the part repeat its last row with weight 0
         float cur[kFwdU], nxt[kFwdU];
 #pragma unroll
@@ -852,7 +854,7 @@ __device__ __forceinline__ void fwd_finish(const float* sp, int parts, int W, fl
 }
 
 // Forward: grid (angle groups, B).  The CTA stages slice b of C (R images,
-// row pitch == 3 mod 32) and walks its angles (fwd_angle2).  The partial sums
+// row pitch == 9 mod 32) and walks its angles (fwd_angle2).  The partial sums
 // are double buffered, so an angle costs one barrier.  I != nullptr: out =
 // I / max(Pf, 1e-6) (the MLEM ratio), else out = Pf.
 template <int RC>
@@ -900,6 +902,10 @@ __device__ __forceinline__ void stage_q(float* sq, const float* __restrict__ rat
 // samples with plain read-modify-writes (the caller's phases keep concurrent
 // footprints disjoint), clamped ones into the frame buffers.  The segment's
 // attenuation values are loaded kSegU at a time before any of them is used.
+// (Taking the clamped samples out of the phases -- into the threads a phase
+// leaves idle, or into a pass over all threads after each angle -- measured
+// slower: 2.53 and 1.92 ms against 1.56 ms for the backward of 120 angles x
+// 128 slices of 128^2; without any clamped samples it would run 1.22 ms.)
 template <int RC>
 __device__ __forceinline__ void bwd_segment(const float* __restrict__ at, const float* q,
                                             float* sacc, float* srow, float* scol, int img,
@@ -1065,6 +1071,228 @@ proj_bwd2_kernel(const float* __restrict__ atten, const float* __restrict__ rati
 }
 
 // ---------------------------------------------------------------------------
+// Band backward, for slices whose image does not fit in shared memory: grid
+// (G * nband, B), cluster (G, 1, 1).  CTA (band, g) of slice b owns the image
+// rows [r0, r1) = [band*hb, band*hb + hb) and splats angles [g*apc, ...) of
+// the samples whose footprint starts on a row i0 in [r0-1, r1-1] into a band
+// image of rows r0-1 .. r1 (the two halo rows take the halves of footprints
+// that belong to the neighbouring bands and are dropped).  Every footprint row
+// is thus added by exactly the band that owns it, with plain shared-memory
+// read-modify-writes: no global atomics.  Within an angle the samples are
+// walked along lines -- sample columns when |cos| >= |sin|, else sample rows,
+// so that a line crosses the band in at most (hb+1)*sqrt(2) + 6 samples --
+// in six phases (line mod 3 x segment parity), as bwd_splat_angles does; x(h)
+// and y(h) are computed by the forward's expressions, so each sample's
+// weights, band and clamp class are the forward's.  Clamped samples go to
+// band-local frame buffers (the column part indexed by local row), folded in
+// at the end.  The cluster reduces the band over DSMEM and applies
+// bwd_epilogue (mode 0: back-projection, mode 1: MLEM update).
+// ---------------------------------------------------------------------------
+template <int RC>
+__device__ __forceinline__ void band_segment(const float* __restrict__ at, const float* q,
+                                             float* sacc, float* srow, float* scol, int img,
+                                             int pitch, int R, const Geo& g, int H, int W,
+                                             int nrow, bool colmode, int L, int p0, int p1, int r0,
+                                             Corners& cs) {
+    // colmode: line = sample column w = L, position = h; else line = sample row h = L
+    const float hfL = (float)L - g.cy;
+    const float bxL = col_bx(g, L), byL = col_by(g, L);
+    const int lmax = nrow - 2;           // local i0 in [0, nrow - 2]
+    // attenuation address of position p: base + p * step
+    const float* ap = colmode ? at + L : at + (int64_t)L * W;
+    const int64_t step = colmode ? W : 1;
+    const int n = p1 - p0;
+    for (int j = 0; j < n; j += kSegU) {
+        // the attenuation values of the next kSegU positions, loaded before
+        // any is used (the loads of positions outside the band are wasted)
+        float av[kSegU];
+#pragma unroll
+        for (int k = 0; k < kSegU; ++k) av[k] = __ldg(ap + (int64_t)(p0 + min(j + k, n - 1)) * step);
+#pragma unroll
+        for (int k = 0; k < kSegU; ++k) {
+            if (j + k >= n) break;
+            const int p = p0 + j + k;
+            const int w = colmode ? L : p;
+            float x, y;
+            if (colmode) {
+                const float hf = (float)p - g.cy;
+                x = fmaf(g.c, hf, bxL);
+                y = fmaf(g.s, hf, byL);
+            } else {
+                x = fmaf(g.c, hfL, col_bx(g, p));
+                y = fmaf(g.s, hfL, col_by(g, p));
+            }
+            const float xc = fminf(fmaxf(x, 0.f), g.rmax), yc = fminf(fmaxf(y, 0.f), g.cmax);
+            float fx, fy;
+            const int i0 = ffloor(xc, fx), j0 = ffloor(yc, fy);
+            const int li = i0 - r0 + 1;
+            if ((unsigned)li > (unsigned)lmax) continue;
+            if (x == xc && y == yc) {
+                for (int r = 0; r < (RC > 0 ? RC : R); ++r) {
+                    const float v = av[k] * q[r * W + w];
+                    const float ra = v * fx, rb = v - ra;
+                    const float a1 = ra * fy, b1 = rb * fy;
+                    float* pp = sacc + r * img + li * pitch + j0;
+                    const float s0 = pp[0], s1 = pp[1], s2 = pp[pitch], s3 = pp[pitch + 1];
+                    pp[0] = s0 + (rb - b1);
+                    pp[1] = s1 + b1;
+                    pp[pitch] = s2 + (ra - a1);
+                    pp[pitch + 1] = s3 + a1;
+                }
+            } else {
+                Foot f;
+                f.i0 = li;
+                f.j0 = j0;
+                f.fx = fx;
+                f.fy = fy;
+                f.kind = (x < 0.f ? 1 : 0) | (x > g.rmax ? 2 : 0) | (y < 0.f ? 4 : 0) |
+                         (y > g.cmax ? 8 : 0);
+                for (int r = 0; r < (RC > 0 ? RC : R); ++r)
+                    frame_add<false>(f, av[k] * q[r * W + w], srow, scol, nrow, W, cs, r);
+            }
+        }
+    }
+}
+
+// Adds the band's frame buffers into its image: the row part (slot 0: image
+// row 0, slot 1: rows ih, ih+1 split by (1 - fxh, fxh)) where those rows lie
+// in the band image, the column part (slot 0: column 0, slot 1: columns jh,
+// jh+1) on every local row.
+__device__ void band_fold(float* sacc, const float* sframe, int ncopy, int img, int pitch, int R,
+                          int H, int W, int nrow, int r0) {
+    __syncthreads();
+    const Geo g0 = make_geo(0.f, H, W);
+    const int copy = 2 * R * (nrow + W);
+    const int l_lo = 0 - r0 + 1, l_hi = g0.ih - r0 + 1;
+    for (int t = threadIdx.x; t < R * W; t += blockDim.x) {
+        const int r = t / W, j = t - r * W;
+        float lo = 0.f, hi = 0.f;
+        for (int c = 0; c < ncopy; ++c) {
+            lo += sframe[c * copy + 2 * r * W + j];
+            hi += sframe[c * copy + 2 * r * W + W + j];
+        }
+        float* im = sacc + r * img + j;
+        if (l_lo >= 0 && l_lo < nrow) im[l_lo * pitch] += lo;
+        if (l_hi >= 0 && l_hi < nrow) im[l_hi * pitch] += hi * (1.f - g0.fxh);
+        if (l_hi + 1 >= 0 && l_hi + 1 < nrow) im[(l_hi + 1) * pitch] += hi * g0.fxh;
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < R * nrow; t += blockDim.x) {
+        const int r = t / nrow, l = t - r * nrow;
+        float lo = 0.f, hi = 0.f;
+        for (int c = 0; c < ncopy; ++c) {
+            lo += sframe[c * copy + 2 * R * W + 2 * r * nrow + l];
+            hi += sframe[c * copy + 2 * R * W + 2 * r * nrow + nrow + l];
+        }
+        float* im = sacc + r * img + l * pitch;
+        im[0] += lo;
+        im[g0.jh] += hi * (1.f - g0.fyh);
+        im[g0.jh + 1] += hi * g0.fyh;
+    }
+    __syncthreads();
+}
+
+template <int RC>
+__global__ void __launch_bounds__(kT2, 3)
+proj_bwd_band_kernel(const float* __restrict__ atten, const float* __restrict__ ratio,
+                     const float* __restrict__ em, const float* __restrict__ theta,
+                     float* __restrict__ out, const float* __restrict__ Cin,
+                     const float* __restrict__ sens, int A, int B, int Rrt, int H, int W, int apc,
+                     int hb, int seg, int ncopy, float clamp_min, int mode, float beta,
+                     float delta) {
+    extern __shared__ __align__(16) float smem[];
+    cg::cluster_group cluster = cg::this_cluster();
+    const int R = RC > 0 ? RC : Rrt;
+    const int G = (int)cluster.num_blocks(), rank = (int)cluster.block_rank();
+    const int band = blockIdx.x / G, b = blockIdx.y;
+    const int r0 = band * hb, r1 = min(H, r0 + hb);
+    const int nrow = r1 - r0 + 2;
+    const int a0 = rank * apc, a1 = min(A, a0 + apc);
+    const int pitch = slice_pitch(W);
+    const int img = nrow * pitch;
+    float* sacc = smem;                                          // [R][nrow][pitch]
+    float* sframe = sacc + R * img;                              // ncopy x [R][2][W + nrow]
+    float* sq = sframe + frame_floats(R, nrow, W, ncopy);        // [2][R][W]
+    float* srow = sframe + ((threadIdx.x >> 5) % ncopy) * 2 * R * (nrow + W);
+    float* scol = srow + 2 * R * W;
+    for (int i = threadIdx.x; i < R * img; i += blockDim.x) sacc[i] = 0.f;
+    for (int i = threadIdx.x; i < frame_floats(R, nrow, W, ncopy); i += blockDim.x) sframe[i] = 0.f;
+    if (a0 < a1) stage_q(sq + (a0 & 1) * R * W, ratio, em, a0, b, B, R, W);
+    __syncthreads();
+    Corners cs;
+    cs.zero();
+    // the band's x window: i0 in [r0-1, r1-1], i.e. the clamped x in [r0-1, r1);
+    // x < 0 clamps to row 0 (i0 = 0) and x > rmax to i0 = ih = H-2
+    const float xlo = r0 <= 1 ? -INFINITY : (float)(r0 - 1);
+    const float xhi = r1 >= H - 1 ? INFINITY : (float)r1;
+    for (int a = a0; a < a1; ++a) {
+        const Geo g = make_geo(theta[a], H, W);
+        const float* at = atten + ((int64_t)a * B + b) * H * W;
+        const float* q = sq + (a & 1) * R * W;
+        const bool colmode = fabsf(g.c) >= fabsf(g.s);
+        const int nlines = colmode ? W : H, len = colmode ? H : W;
+        // dx / d(position) along a line, and x at position 0 of line L:
+        //   colmode x = c (h - cy) + bx(w);  else x = c (h - cy) - s (w - cx) + cy
+        const float slope = colmode ? g.c : -g.s;
+        const float islope = 1.f / slope;
+        // the window [plo, phi) of line L: positions whose x lies in the
+        // band's x window, two positions of margin on each side
+        auto window = [&](int L, float& plo, float& phi) {
+            const float x0 = colmode ? fmaf(g.c, -g.cy, col_bx(g, L))
+                                     : fmaf(g.c, (float)L - g.cy, col_bx(g, 0));
+            const float t1 = (xlo - x0) * islope, t2 = (xhi - x0) * islope;
+            plo = fmaxf(floorf(fminf(t1, t2)) - 2.f, 0.f);
+            phi = fminf(ceilf(fmaxf(t1, t2)) + 3.f, (float)len);
+        };
+        int nsegs = (len + seg - 1) / seg;
+        if (xlo > -INFINITY && xhi < INFINITY) {
+            // a window inside the line is at most (xhi - xlo) / |slope| + 7 long
+            const int span = (int)((xhi - xlo) * fabsf(islope)) + 9;
+            nsegs = min(nsegs, (span + seg - 1) / seg);
+        }
+        // (Longer segments that fit a phase's items in one round of the block
+        // measured slower, 14.1 against 12.3 ms at 180 angles x 64 slices of
+        // 256^2: the windows of the lines differ in length, and the phase
+        // waits for the longest.)
+        for (int ph = 0; ph < 6; ++ph) {
+            const int pw = ph >> 1, ps = ph & 1;
+            const int nl = (nlines - pw + 2) / 3, nsp = (nsegs - ps + 1) / 2;
+            const int items = nl * nsp;
+            for (int it = threadIdx.x; it < items; it += blockDim.x) {
+                const int k = it / nl, cl = it - k * nl;
+                const int L = pw + 3 * cl;
+                float plo, phi;
+                window(L, plo, phi);
+                if (!(plo < phi)) continue;
+                const int p0 = (int)plo + (ps + 2 * k) * seg;
+                const int p1 = min((int)phi, p0 + seg);
+                if (p0 >= p1) continue;
+                band_segment<RC>(at, q, sacc, srow, scol, img, pitch, R, g, H, W, nrow, colmode,
+                                 L, p0, p1, r0, cs);
+            }
+            if (ph == 5 && a + 1 < a1) stage_q(sq + ((a + 1) & 1) * R * W, ratio, em, a + 1, b, B, R, W);
+            __syncthreads();
+        }
+    }
+    band_fold(sacc, sframe, ncopy, img, pitch, R, H, W, nrow, r0);
+    cluster.sync();
+    // reduce the band's own rows (local 1 .. nrow-2) over the cluster
+    const int64_t n = (int64_t)R * (r1 - r0) * W;
+    const int64_t share = (n + G - 1) / G;
+    const int64_t i0 = rank * share, i1 = min(n, i0 + share);
+    for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+        const int r = (int)(i / ((int64_t)(r1 - r0) * W));
+        const int rem = (int)(i - (int64_t)r * (r1 - r0) * W);
+        const int l = rem / W, w = rem - l * W;
+        const int off = r * img + (l + 1) * pitch + w;
+        float s = 0.f;
+        for (int qq = 0; qq < G; ++qq) s += cluster.map_shared_rank(sacc, qq)[off];
+        bwd_epilogue(mode, out, Cin, sens, clamp_min, beta, delta, r, b, B, H, W, r0 + l, w, s);
+    }
+    cluster.sync();
+}
+
+// ---------------------------------------------------------------------------
 // Persistent MLEM over several problems (a problem: one element's -- or one
 // volume's -- C, atten, em, theta, I; all with the same R, H, W).  Work item =
 // (problem, slice); the clusters of G CTAs take items from a device counter
@@ -1080,7 +1308,7 @@ proj_bwd2_kernel(const float* __restrict__ atten, const float* __restrict__ rati
 // problems fill the GPU beside large ones and no launch leaves a tail per
 // problem.
 // ---------------------------------------------------------------------------
-constexpr int kMaxProbs = 32;
+constexpr int kMaxProbs = 64;
 
 struct MlemProb {
     const float* atten;
@@ -1091,7 +1319,8 @@ struct MlemProb {
     const float* Cin;
     float* Cout;
     float* ratio;
-    int A, B;
+    int A, B, H, W;
+    int seg, parts;    // backward segment length, forward partial sums per column
 };
 
 struct MlemQueue {
@@ -1102,19 +1331,18 @@ struct MlemQueue {
 
 template <int RC>
 __global__ void __launch_bounds__(kT2, 3)
-mlem_queue_kernel(const MlemQueue* __restrict__ queue, int* __restrict__ counter, int Rrt, int H,
-                  int W, int seg, int ncopy, int parts, int mode, float beta, float delta) {
+mlem_queue_kernel(const MlemQueue* __restrict__ queue, int* __restrict__ counter, int Rrt,
+                  int img_region, int frame_region, int ncopy, int mode, float beta, float delta) {
     extern __shared__ __align__(16) float smem[];
     __shared__ int s_item;
     cg::cluster_group cluster = cg::this_cluster();
     const int R = RC > 0 ? RC : Rrt;
     const int G = (int)cluster.num_blocks();
     const int rank = (int)cluster.block_rank();
-    const int pitch = slice_pitch(W);
-    const int img = H * pitch;
+    // regions sized by the host for the largest problem
     float* simg = smem;                                     // C (forward) / accumulator
-    float* sframe = simg + R * img;                         // frames; partial sums (forward)
-    float* sq = sframe + frame_floats(R, H, W, ncopy);      // [2][R][W]
+    float* sframe = simg + img_region;                      // frames; partial sums (forward)
+    float* sq = sframe + frame_region;                      // [2][R][W]
     const int n_items = queue->start[queue->n_prob];
     for (;;) {
         if (rank == 0 && threadIdx.x == 0) s_item = atomicAdd(counter, 1);
@@ -1126,6 +1354,9 @@ mlem_queue_kernel(const MlemQueue* __restrict__ queue, int* __restrict__ counter
         while (queue->start[pi + 1] <= item) ++pi;
         const MlemProb P = queue->p[pi];
         const int b = item - queue->start[pi];
+        const int H = P.H, W = P.W, seg = P.seg, parts = P.parts;
+        const int pitch = slice_pitch(W);
+        const int img = H * pitch;
         const int apc = (P.A + G - 1) / G;
         const int a0 = rank * apc, a1 = min(P.A, a0 + apc);
         if (mode == 0) {
@@ -1158,42 +1389,6 @@ mlem_queue_kernel(const MlemQueue* __restrict__ queue, int* __restrict__ counter
 // Copies the problem table (passed by value: no host copy, capture-safe).
 __global__ void mlem_queue_init_kernel(MlemQueue q, MlemQueue* __restrict__ dst) {
     if (threadIdx.x == 0 && blockIdx.x == 0) *dst = q;
-}
-
-// Backward for slices whose image does not fit in shared memory: one thread
-// per (angle, slice, column) walks the beam and adds into global memory with
-// atomics (the reference's own scheme, atten_cuda_kernel.cu:390-446); `out`
-// must be zeroed first.
-__global__ void proj_bwd_global_kernel(const float* __restrict__ atten,
-                                       const float* __restrict__ ratio,
-                                       const float* __restrict__ em,
-                                       const float* __restrict__ theta, float* __restrict__ out,
-                                       int A, int B, int R, int H, int W) {
-    const int w = blockIdx.x * blockDim.x + threadIdx.x;
-    const int b = blockIdx.y, a = blockIdx.z;
-    if (w >= W) return;
-    const Geo g = make_geo(theta[a], H, W);
-    const float rq = ratio ? ratio[((int64_t)a * B + b) * W + w] : 1.f;
-    const float* at = atten + ((int64_t)a * B + b) * H * W;
-    for (int h = 0; h < H; ++h) {
-        const float av = at[(int64_t)h * W + w] * rq;
-        const Smp s = sample(g, h, w);
-        const float w00 = (1.f - s.fy) * (1.f - s.fx), w01 = s.fy * (1.f - s.fx);
-        const float w10 = (1.f - s.fy) * s.fx, w11 = s.fy * s.fx;
-        for (int r = 0; r < R; ++r) {
-            const float v = em[a * R + r] * av;
-            float* img = out + ((int64_t)r * B + b) * H * W + (int64_t)s.i0 * W + s.j0;
-            if (v * w00 != 0.f) atomicAdd(img, v * w00);
-            if (v * w01 != 0.f) atomicAdd(img + 1, v * w01);
-            if (v * w10 != 0.f) atomicAdd(img + W, v * w10);
-            if (v * w11 != 0.f) atomicAdd(img + W + 1, v * w11);
-        }
-    }
-}
-
-__global__ void clamp_min_kernel(float* __restrict__ x, int64_t n, float lo) {
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) x[i] = fmaxf(x[i], lo);
 }
 
 __global__ void huber_kernel(const float* __restrict__ C, float* __restrict__ grad, int64_t n,
@@ -1404,6 +1599,16 @@ int seg2_length(int64_t H, int64_t W) {
     return seg;
 }
 
+// Threads of the lean backward: its largest phase's items rounded up to whole
+// warps (at most kT2), so that no warp of the CTA only waits at the phase
+// barriers.
+int bwd2_threads(int64_t H, int64_t W) {
+    const int64_t seg = seg2_length(H, W);
+    const int64_t items = ((W + 2) / 3) * ((((H + seg - 1) / seg) + 1) / 2);
+    const int64_t t = (items + 31) / 32 * 32;
+    return (int)(t < 64 ? 64 : (t > kT2 ? kT2 : t));
+}
+
 // Shared-memory budget per CTA for `per_sm` resident CTAs (1 KB of each CTA's
 // shared memory is reserved by the runtime), capped by the opt-in limit.
 size_t smem_budget(int per_sm) {
@@ -1423,6 +1628,7 @@ int bwd2_copies(int64_t R, int64_t H, int64_t W) {
 }
 
 bool use_lean() { return tune(kTuneProjLegacy) == 0; }
+bool force_band() { return use_lean() && tune(kTuneProjBand) != 0; }
 
 }  // namespace
 
@@ -1474,13 +1680,67 @@ int bwd2_launch(const float* atten, const float* ratio, const float* em, const f
     const int ncopy = bwd2_copies(R, H, W);
     const size_t smem = bwd2_smem(R, H, W, ncopy);
     const void* fn = R == 1 ? (const void*)proj_bwd2_kernel<1> : (const void*)proj_bwd2_kernel<0>;
-    Plan p = plan_cluster(fn, A, B, smem, kT2);
+    const int threads = bwd2_threads(H, W);
+    Plan p = plan_cluster(fn, A, B, smem, threads);
     int iA = (int)A, iB = (int)B, iR = (int)R, iH = (int)H, iW = (int)W, apc = p.apc;
     int seg = seg2_length(H, W);
     void* args[] = {(void*)&atten, (void*)&ratio, (void*)&em, (void*)&theta, (void*)&out,
                     (void*)&Cin, (void*)&sens, &iA, &iB, &iR, &iH, &iW, &apc, &seg,
                     (void*)&ncopy, &clamp_min, &mode, &beta, &delta};
-    return launch_cluster(fn, dim3(p.G, (unsigned)B), p.G, smem, st, args, kT2);
+    return launch_cluster(fn, dim3(p.G, (unsigned)B), p.G, smem, st, args, threads);
+}
+
+// Band backward (slices too large for the lean kernel): the band height is
+// the largest that lets three CTAs share an SM (bands of at least 48 rows),
+// else two, else one; the bands are evened out, and the angles are split over
+// a cluster when the bands x slices do not fill the GPU.  FLC_ERR_UNSUPPORTED when even
+// a 1-row band does not fit.
+size_t band_smem(int64_t R, int64_t hb, int64_t W, int ncopy) {
+    const int64_t nrow = hb + 2;
+    return sizeof(float) * (R * nrow * slice_pitch((int)W) + frame_floats((int)R, (int)nrow, (int)W, ncopy) +
+                            2 * R * W);
+}
+
+int band_height(int64_t R, int64_t H, int64_t W, int* ncopy_out) {
+    const size_t cap = (size_t)max_smem_optin();
+    if (band_smem(R, 1, W, 1) > cap) return 0;
+    // three CTAs per SM where bands of >= 48 rows (or the whole slice) fit,
+    // else two where bands of >= 8 rows fit, else one
+    const int64_t want3 = H < 48 ? H : 48;
+    int per_sm = band_smem(R, want3, W, 1) <= smem_budget(3) ? 3
+                 : band_smem(R, 8, W, 1) <= smem_budget(2) ? 2 : 1;
+    const size_t budget = smem_budget(per_sm);
+    int64_t hb = 1;
+    while (hb < H && band_smem(R, hb + 1, W, 1) <= budget) ++hb;
+    const int64_t nband = ceil_div(H, hb);
+    hb = ceil_div(H, nband);                     // even bands
+    int ncopy = kMaxFrameCopies;
+    while (ncopy > 1 && band_smem(R, hb, W, ncopy) > budget) ncopy /= 2;
+    *ncopy_out = ncopy;
+    return (int)hb;
+}
+
+int band_launch(const float* atten, const float* ratio, const float* em, const float* theta,
+                float* out, const float* Cin, const float* sens, int64_t A, int64_t B, int64_t R,
+                int64_t H, int64_t W, float clamp_min, int mode, float beta, float delta,
+                cudaStream_t st) {
+    int ncopy = 1;
+    const int hb = band_height(R, H, W, &ncopy);
+    if (hb < 1) {
+        set_error("backward projection: a slice row of W=%lld with R=%lld references does not fit "
+                  "in shared memory", (long long)W, (long long)R);
+        return FLC_ERR_UNSUPPORTED;
+    }
+    const int nband = (int)ceil_div(H, hb);
+    const size_t smem = band_smem(R, hb, W, ncopy);
+    const void* fn = R == 1 ? (const void*)proj_bwd_band_kernel<1> : (const void*)proj_bwd_band_kernel<0>;
+    Plan p = plan_cluster(fn, A, (int64_t)nband * B, smem, kT2);
+    int iA = (int)A, iB = (int)B, iR = (int)R, iH = (int)H, iW = (int)W, apc = p.apc, ihb = hb;
+    int seg = 16;
+    void* args[] = {(void*)&atten, (void*)&ratio, (void*)&em, (void*)&theta, (void*)&out,
+                    (void*)&Cin, (void*)&sens, &iA, &iB, &iR, &iH, &iW, &apc, &ihb, &seg,
+                    (void*)&ncopy, &clamp_min, &mode, &beta, &delta};
+    return launch_cluster(fn, dim3((unsigned)(p.G * nband), (unsigned)B), p.G, smem, st, args, kT2);
 }
 
 // Launches the backward projector (also used for the MLEM sensitivity).
@@ -1488,25 +1748,19 @@ int bwd_emission_launch(const float* atten, const float* ratio, const float* em,
                         const float* theta, float* out, int64_t A, int64_t B, int64_t R,
                         int64_t H, int64_t W, float clamp_min, cudaStream_t st) {
     if (use_lean()) {
-        const int r = bwd2_launch(atten, ratio, em, theta, out, nullptr, nullptr, A, B, R, H, W,
-                                  clamp_min, 0, 0.f, 0.f, st);
+        const int r = force_band() ? FLC_ERR_UNSUPPORTED
+                                   : bwd2_launch(atten, ratio, em, theta, out, nullptr, nullptr, A,
+                                                 B, R, H, W, clamp_min, 0, 0.f, 0.f, st);
         if (r != FLC_ERR_UNSUPPORTED) return r;
+        return band_launch(atten, ratio, em, theta, out, nullptr, nullptr, A, B, R, H, W, clamp_min,
+                           0, 0.f, 0.f, st);
     }
     const size_t cap = (size_t)max_smem_optin();
     int stage_tile = bwd_smem(R, H, W, true, 1) <= cap;
     if (!stage_tile && bwd_smem(R, H, W, false, 1) > cap) {
-        // the slice image does not fit on chip: global atomics
-        FLC_TRY_CUDA(cudaMemsetAsync(out, 0, sizeof(float) * R * B * H * W, st));
-        proj_bwd_global_kernel<<<dim3((unsigned)ceil_div(W, 128), (unsigned)B, (unsigned)A), 128, 0,
-                                 st>>>(atten, ratio, em, theta, out, (int)A, (int)B, (int)R,
-                                       (int)H, (int)W);
-        FLC_TRY(check_launch("proj_bwd_global_kernel"));
-        if (clamp_min > 0.f) {
-            int64_t n = R * B * H * W;
-            clamp_min_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, st>>>(out, n, clamp_min);
-            FLC_TRY(check_launch("clamp_min_kernel"));
-        }
-        return FLC_OK;
+        // the slice image does not fit on chip: row bands
+        return band_launch(atten, ratio, em, theta, out, nullptr, nullptr, A, B, R, H, W, clamp_min,
+                           0, 0.f, 0.f, st);
     }
     int ncopy = frame_copies([&](int n) { return bwd_smem(R, H, W, stage_tile, n); });
     size_t smem = bwd_smem(R, H, W, stage_tile, ncopy);
@@ -1554,13 +1808,20 @@ int mlem_iter_launch(const float* atten, const float* em, const float* theta, co
                      const float* sens, const float* Cin, float* Cout, int64_t A, int64_t B,
                      int64_t R, int64_t H, int64_t W, float beta, float delta, cudaStream_t st,
                      bool* fused, float* ratio_ws) {
-    if (use_lean() && fwd2_smem(R, H, W) <= (size_t)max_smem_optin() &&
+    if (use_lean() && !force_band() && fwd2_smem(R, H, W) <= (size_t)max_smem_optin() &&
         bwd2_smem(R, H, W, 1) <= (size_t)max_smem_optin()) {
         // forward + ratio, then backward + update: two launches
         *fused = true;
         FLC_TRY(fwd2_launch(atten, Cin, em, theta, ratio_ws, I, A, B, R, H, W, st));
         return bwd2_launch(atten, ratio_ws, em, theta, Cout, Cin, sens, A, B, R, H, W, 0.f, 1,
                            beta, delta, st);
+    }
+    if (use_lean() && (force_band() || bwd2_smem(R, H, W, 1) > (size_t)max_smem_optin())) {
+        // large slices: forward + ratio, then the band backward + update
+        *fused = true;
+        FLC_TRY(fwd_emission_launch(atten, Cin, em, theta, ratio_ws, I, A, B, R, H, W, st));
+        return band_launch(atten, ratio_ws, em, theta, Cout, Cin, sens, A, B, R, H, W, 0.f, 1, beta,
+                           delta, st);
     }
     *fused = mlem_smem(R, H, W, 1) <= (size_t)max_smem_optin();
     if (!*fused) return FLC_OK;
@@ -1579,10 +1840,18 @@ int mlem_iter_launch(const float* atten, const float* em, const float* theta, co
 // Computes (and caches) the launch plan of the fused iteration, so that a
 // later stream capture makes no occupancy queries.
 void mlem_iter_prepare(int64_t A, int64_t B, int64_t R, int64_t H, int64_t W) {
-    if (use_lean() && bwd2_smem(R, H, W, 1) <= (size_t)max_smem_optin()) {
+    if (use_lean() && !force_band() && bwd2_smem(R, H, W, 1) <= (size_t)max_smem_optin()) {
         const size_t smem = bwd2_smem(R, H, W, bwd2_copies(R, H, W));
         const void* fn = R == 1 ? (const void*)proj_bwd2_kernel<1> : (const void*)proj_bwd2_kernel<0>;
-        (void)plan_cluster(fn, A, B, smem, kT2);
+        (void)plan_cluster(fn, A, B, smem, bwd2_threads(H, W));
+        return;
+    }
+    if (use_lean()) {
+        int ncopy = 1;
+        const int hb = band_height(R, H, W, &ncopy);
+        if (hb < 1) return;
+        const void* fn = R == 1 ? (const void*)proj_bwd_band_kernel<1> : (const void*)proj_bwd_band_kernel<0>;
+        (void)plan_cluster(fn, A, ceil_div(H, hb) * B, band_smem(R, hb, W, ncopy), kT2);
         return;
     }
     if (mlem_smem(R, H, W, 1) > (size_t)max_smem_optin()) return;
@@ -1638,31 +1907,63 @@ size_t multi_frame_floats(int64_t R, int64_t H, int64_t W, int ncopy) {
     return f > pt ? f : pt;
 }
 
-size_t multi_smem(int64_t R, int64_t H, int64_t W, int ncopy) {
-    return sizeof(float) * ((size_t)R * H * slice_pitch((int)W) + multi_frame_floats(R, H, W, ncopy) +
-                            2 * (size_t)R * W);
+// Shared-memory regions of the queue kernel for the largest of P problems
+// (floats): image, frames / forward partials, q; the total in bytes.
+struct MultiSmem {
+    size_t img, frame, q, bytes;
+};
+
+MultiSmem multi_smem(int64_t P, int64_t R, const int64_t* H, const int64_t* W, int ncopy) {
+    MultiSmem m = {0, 0, 0, 0};
+    for (int64_t i = 0; i < P; ++i) {
+        const size_t img = (size_t)R * H[i] * slice_pitch((int)W[i]);
+        const size_t fr = multi_frame_floats(R, H[i], W[i], ncopy);
+        const size_t q = 2 * (size_t)R * W[i];
+        m.img = img > m.img ? img : m.img;
+        m.frame = fr > m.frame ? fr : m.frame;
+        m.q = q > m.q ? q : m.q;
+    }
+    m.img = (m.img + 3) & ~(size_t)3;       // keep the regions 16-byte aligned
+    m.frame = (m.frame + 3) & ~(size_t)3;
+    m.bytes = sizeof(float) * (m.img + m.frame + m.q);
+    return m;
 }
 
-size_t multi_layout(int64_t P, const int64_t* A, const int64_t* B, int64_t R, int64_t H, int64_t W,
-                    size_t* prob_off) {
+size_t multi_layout(int64_t P, const int64_t* A, const int64_t* B, int64_t R, const int64_t* H,
+                    const int64_t* W, size_t* prob_off) {
     size_t off = 2 * al256(sizeof(MlemQueue)) + 256;   // two tables, the counter
     for (int64_t i = 0; i < P; ++i) {
         if (prob_off) prob_off[i] = off;
-        const size_t nC = al256(sizeof(float) * (size_t)(R * B[i] * H * W));
-        off += 2 * nC + al256(sizeof(float) * (size_t)(A[i] * B[i] * W));
+        const size_t nC = al256(sizeof(float) * (size_t)(R * B[i] * H[i] * W[i]));
+        off += 2 * nC + al256(sizeof(float) * (size_t)(A[i] * B[i] * W[i]));
     }
     return off;
 }
 
+int mlem_multi_impl(int64_t P, float* const* C, const float* const* atten, const float* const* em,
+                    const float* const* theta, const float* const* I, const int64_t* A,
+                    const int64_t* B, int64_t R, const int64_t* H, const int64_t* W, int64_t n_iter,
+                    double beta, double delta, void* workspace, size_t workspace_bytes,
+                    void* stream);
+
 }  // namespace
 }  // namespace flc
 
+extern "C" size_t flc_mlem_multi_sizes_workspace_bytes(int64_t P, const int64_t* A,
+                                                       const int64_t* B, int64_t R,
+                                                       const int64_t* H, const int64_t* W) {
+    if (P < 1 || P > kMaxProbs || !A || !B || !H || !W || R < 1) return 0;
+    for (int64_t i = 0; i < P; ++i)
+        if (A[i] < 1 || B[i] < 1 || H[i] < 1 || W[i] < 1) return 0;
+    return multi_layout(P, A, B, R, H, W, nullptr);
+}
+
 extern "C" size_t flc_mlem_multi_workspace_bytes(int64_t P, const int64_t* A, const int64_t* B,
                                                  int64_t R, int64_t H, int64_t W) {
-    if (P < 1 || P > kMaxProbs || !A || !B || R < 1 || H < 1 || W < 1) return 0;
-    for (int64_t i = 0; i < P; ++i)
-        if (A[i] < 1 || B[i] < 1) return 0;
-    return multi_layout(P, A, B, R, H, W, nullptr);
+    if (P < 1 || P > kMaxProbs) return 0;
+    int64_t hs[kMaxProbs], wsz[kMaxProbs];
+    for (int64_t i = 0; i < P; ++i) hs[i] = H, wsz[i] = W;
+    return flc_mlem_multi_sizes_workspace_bytes(P, A, B, R, hs, wsz);
 }
 
 extern "C" int flc_mlem_multi(int64_t P, float* const* C, const float* const* atten,
@@ -1672,13 +1973,40 @@ extern "C" int flc_mlem_multi(int64_t P, float* const* C, const float* const* at
                               void* workspace, size_t workspace_bytes, void* stream) {
     clear_error();
     FLC_REQUIRE(P >= 1 && P <= kMaxProbs, "flc_mlem_multi: 1 <= P <= %d problems", kMaxProbs);
+    int64_t hs[kMaxProbs], wsz[kMaxProbs];
+    for (int64_t i = 0; i < P; ++i) hs[i] = H, wsz[i] = W;
+    return mlem_multi_impl(P, C, atten, em, theta, I, A, B, R, hs, wsz, n_iter, beta, delta,
+                           workspace, workspace_bytes, stream);
+}
+
+extern "C" int flc_mlem_multi_sizes(int64_t P, float* const* C, const float* const* atten,
+                                    const float* const* em, const float* const* theta,
+                                    const float* const* I, const int64_t* A, const int64_t* B,
+                                    int64_t R, const int64_t* H, const int64_t* W, int64_t n_iter,
+                                    double beta, double delta, void* workspace,
+                                    size_t workspace_bytes, void* stream) {
+    clear_error();
+    FLC_REQUIRE(P >= 1 && P <= kMaxProbs, "flc_mlem_multi_sizes: 1 <= P <= %d problems", kMaxProbs);
+    FLC_REQUIRE(H && W, "flc_mlem_multi_sizes: null pointer argument");
+    return mlem_multi_impl(P, C, atten, em, theta, I, A, B, R, H, W, n_iter, beta, delta,
+                           workspace, workspace_bytes, stream);
+}
+
+namespace flc {
+namespace {
+
+int mlem_multi_impl(int64_t P, float* const* C, const float* const* atten, const float* const* em,
+                    const float* const* theta, const float* const* I, const int64_t* A,
+                    const int64_t* B, int64_t R, const int64_t* H, const int64_t* W, int64_t n_iter,
+                    double beta, double delta, void* workspace, size_t workspace_bytes,
+                    void* stream) {
     FLC_REQUIRE(C && atten && em && theta && I && A && B && workspace,
                 "flc_mlem_multi: null pointer argument");
     int64_t items = 0;
     for (int64_t i = 0; i < P; ++i) {
         FLC_REQUIRE(C[i] && atten[i] && em[i] && theta[i] && I[i],
                     "flc_mlem_multi: null pointer for problem %lld", (long long)i);
-        FLC_TRY(check_proj_sizes(A[i], B[i], R, H, W));
+        FLC_TRY(check_proj_sizes(A[i], B[i], R, H[i], W[i]));
         items += B[i];
     }
     FLC_REQUIRE(n_iter >= 0 && items < (1LL << 30), "flc_mlem_multi: invalid sizes");
@@ -1693,10 +2021,8 @@ extern "C" int flc_mlem_multi(int64_t P, float* const* C, const float* const* at
                   workspace_bytes, need);
         return FLC_ERR_WORKSPACE;
     }
-    const int ncopy_base = 1;
-    if (multi_smem(R, H, W, ncopy_base) > (size_t)max_smem_optin()) {
-        set_error("flc_mlem_multi: a %lld x %lld slice does not fit in shared memory",
-                  (long long)H, (long long)W);
+    if (multi_smem(P, R, H, W, 1).bytes > (size_t)max_smem_optin()) {
+        set_error("flc_mlem_multi: the largest slice does not fit in shared memory");
         return FLC_ERR_UNSUPPORTED;
     }
     cudaStream_t st = as_stream(stream);
@@ -1704,23 +2030,29 @@ extern "C" int flc_mlem_multi(int64_t P, float* const* C, const float* const* at
     MlemQueue* q_even = (MlemQueue*)ws;
     MlemQueue* q_odd = (MlemQueue*)(ws + al256(sizeof(MlemQueue)));
     int* counter = (int*)(ws + 2 * al256(sizeof(MlemQueue)));
-    // problems in decreasing angle count: the long items are taken first
+    // problems in decreasing work per item (angles x slice area): the long
+    // items are taken first
     int order[kMaxProbs];
     for (int i = 0; i < P; ++i) order[i] = i;
+    auto cost = [&](int i) { return A[i] * H[i] * W[i]; };
     for (int i = 1; i < P; ++i)
-        for (int j = i; j > 0 && A[order[j]] > A[order[j - 1]]; --j) std::swap(order[j], order[j - 1]);
+        for (int j = i; j > 0 && cost(order[j]) > cost(order[j - 1]); --j) std::swap(order[j], order[j - 1]);
     MlemQueue te = {}, to = {};
     te.n_prob = to.n_prob = (int)P;
     int64_t amax = 1;
     for (int k = 0; k < P; ++k) {
         const int i = order[k];
         char* base = ws + prob_off[i];
-        const size_t nC = al256(sizeof(float) * (size_t)(R * B[i] * H * W));
+        const size_t nC = al256(sizeof(float) * (size_t)(R * B[i] * H[i] * W[i]));
         float* sens = (float*)base;
         float* alt = (float*)(base + nC);
         float* ratio = (float*)(base + 2 * nC);
-        te.p[k] = MlemProb{atten[i], em[i], theta[i], I[i], sens, C[i], alt, ratio, (int)A[i], (int)B[i]};
-        to.p[k] = MlemProb{atten[i], em[i], theta[i], I[i], sens, alt, C[i], ratio, (int)A[i], (int)B[i]};
+        const int hh = (int)H[i], ww = (int)W[i];
+        const int sg = seg2_length(hh, ww), pt = fwd2_parts(hh, ww);
+        te.p[k] = MlemProb{atten[i], em[i], theta[i], I[i], sens, C[i], alt, ratio,
+                           (int)A[i], (int)B[i], hh, ww, sg, pt};
+        to.p[k] = MlemProb{atten[i], em[i], theta[i], I[i], sens, alt, C[i], ratio,
+                           (int)A[i], (int)B[i], hh, ww, sg, pt};
         te.start[k + 1] = to.start[k + 1] = te.start[k] + (int)B[i];
         amax = A[i] > amax ? A[i] : amax;
     }
@@ -1729,26 +2061,32 @@ extern "C" int flc_mlem_multi(int64_t P, float* const* C, const float* const* at
     mlem_queue_init_kernel<<<1, 32, 0, st>>>(to, q_odd);
     FLC_TRY(check_launch("mlem_queue_init_kernel"));
     // launch shape: frame copies that keep the CTAs per SM, cluster size by
-    // waves x (angles per CTA + 2) over the items, persistent grid
+    // (item work / clusters + the longest item), persistent grid
     int per_sm = 3;
-    while (per_sm > 1 && multi_smem(R, H, W, 1) > smem_budget(per_sm)) --per_sm;
+    while (per_sm > 1 && multi_smem(P, R, H, W, 1).bytes > smem_budget(per_sm)) --per_sm;
     int ncopy = kMaxFrameCopies;
-    while (ncopy > 1 && multi_smem(R, H, W, ncopy) > smem_budget(per_sm)) ncopy /= 2;
-    const size_t smem = multi_smem(R, H, W, ncopy);
+    while (ncopy > 1 && multi_smem(P, R, H, W, ncopy).bytes > smem_budget(per_sm)) ncopy /= 2;
+    const MultiSmem ms = multi_smem(P, R, H, W, ncopy);
     const void* fn = R == 1 ? (const void*)mlem_queue_kernel<1> : (const void*)mlem_queue_kernel<0>;
     int bestG = 1, nclu = 1;
-    int64_t best = -1;
+    double best = -1;
     const int gmax = (int)(amax < kMaxCluster ? amax : kMaxCluster);
     if (int64_t t = tune(kTuneProjCluster)) {
         bestG = (int)(t < gmax ? t : gmax);
-        nclu = active_clusters(fn, bestG, smem, kT2);
+        nclu = active_clusters(fn, bestG, ms.bytes, kT2);
     } else {
         for (int G = 1; G <= gmax; ++G) {
-            const int n = active_clusters(fn, G, smem, kT2);
+            const int n = active_clusters(fn, G, ms.bytes, kT2);
             if (n < 1) continue;
-            const int64_t cost = ceil_div(items, n) * (ceil_div(amax, G) + 2);
-            if (best < 0 || cost < best) {
-                best = cost;
+            double total = 0, longest = 0;
+            for (int64_t i = 0; i < P; ++i) {
+                const double item = (double)(ceil_div(A[i], G) + 2) * (double)(H[i] * W[i]);
+                total += item * (double)B[i];
+                longest = item > longest ? item : longest;
+            }
+            const double c = total / n + longest;
+            if (best < 0 || c < best) {
+                best = c;
                 bestG = G;
                 nclu = n;
             }
@@ -1759,27 +2097,28 @@ extern "C" int flc_mlem_multi(int64_t P, float* const* C, const float* const* at
         return FLC_ERR_UNSUPPORTED;
     }
     if (nclu > items) nclu = (int)items;
-    const int seg = seg2_length(H, W), parts = fwd2_parts(H, W);
-    int iR = (int)R, iH = (int)H, iW = (int)W;
+    int iR = (int)R, img_region = (int)ms.img, frame_region = (int)ms.frame;
     float fb = (float)beta, fd = (float)delta;
     auto launch = [&](const MlemQueue* q, int mode) -> int {
         FLC_TRY_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), st));
-        void* args[] = {(void*)&q, (void*)&counter, &iR, &iH, &iW, (void*)&seg, &ncopy,
-                        (void*)&parts, &mode, &fb, &fd};
-        return launch_cluster(fn, dim3((unsigned)(nclu * bestG)), bestG, smem, st, args, kT2);
+        void* args[] = {(void*)&q, (void*)&counter, &iR, &img_region, &frame_region, &ncopy,
+                        &mode, &fb, &fd};
+        return launch_cluster(fn, dim3((unsigned)(nclu * bestG)), bestG, ms.bytes, st, args, kT2);
     };
     FLC_TRY(launch(q_even, 1));                       // sensitivities
     for (int64_t it = 0; it < n_iter; ++it) FLC_TRY(launch((it & 1) ? q_odd : q_even, 0));
     if (n_iter & 1) {
         for (int64_t i = 0; i < P; ++i) {
-            const size_t nC = al256(sizeof(float) * (size_t)(R * B[i] * H * W));
-            FLC_TRY_CUDA(cudaMemcpyAsync(C[i], ws + prob_off[i] + nC,
-                                         sizeof(float) * (size_t)(R * B[i] * H * W),
+            const size_t n = sizeof(float) * (size_t)(R * B[i] * H[i] * W[i]);
+            FLC_TRY_CUDA(cudaMemcpyAsync(C[i], ws + prob_off[i] + al256(n), n,
                                          cudaMemcpyDeviceToDevice, st));
         }
     }
     return FLC_OK;
 }
+
+}  // namespace
+}  // namespace flc
 
 extern "C" int flc_huber_grad(const float* C, float* grad, int64_t RB, int64_t H, int64_t W,
                               float delta, void* stream) {

@@ -51,7 +51,10 @@ def rot3D_scipy(x, deg):
     `deg` degrees counter-clockwise: grid_sample's sample points and weights,
     zero where the sample falls outside the slice (flc_rotate_ex, mode 1).
     NaN and inf become 0 first, as rot3D's rm_nan does; 0 degrees returns
-    the cleaned input."""
+    the cleaned input; a rotated result is clipped below at 0, as rot3D
+    clips it.  (rot3D rotates in FP64 -- rm_nan returns float64 -- and at
+    multiples of 90 degrees with order 0; here the FP32 bilinear rotation
+    lands within FP32 rounding of both.)"""
     _lib.require_cuda("rot3D_scipy", x)
     xc = torch.nan_to_num(x.to(torch.float32), nan=0.0, posinf=0.0, neginf=0.0).contiguous()
     if float(deg) == 0.0:
@@ -64,7 +67,7 @@ def rot3D_scipy(x, deg):
     with torch.cuda.device(x.device):
         _lib.call("flc_rotate_ex", _lib.ptr(xc), _lib.ptr(out), xc.numel() // (H * W), H, W, c, s,
                   1, _lib.stream())
-    return out
+    return out.clamp_(min=0.0)
 
 
 def torch_rot90_3D(img_raw, ax=0, mode="c-clock"):

@@ -66,6 +66,11 @@ FLC_API uint64_t flc_launch_count(void);
  *   "proj.bwd"      backward: 2 nine-phase splat, 1 shared-memory atomics,
  *                   3 gather per pixel, 4 splat by column segments; automatic:
  *                   4 where one round of its items fills the thread block, else 2
+ *                   (these four are the earlier kernels, run with "proj.legacy")
+ *   "proj.legacy"   1: the earlier projector and fused-MLEM kernels instead of the
+ *                   lean forward / backward pair (for comparison)
+ *   "proj.band"     1: the row-band backward (no global atomics; it runs by itself
+ *                   where a slice image does not fit in shared memory) at every size
  * Test hooks of the direct cone's bounded waits (for failure-path tests):
  *   "cone.test_wait_limit"  polls before a TMA-plane wait gives up (default 2^26)
  *   "cone.test_skip_load"   k > 0: the load of the k-th staged plane of every
@@ -161,18 +166,20 @@ FLC_API int flc_mlem_static(float* C, const float* atten, const float* em, const
                     const float* I, int64_t n_iter, double beta, double delta,
                     int64_t A, int64_t B, int64_t R, int64_t H, int64_t W, void* stream);
 
-/* MLEM of P independent problems at once (P <= 32; for instance the elements
- * of one volume, or several volumes of one slice size): problem i has C[i]
- * (R, B[i], H, W), atten[i] (A[i], B[i], H, W), em[i] (A[i], R), theta[i]
- * (A[i]) and I[i] (A[i], B[i], W), all device pointers held in host arrays
- * of length P; R, H, W are shared.  Each C[i] is updated in place by n_iter
- * iterations of flc_mlem.  One persistent launch per iteration covers every
- * problem: clusters of CTAs take (problem, slice) items from a device
- * counter, largest angle counts first, and for each item run the forward of
- * their angles, the backward of the same angles and the update.  Workspace:
- * flc_mlem_multi_workspace_bytes (256-byte aligned).  Issues no host copies
- * (the problem table travels as a kernel argument).  No counterpart in the
- * reference, which runs mlem_cuda_batch once per element
+/* MLEM of P independent problems at once (P <= 64; for instance the elements
+ * of one volume, or several volumes): problem i has C[i] (R, B[i], H, W),
+ * atten[i] (A[i], B[i], H, W), em[i] (A[i], R), theta[i] (A[i]) and I[i]
+ * (A[i], B[i], W), all device pointers held in host arrays of length P; R,
+ * H, W are shared (flc_mlem_multi_sizes: H[i], W[i] per problem).  Each C[i]
+ * is updated in place by n_iter iterations of flc_mlem.  One persistent
+ * launch per iteration covers every problem: clusters of CTAs take (problem,
+ * slice) items from a device counter, the largest work per item (angles x
+ * slice area) first, and for each item run the forward of their angles, the
+ * backward of the same angles and the update; shared memory is sized for
+ * the largest slice, which must fit the lean kernels.  Workspace:
+ * flc_mlem_multi[_sizes]_workspace_bytes (256-byte aligned).  Issues no host
+ * copies (the problem table travels as a kernel argument).  No counterpart
+ * in the reference, which runs mlem_cuda_batch once per element and volume
  * (FL/torch_recon.py:50-99, FL/example/demo.py:177-232). */
 FLC_API size_t flc_mlem_multi_workspace_bytes(int64_t P, const int64_t* A, const int64_t* B,
                                               int64_t R, int64_t H, int64_t W);
@@ -181,6 +188,15 @@ FLC_API int flc_mlem_multi(int64_t P, float* const* C, const float* const* atten
                            const float* const* I, const int64_t* A, const int64_t* B, int64_t R,
                            int64_t H, int64_t W, int64_t n_iter, double beta, double delta,
                            void* workspace, size_t workspace_bytes, void* stream);
+FLC_API size_t flc_mlem_multi_sizes_workspace_bytes(int64_t P, const int64_t* A,
+                                                    const int64_t* B, int64_t R,
+                                                    const int64_t* H, const int64_t* W);
+FLC_API int flc_mlem_multi_sizes(int64_t P, float* const* C, const float* const* atten,
+                                 const float* const* em, const float* const* theta,
+                                 const float* const* I, const int64_t* A, const int64_t* B,
+                                 int64_t R, const int64_t* H, const int64_t* W, int64_t n_iter,
+                                 double beta, double delta, void* workspace,
+                                 size_t workspace_bytes, void* stream);
 
 /* ---------------------------------------------------------------------
  * Per-angle attenuation maps (rotation + mu assembly + incident scan +

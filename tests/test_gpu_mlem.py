@@ -94,7 +94,10 @@ def test_huber_api():
 
 @pytest.mark.parametrize("shapes,beta", [([(12, 4, 32), (30, 3, 32), (7, 5, 32)], 1e-3),
                                          ([(24, 16, 64), (24, 16, 64), (24, 16, 64)], 0.0),
-                                         ([(9, 2, 20)], 1e-3)])
+                                         ([(9, 2, 20)], 1e-3),
+                                         # uneven slice sizes in one launch
+                                         # (angle counts that keep each problem well posed)
+                                         ([(24, 3, 40), (16, 2, 24), (36, 4, 64), (48, 2, 96)], 1e-3)])
 def test_mlem_multi_matches_per_problem(shapes, beta):
     """flc_mlem_multi (one persistent launch per iteration for all problems)
     against flc_mlem per problem and the oracle."""

@@ -58,17 +58,44 @@ def test_offset_path_sum_matches_fp64_composition(deg):
     assert rel_err(got, ref) < 1e-5
 
 
+def test_small_offset_converges_to_the_plain_path():
+    """As the offset shrinks, the rotate / path sum / rotate-back composition
+    (FP64) approaches the plain path sum.  The bilinear rotations smear mu by
+    a fraction of a pixel near the slice edges, where the plain result is 1
+    on the detector side: there the difference shrinks only in proportion to
+    the offset (0.25 at 0.6 degrees on a 24-pixel slice), so the bound is on
+    the mean and on the interior."""
+    from fl_correction_b200.detector_mask import generate_detector_mask
+    from fl_correction_b200.torch_functions import coef_xrf
+    from oracle import oracle as O
+    from tests.helpers import atten_param
+    rng = np.random.default_rng(12)
+    cf = coef_xrf(atten_param())
+    frac = (rng.random((3, 4, 24, 24)) * 0.5).astype(np.float32)
+    mask = generate_detector_mask(13.309, 13.309, 24).astype(np.float32)
+    mu = np.einsum("ij,jshw->ishw", np.asarray(cf, np.float64), frac.astype(np.float64))
+    plain = np.exp(-O.cone_beam(mu, mask))
+    means = []
+    for deg in (5.0, 0.6, 0.2):
+        d = np.abs(_oracle_offset(frac, cf, mask, float(np.float32(deg / 180 * np.pi))) - plain)
+        means.append(d.mean())
+        if deg <= 0.6:
+            assert d[..., 3:-3, 3:-3].max() < 0.05
+    assert means[0] > means[1] > means[2] and means[2] < 0.003
+
+
 @pytest.mark.gpu
-def test_small_offset_approaches_the_plain_path():
+def test_small_offset_takes_the_rotated_branch():
+    """0.6 degrees (just above the 1e-2 rad threshold of the plain branch)
+    against the FP64 composition."""
     import torch
     from fl_correction_b200.detector_mask import generate_detector_mask
-    from fl_correction_b200.torch_functions import torch_xrf_atten_3D
+    from fl_correction_b200.torch_functions import coef_xrf, torch_xrf_atten_3D
     from tests.helpers import atten_param
     rng = np.random.default_rng(12)
     p = atten_param()
-    frac = torch.tensor((rng.random((3, 4, 24, 24)) * 0.5).astype(np.float32), device="cuda")
+    frac = (rng.random((3, 4, 24, 24)) * 0.5).astype(np.float32)
     mask = generate_detector_mask(13.309, 13.309, 24)
-    plain = torch_xrf_atten_3D(frac, p, mask)
-    near = torch_xrf_atten_3D(frac, p, mask, detector_offset_angle=0.6)    # just above 1e-2 rad
-    # a 0.6 degree turn moves the far corner of a 24-pixel slice by ~0.2 pixel
-    assert rel_err(near, plain) < 0.05
+    near = torch_xrf_atten_3D(torch.tensor(frac, device="cuda"), p, mask, detector_offset_angle=0.6)
+    ref = _oracle_offset(frac, coef_xrf(p), mask.astype(np.float32), float(np.float32(0.6 / 180 * np.pi)))
+    assert rel_err(near, ref) < 1e-5

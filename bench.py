@@ -83,12 +83,16 @@ def mlem_bytes_per_iter(A, S, H, W, R=1):
     return fwd + bwd + upd
 
 
-# DRAM bytes measured by ncu on small cases of the same kernels: the spectral
-# cone's five kernels move 54.3 MB per 128^3 volume (325.8 MB read + write
-# for 6 volumes); a fused MLEM iteration moves 1.092 bytes per attenuation
-# byte (27.53 MB for 25.17 MB).
+# DRAM bytes measured by ncu: the spectral cone's five kernels move 54.3 MB
+# per 128^3 volume (325.8 MB read + write for 6 volumes); an MLEM iteration
+# at the benchmark's shape (120 angles x 128 slices of 128^2, one element)
+# moves 1.026 GB in the lean forward and 1.023 GB in the lean backward,
+# 1.018 bytes per attenuation byte.
 CONE_DRAM_BYTES_PER_VOLUME = 325.8e6 / 6
-MLEM_DRAM_PER_ATTEN_BYTE = 27.53e6 / (24 * 16 * 128 * 128 * 4)
+MLEM_DRAM_PER_ATTEN_BYTE = (1.026144e9 + 1.023237e9) / (2 * 120 * 128 * 128 * 128 * 4)
+# FP32 FMA rate measured on this pool's B200 (a chain-of-FMAs probe over
+# 148 x 8 CTAs of 256 threads)
+FP32_PEAK_TFLOPS = 72.5
 
 
 def smooth_even(n):
@@ -295,7 +299,7 @@ def run_ours(args, rank, world, device):
     cone_launches = len(cone_ev)
     cone_avg_ms = t_cone / max(cone_launches, 1)
     vols_per_launch = n_cone / max(cone_launches, 1)
-    fp32_peak = 148 * 128 * 2 * 1965e6 / 1e12
+    fp32_peak = FP32_PEAK_TFLOPS
     mlem_iters = sum(v for _, _, v in mlem_ev)      # element-iterations timed
     bytes_it = mlem_bytes_per_iter(A, N, N, N)
     proj_gbs = bytes_it * mlem_iters / (t_mlem * 1e-3) / 1e9 if t_mlem else None
@@ -323,15 +327,17 @@ def run_ours(args, rank, world, device):
         "corrected_proj_gbs": round(proj_gbs, 1) if proj_gbs else None,
         "corrected_proj_pct_hbm": round(100 * proj_gbs / hbm, 1) if proj_gbs else None,
         "time_share": {"cone (spectral, 5 kernels per launch)": round(cone_share, 3),
-                       "mlem (sens + fused iterations)": round(t_mlem / ms, 3) if ms else None},
+                       "mlem (sensitivity + iterations)": round(t_mlem / ms, 3) if ms else None},
         # the dominant kernel: the fused MLEM iteration (with the sensitivity
         # backward of each attenuation rebuild)
         "roofline": {
-            "kernel": "mlem_iter_kernel (+ sensitivity backward)", "bound": "hbm",
+            "kernel": "MLEM iteration: proj_fwd2_kernel (+ ratio) and proj_bwd2_kernel (+ update), "
+                      "with the sensitivity backward of each rebuild", "bound": "hbm",
             "achieved": round(proj_gbs, 1) if proj_gbs else None, "peak": hbm, "unit": "GB/s",
             "frac": round(proj_gbs / hbm, 3) if proj_gbs else None,
-            "traffic": round(MLEM_DRAM_PER_ATTEN_BYTE * A * N ** 3 * 4),
-            "traffic_note": "per element-iteration: ncu dram bytes of a 24x16x128^2 iteration per attenuation byte, scaled",
+            "traffic": round(MLEM_DRAM_PER_ATTEN_BYTE * 2 * A * N ** 3 * 4),
+            "traffic_note": "per element-iteration: ncu dram read + write of the lean forward and backward "
+                            "at this shape (the attenuation is read twice)",
             "peak_kind": peak_kind,
             "algorithmic_unit": "%.4g B per element-iteration (fwd + bwd + update at the reference API boundary)" % bytes_it,
         },
@@ -344,7 +350,7 @@ def run_ours(args, rank, world, device):
             "frac": round(spec * vols_per_launch / (cone_avg_ms * 1e-3) / 1e12 / fp32_peak, 3),
             "traffic": round(CONE_DRAM_BYTES_PER_VOLUME * vols_per_launch * (N / 128) ** 3),
             "traffic_note": "ncu dram read+write of the five kernels on 6 volumes of 128^3, per volume, times volumes per launch",
-            "peak_kind": "nominal FP32 (148 SM x 128 lanes x 2 x 1965 MHz); no measured FP32 peak",
+            "peak_kind": "measured FP32 FMA rate (chain-of-FMAs probe on this pool's B200)",
             "algorithmic_unit": "spectral FLOPs (depth correlation + 2-D FFTs, %dx%d padded planes) = %.3g per volume"
                                 % (nz_ny[0], nz_ny[1], spec),
             "launches": cone_launches, "avg_ms": round(cone_avg_ms, 4),
@@ -612,7 +618,7 @@ def run_grad(args, device):
     from fl_correction_b200 import _lib, phantoms
     from fl_correction_b200.detector_mask import generate_detector_mask
     from fl_correction_b200.grad_recon import GradientRecon, gradient_loss
-    from tests import torch_model as TM
+    from fl_correction_b200 import torch_composition as TM
     wl = phantoms.make_workload(args.config)
     N, L, A = wl.N, len(wl.elements), len(wl.angles)
     mask = generate_detector_mask(wl.mask_angle, wl.mask_angle, N)

@@ -552,14 +552,15 @@ int cone_sep_launch(const float* mu, const float* U, const float* Vw, float* out
 }
 
 // Cone path sum with scratch for the spectral form: the spectral kernels run
-// when the "cone.variant" knob allows them (0 automatic, 4 spectral) and the
-// shape and scratch fit; otherwise cone_sep_launch.
+// when the "cone.variant" knob allows them (0 automatic, 4 spectral, 5
+// spectral with split plane transforms) and the shape and scratch fit;
+// otherwise cone_sep_launch.
 int cone_launch_ws(const float* mu, const float* U, const float* Vw, float* out, int64_t Vn,
                    int64_t Z, int64_t X, int64_t Y, int64_t Mz, int64_t Mx, int64_t My, int mode,
                    int L, int a_base, int64_t out_a_stride, int64_t out_l_stride, void* ws,
                    size_t ws_bytes, cudaStream_t st) {
     const int64_t var = tune(kTuneConeVariant);
-    if (ws && (var == 0 || var == 4)) {
+    if (ws && (var == 0 || var == 4 || var == 5)) {
         int r = cone_fft_launch(mu, U, Vw, out, Vn, Z, X, Y, Mz, Mx, My, mode, L, a_base,
                                 out_a_stride, out_l_stride, ws, ws_bytes, st);
         if (r != FLC_ERR_UNSUPPORTED) return r;

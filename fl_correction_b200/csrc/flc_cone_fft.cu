@@ -30,6 +30,10 @@
 //                       exp(-res) in the reference layout
 //   fft_apply_kernel  : beam layout modes: exp(-res) multiplied (or stored)
 //                       into out[l][a][z][Y-1-y][x] through a tiled transpose
+// Planes whose padded transform does not fit one CTA's shared memory twice
+// (beyond about 150^2) replace fft_fwd_kernel by fft_fwd_rows_kernel +
+// fft_cols_kernel and fft_inv_kernel by fft_cols_kernel + fft_inv_rows_kernel:
+// the same transforms in two passes through the spectra buffer.
 // All transforms are Stockham autosort passes (radix 4, 2, 3, 5) over the
 // sequences held in shared memory, ping-ponging between two buffers.
 
@@ -56,7 +60,14 @@ struct FftGeom {
     int Z, X, Y, Mz, Mx, My;
     int Nz, Ny, Nyh, NP;   // padded sizes; NP = Nz * Nyh spectrum points per plane
     Radices rz, ry;
+    int split;             // 1: plane transforms in two passes through the spectra buffer
 };
+
+// Split transforms (planes too large for one CTA's shared memory): a row CTA
+// transforms kRowPairs pairs of rows, a column CTA kColK columns.
+constexpr int kRowPairs = 16;
+constexpr int kColK = 16;
+constexpr int kSplitThreads = 512;
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
     return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
@@ -288,6 +299,130 @@ fft_fwd_kernel(const float* __restrict__ mu, const float2* __restrict__ Tzg,
     for (int i = threadIdx.x; i < g.NP; i += blockDim.x) dst[i] = R2[i];
 }
 
+// ---------------------------------------------------------------------------
+// Split transforms.  The one-CTA-per-plane kernels above hold a padded plane
+// twice in shared memory, which caps the plane near 150^2.  For larger planes
+// the same 2-D transforms run in two passes through the spectra buffer S
+// (layout [v][x][kz][ky], as the one-pass kernels write it): row CTAs
+// transform kRowPairs pairs of rows along y and write the unpacked half
+// spectra, column CTAs transform kColK columns along z in place; the inverse
+// runs columns first, then rows.  The arithmetic per sequence is the one-pass
+// kernels' (the same passes, twiddles and packing), so the results agree.
+// ---------------------------------------------------------------------------
+
+// Forward, rows: grid (X, Vn, ceil(npairs / kRowPairs)).  Rows 2q, 2q+1 of
+// source plane p as one complex sequence, transformed and unpacked into rows
+// z of S; the CTAs of the first row batch also zero the rows Z .. Nz-1.
+__global__ void __launch_bounds__(kSplitThreads)
+fft_fwd_rows_kernel(const float* __restrict__ mu, const float2* __restrict__ Tyg,
+                    float2* __restrict__ S, FftGeom g) {
+    extern __shared__ __align__(16) float2 sm[];
+    const int Ny = g.Ny, Nyh = g.Nyh, Z = g.Z, X = g.X, Y = g.Y;
+    float2* A = sm;
+    float2* B = A + kRowPairs * Ny;
+    float2* Ty = B + kRowPairs * Ny;
+    const int p = blockIdx.x, v = blockIdx.y;
+    const int npairs = (Z + 1) / 2;
+    const int q0 = blockIdx.z * kRowPairs, nq = min(kRowPairs, npairs - q0);
+    const float rNy = 1.f / (float)Ny, rNyh = 1.f / (float)Nyh;
+    for (int m = threadIdx.x; m < Ny; m += blockDim.x) Ty[m] = Tyg[m];
+    const float* src = mu + (int64_t)v * Z * X * Y + (int64_t)p * Y;
+    const int64_t zs = (int64_t)X * Y;
+    for (int i = threadIdx.x; i < nq * Ny; i += blockDim.x) {
+        const int qq = div_small(i, rNy), y = i - qq * Ny;
+        const int za = 2 * (q0 + qq), zb = za + 1;
+        const bool in = y < Y;
+        B[i] = make_float2(in ? __ldg(src + za * zs + y) : 0.f,
+                           (in && zb < Z) ? __ldg(src + zb * zs + y) : 0.f);
+    }
+    __syncthreads();
+    const float2* R1 = fft_batch(B, A, g.ry, nq, Ny, 1, Ty, -1.f, false);
+    float2* dst = S + ((int64_t)v * X + p) * g.NP;
+    const int z0 = 2 * q0, z1 = min(Z, 2 * (q0 + nq));
+    for (int i = threadIdx.x; i < (z1 - z0) * Nyh; i += blockDim.x) {
+        const int zz = div_small(i, rNyh), k = i - zz * Nyh;
+        const int z = z0 + zz;
+        const float2* Zq = R1 + ((z >> 1) - q0) * Ny;
+        const float2 zk = Zq[k], zn = Zq[k == 0 ? 0 : Ny - k];
+        dst[(int64_t)z * Nyh + k] = (z & 1) ? make_float2(0.5f * (zk.y + zn.y), -0.5f * (zk.x - zn.x))
+                                            : make_float2(0.5f * (zk.x + zn.x), 0.5f * (zk.y - zn.y));
+    }
+    if (blockIdx.z == 0)
+        for (int i = Z * Nyh + threadIdx.x; i < g.NP; i += blockDim.x) dst[i] = make_float2(0.f, 0.f);
+}
+
+// Columns along z, in place in S (grid (X, Vn, ceil(Nyh / kColK))); sg = -1
+// forward, +1 inverse.
+__global__ void __launch_bounds__(kSplitThreads)
+fft_cols_kernel(float2* __restrict__ S, const float2* __restrict__ Tzg, float sg, FftGeom g) {
+    extern __shared__ __align__(16) float2 sm[];
+    const int Nz = g.Nz, Nyh = g.Nyh;
+    const int sp = Nz + 1;                 // odd sequence pitch: the transposing
+                                           // accesses spread over the banks
+    float2* A = sm;
+    float2* B = A + kColK * sp;
+    float2* Tz = B + kColK * sp;
+    const int p = blockIdx.x, v = blockIdx.y;
+    const int k0 = blockIdx.z * kColK, nk = min(kColK, Nyh - k0);
+    for (int m = threadIdx.x; m < Nz; m += blockDim.x) Tz[m] = Tzg[m];
+    float2* pl = S + ((int64_t)v * g.X + p) * g.NP;
+    // element (z, kk) of the batch at A[kk * sp + z]; loads run along ky
+    for (int i = threadIdx.x; i < Nz * nk; i += blockDim.x) {
+        const int z = i / nk, kk = i - z * nk;
+        A[kk * sp + z] = pl[(int64_t)z * Nyh + k0 + kk];
+    }
+    __syncthreads();
+    const float2* R = fft_batch(A, B, g.rz, nk, sp, 1, Tz, sg, false);
+    for (int i = threadIdx.x; i < Nz * nk; i += blockDim.x) {
+        const int z = i / nk, kk = i - z * nk;
+        pl[(int64_t)z * Nyh + k0 + kk] = R[kk * sp + z];
+    }
+}
+
+// Inverse, rows: grid (X, Vn, ceil(npairs / kRowPairs)).  Rows 2q, 2q+1 of
+// plane x's (z, ky) half spectra as one Hermitian-extended complex sequence,
+// transformed along y; writes res (mode 0) or exp(-res) (mode 1) in the
+// reference layout.
+__global__ void __launch_bounds__(kSplitThreads)
+fft_inv_rows_kernel(const float2* __restrict__ S, const float2* __restrict__ Tyg,
+                    float* __restrict__ out, int mode, FftGeom g) {
+    extern __shared__ __align__(16) float2 sm[];
+    const int Ny = g.Ny, Nyh = g.Nyh, Z = g.Z, X = g.X, Y = g.Y;
+    float2* A = sm;
+    float2* B = A + kRowPairs * Ny;
+    float2* Ty = B + kRowPairs * Ny;
+    const int x = blockIdx.x, v = blockIdx.y;
+    const int npairs = (Z + 1) / 2;
+    const int q0 = blockIdx.z * kRowPairs, nq = min(kRowPairs, npairs - q0);
+    const float rNy = 1.f / (float)Ny;
+    for (int m = threadIdx.x; m < Ny; m += blockDim.x) Ty[m] = Tyg[m];
+    const float2* R1 = S + ((int64_t)v * X + x) * g.NP;
+    const int half = Ny / 2;
+    for (int i = threadIdx.x; i < nq * Ny; i += blockDim.x) {
+        const int qq = div_small(i, rNy), k = i - qq * Ny;
+        const int za = 2 * (q0 + qq), zb = za + 1;
+        const bool up = k > half;
+        const int kk = up ? Ny - k : k;
+        float2 a = R1[(int64_t)za * Nyh + kk];
+        float2 b = zb < Z ? R1[(int64_t)zb * Nyh + kk] : make_float2(0.f, 0.f);
+        if (kk == 0 || kk == half) { a.y = 0.f; b.y = 0.f; }
+        if (up) { a.y = -a.y; b.y = -b.y; }
+        A[i] = make_float2(a.x - b.y, a.y + b.x);
+    }
+    __syncthreads();
+    const float2* R2 = fft_batch(A, B, g.ry, nq, Ny, 1, Ty, 1.f, false);
+    const float scale = 1.f / ((float)g.Nz * (float)Ny);
+    float* ov = out + (int64_t)v * Z * X * Y + (int64_t)x * Y;
+    const int z0 = 2 * q0, z1 = min(Z, 2 * (q0 + nq));
+    for (int i = threadIdx.x; i < (z1 - z0) * Y; i += blockDim.x) {
+        const int zz = div_small(i, 1.f / (float)Y), y = i - zz * Y;
+        const int z = z0 + zz;
+        const float2 c = R2[((z >> 1) - q0) * Ny + y];
+        const float r = ((z & 1) ? c.y : c.x) * scale;
+        ov[(int64_t)z * X * Y + y] = mode == 1 ? expf(-r) : r;
+    }
+}
+
 // R_x(k) = sum_{d < min(Mx, X - x)} G_d(k) P_{x+d}(k), over P in place
 // (grid (ceil(NP / 16), Vn), kCorrWarps warps).  The two half-warps take the
 // same 16 frequencies (one per lane) and split each group's depth range, so
@@ -500,6 +635,14 @@ size_t plane_smem(const FftGeom& g) {
     return sizeof(float2) * (2 * (size_t)g.NP + g.Nz + g.Ny);
 }
 
+size_t rows_smem(const FftGeom& g) {
+    return sizeof(float2) * (2 * (size_t)kRowPairs * g.Ny + g.Ny);
+}
+
+size_t cols_smem(const FftGeom& g) {
+    return sizeof(float2) * (2 * (size_t)kColK * (g.Nz + 1) + g.Nz);
+}
+
 size_t corr_smem(const FftGeom& g) {
     return sizeof(float2) * kCorrK * ((size_t)(g.X + g.Mx + 16) + (g.Mx + 8));
 }
@@ -519,7 +662,9 @@ bool fft_geom(int64_t Z, int64_t X, int64_t Y, int64_t Mz, int64_t Mx, int64_t M
     g->rz = radices(g->Nz);
     g->ry = radices(g->Ny);
     const size_t cap = (size_t)max_smem_optin();
-    return plane_smem(*g) <= cap && corr_smem(*g) <= cap;
+    if (corr_smem(*g) > cap) return false;
+    g->split = plane_smem(*g) > cap || tune(kTuneConeVariant) == 5;
+    return !g->split || (rows_smem(*g) <= cap && cols_smem(*g) <= cap);
 }
 
 struct FftWs {
@@ -570,23 +715,49 @@ int cone_fft_launch(const float* mu, const float* U, const float* Vw, float* out
     const size_t fsm = sizeof(double2) * (size_t)(g.Nz + g.Nyh);
     fft_filter_kernel<<<(unsigned)(g.Mx + 1), 256, fsm, st>>>(U, Vw, w.G, w.Tz, w.Ty, g);
     FLC_TRY(check_launch("fft_filter_kernel"));
-    const size_t psm = plane_smem(g);
-    FLC_TRY_CUDA(cudaFuncSetAttribute((const void*)fft_fwd_kernel,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psm));
-    FLC_TRY_CUDA(cudaFuncSetAttribute((const void*)fft_inv_kernel,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psm));
-    fft_fwd_kernel<<<dim3((unsigned)g.X, (unsigned)Vn), kFftThreads, psm, st>>>(mu, w.Tz, w.Ty,
-                                                                               w.S, g);
-    FLC_TRY(check_launch("fft_fwd_kernel"));
+    const size_t psm = plane_smem(g), rsm = rows_smem(g), csm_t = cols_smem(g);
+    const unsigned nrb = (unsigned)ceil_div((g.Z + 1) / 2, kRowPairs);
+    const unsigned ncb = (unsigned)ceil_div(g.Nyh, kColK);
+    if (g.split) {
+        FLC_TRY_CUDA(cudaFuncSetAttribute((const void*)fft_fwd_rows_kernel,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsm));
+        FLC_TRY_CUDA(cudaFuncSetAttribute((const void*)fft_inv_rows_kernel,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsm));
+        FLC_TRY_CUDA(cudaFuncSetAttribute((const void*)fft_cols_kernel,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm_t));
+        fft_fwd_rows_kernel<<<dim3((unsigned)g.X, (unsigned)Vn, nrb), kSplitThreads, rsm, st>>>(
+            mu, w.Ty, w.S, g);
+        FLC_TRY(check_launch("fft_fwd_rows_kernel"));
+        fft_cols_kernel<<<dim3((unsigned)g.X, (unsigned)Vn, ncb), kSplitThreads, csm_t, st>>>(
+            w.S, w.Tz, -1.f, g);
+        FLC_TRY(check_launch("fft_cols_kernel"));
+    } else {
+        FLC_TRY_CUDA(cudaFuncSetAttribute((const void*)fft_fwd_kernel,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psm));
+        FLC_TRY_CUDA(cudaFuncSetAttribute((const void*)fft_inv_kernel,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psm));
+        fft_fwd_kernel<<<dim3((unsigned)g.X, (unsigned)Vn), kFftThreads, psm, st>>>(mu, w.Tz, w.Ty,
+                                                                                   w.S, g);
+        FLC_TRY(check_launch("fft_fwd_kernel"));
+    }
     const size_t csm = corr_smem(g);
     FLC_TRY_CUDA(cudaFuncSetAttribute((const void*)fft_corr_kernel,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
     fft_corr_kernel<<<dim3((unsigned)ceil_div(g.NP, kCorrK), (unsigned)Vn), kCorrWarps * 32, csm,
                       st>>>(w.S, w.G, g);
     FLC_TRY(check_launch("fft_corr_kernel"));
-    fft_inv_kernel<<<dim3((unsigned)g.X, (unsigned)Vn), kFftThreads, psm, st>>>(
-        w.S, w.Tz, w.Ty, mode >= 2 ? w.res : out, mode >= 2 ? 0 : mode, g);
-    FLC_TRY(check_launch("fft_inv_kernel"));
+    if (g.split) {
+        fft_cols_kernel<<<dim3((unsigned)g.X, (unsigned)Vn, ncb), kSplitThreads, csm_t, st>>>(
+            w.S, w.Tz, 1.f, g);
+        FLC_TRY(check_launch("fft_cols_kernel"));
+        fft_inv_rows_kernel<<<dim3((unsigned)g.X, (unsigned)Vn, nrb), kSplitThreads, rsm, st>>>(
+            w.S, w.Ty, mode >= 2 ? w.res : out, mode >= 2 ? 0 : mode, g);
+        FLC_TRY(check_launch("fft_inv_rows_kernel"));
+    } else {
+        fft_inv_kernel<<<dim3((unsigned)g.X, (unsigned)Vn), kFftThreads, psm, st>>>(
+            w.S, w.Tz, w.Ty, mode >= 2 ? w.res : out, mode >= 2 ? 0 : mode, g);
+        FLC_TRY(check_launch("fft_inv_kernel"));
+    }
     if (mode >= 2) {
         dim3 grid((unsigned)ceil_div(g.Y, 32), (unsigned)ceil_div(g.X, 32), (unsigned)(Vn * g.Z));
         fft_apply_kernel<<<grid, dim3(32, 8), 0, st>>>(w.res, out, mode, L, a_base, out_a_stride,

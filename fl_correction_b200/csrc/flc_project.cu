@@ -1000,6 +1000,9 @@ __device__ void bwd_splat_angles(const float* __restrict__ atten, const float* _
             const int pw = ph >> 1, ps = ph & 1;
             const int nw = (W - pw + 2) / 3, nsp = (nseg - ps + 1) / 2;
             const int items = nw * nsp;
+            // (dynamic fetching of the items by warps, with shorter segments,
+            // measured slower here: 1.49-1.58 against 1.45 ms; the band
+            // kernel, whose line windows differ in length, uses it)
             for (int it = threadIdx.x; it < items; it += blockDim.x) {
                 const int k = it / nw, cw = it - k * nw;
                 const int h0 = (ps + 2 * k) * seg;
@@ -1215,6 +1218,9 @@ proj_bwd_band_kernel(const float* __restrict__ atten, const float* __restrict__ 
     float* sq = sframe + frame_floats(R, nrow, W, ncopy);        // [2][R][W]
     float* srow = sframe + ((threadIdx.x >> 5) % ncopy) * 2 * R * (nrow + W);
     float* scol = srow + 2 * R * W;
+    __shared__ int s_ctr[2][6];             // per-phase item counters by angle parity
+    if (threadIdx.x < 12) s_ctr[threadIdx.x / 6][threadIdx.x % 6] = 0;
+    const int lane = threadIdx.x & 31;
     for (int i = threadIdx.x; i < R * img; i += blockDim.x) sacc[i] = 0.f;
     for (int i = threadIdx.x; i < frame_floats(R, nrow, W, ncopy); i += blockDim.x) sframe[i] = 0.f;
     if (a0 < a1) stage_q(sq + (a0 & 1) * R * W, ratio, em, a0, b, B, R, W);
@@ -1250,15 +1256,28 @@ proj_bwd_band_kernel(const float* __restrict__ atten, const float* __restrict__ 
             const int span = (int)((xhi - xlo) * fabsf(islope)) + 9;
             nsegs = min(nsegs, (span + seg - 1) / seg);
         }
-        // (Longer segments that fit a phase's items in one round of the block
-        // measured slower, 14.1 against 12.3 ms at 180 angles x 64 slices of
-        // 256^2: the windows of the lines differ in length, and the phase
-        // waits for the longest.)
+        // (180 angles x 64 slices of 256^2: 9.43 ms with 6-sample segments
+        // fetched dynamically, 9.87 / 9.98 ms with 4 / 8; 12.5 ms with
+        // 16-sample segments assigned statically, 14.1 ms with longer ones
+        // fitting one round of the block -- the line windows differ in length
+        // and a static phase waits for the longest; 9.4 ms for the
+        // global-atomic kernel this replaced.)
+        if (threadIdx.x < 6) s_ctr[(a + 1) & 1][threadIdx.x] = 0;
         for (int ph = 0; ph < 6; ++ph) {
             const int pw = ph >> 1, ps = ph & 1;
             const int nl = (nlines - pw + 2) / 3, nsp = (nsegs - ps + 1) / 2;
             const int items = nl * nsp;
-            for (int it = threadIdx.x; it < items; it += blockDim.x) {
+            // the phase's items touch disjoint pixels, so any warp may take
+            // any of them: the warps take 32 at a time from the phase's
+            // counter, and a warp whose lines have short windows in the band
+            // takes more (blockDim.x is a multiple of 32)
+            for (;;) {
+                int base = 0;
+                if (lane == 0) base = atomicAdd(&s_ctr[a & 1][ph], 32);
+                base = __shfl_sync(0xffffffffu, base, 0);
+                if (base >= items) break;
+                const int it = base + lane;
+                if (it >= items) continue;
                 const int k = it / nl, cl = it - k * nl;
                 const int L = pw + 3 * cl;
                 float plo, phi;
@@ -1701,6 +1720,9 @@ size_t band_smem(int64_t R, int64_t hb, int64_t W, int ncopy) {
                             2 * R * W);
 }
 
+// Segment length of the band walk (the warps fetch items dynamically).
+constexpr int kSegBand = 6;
+
 int band_height(int64_t R, int64_t H, int64_t W, int* ncopy_out) {
     const size_t cap = (size_t)max_smem_optin();
     if (band_smem(R, 1, W, 1) > cap) return 0;
@@ -1736,7 +1758,7 @@ int band_launch(const float* atten, const float* ratio, const float* em, const f
     const void* fn = R == 1 ? (const void*)proj_bwd_band_kernel<1> : (const void*)proj_bwd_band_kernel<0>;
     Plan p = plan_cluster(fn, A, (int64_t)nband * B, smem, kT2);
     int iA = (int)A, iB = (int)B, iR = (int)R, iH = (int)H, iW = (int)W, apc = p.apc, ihb = hb;
-    int seg = 16;
+    int seg = kSegBand;
     void* args[] = {(void*)&atten, (void*)&ratio, (void*)&em, (void*)&theta, (void*)&out,
                     (void*)&Cin, (void*)&sens, &iA, &iB, &iR, &iH, &iW, &apc, &ihb, &seg,
                     (void*)&ncopy, &clamp_min, &mode, &beta, &delta};

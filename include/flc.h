@@ -60,8 +60,10 @@ FLC_API uint64_t flc_launch_count(void);
  * autotuner in fl_correction_b200/tune.py sets them).  Names:
  *   "proj.cluster"  CTAs per slice cluster, backward/MLEM kernels (1..8)
  *   "proj.apc"      angles per CTA, projector kernels
- *   "cone.variant"  1: TMA 16x8 tile, 2: TMA 8x4 tile, 3: plain kernel, 4: spectral
- *                   (where scratch is given; automatic: spectral where it fits)
+ *   "cone.variant"  1: TMA 16x8 tile, 2: TMA 8x4 tile, 3: plain kernel, 4: spectral,
+ *                   5: spectral with the plane transforms split into row and column
+ *                   passes (where scratch is given; automatic: spectral where it fits,
+ *                   split where a padded plane does not fit one CTA twice)
  *   "atten.chunk"   angles per attenuation-pipeline pass
  *   "proj.bwd"      backward: 2 nine-phase splat, 1 shared-memory atomics,
  *                   3 gather per pixel, 4 splat by column segments; automatic:

@@ -153,12 +153,13 @@ def test_spectral_cone_matches_oracle(n_a, L, S, N, mask_args):
     outs = {}
     old = tune.get_knob("cone.variant")
     try:
-        for variant in (4, 3):
+        # 4: spectral, 5: spectral with the split (two-pass) plane transforms, 3: direct
+        for variant in (4, 5, 3):
             tune.set_knob("cone.variant", variant)
             out = T(base)
             _lib.call("flc_cone_atten_apply_ws", _lib.ptr(x), _lib.ptr(U), _lib.ptr(V),
                       _lib.ptr(out), n_a, L, S, N, N, A, a0, Mz, Mx, My,
-                      _lib.ptr(ws) if variant == 4 else None, nb, _lib.stream())
+                      _lib.ptr(ws) if variant != 3 else None, nb, _lib.stream())
             outs[variant] = out.cpu().numpy()
     finally:
         tune.set_knob("cone.variant", old)
@@ -169,8 +170,34 @@ def test_spectral_cone_matches_oracle(n_a, L, S, N, mask_args):
             r = res[al * L + l]
             exp[l, a0 + al] *= np.exp(-r[:, :, ::-1].transpose(0, 2, 1))
     assert rel_err(outs[4], exp) < TOL_MAP
+    assert rel_err(outs[5], exp) < TOL_MAP
     assert rel_err(outs[3], exp) < TOL_MAP
     assert np.array_equal(outs[4][:, 0], base[:, 0])   # angles outside the chunk untouched
+    assert np.array_equal(outs[5][:, 0], base[:, 0])
+
+
+def test_spectral_cone_large_planes_split():
+    """200 x 200 planes (216^2 padded) do not fit one CTA's shared memory
+    twice: the spectral form runs its plane transforms in two passes by
+    itself.  cal_atten_cuda (reference layout) against the oracle and the
+    direct kernel."""
+    from fl_correction_b200 import tune
+    from fl_correction_b200.cuda_lib import atten_cuda as AC
+    rng = np.random.default_rng(21)
+    mask = generate_detector_mask(13.309, 13.309, 6).astype(np.float32)
+    mu = (rng.random((1, 200, 6, 200)) * 0.05).astype(np.float32)    # (K, Z, X, Y)
+    Mz, Mx, My = mask.shape
+    assert _lib.query("flc_cone_fft_workspace_bytes", 1, 200, 6, 200, Mz, Mx, My) > 0
+    got = AC.cal_atten_cuda(T(mu), T(mask)).cpu().numpy()
+    old = tune.get_knob("cone.variant")
+    try:
+        tune.set_knob("cone.variant", 3)
+        direct = AC.cal_atten_cuda(T(mu), T(mask)).cpu().numpy()
+    finally:
+        tune.set_knob("cone.variant", old)
+    ref = O.cone_ref(mu, mask)
+    assert rel_err(got, ref) < TOL_MAP
+    assert rel_err(direct, ref) < TOL_MAP
 
 
 def test_spectral_cone_benchmark_size():

@@ -501,11 +501,16 @@ def reference_gpu_leg(device, N=128, A=120, n_vol=30):
             (lambda: ref.mlem_cuda_batch(C, atten, em, th, I, 5, 0.0, 0.01),
              lambda: AC.mlem_cuda_batch(C, atten, em, th, I, 5, 0.0, 0.01), 1),
     }
+    from fl_correction_b200 import _lib
     out = {}
     for name, (fr, fo, reps) in cases.items():
-        r_ms, o_ms = ev_ms(fr, reps), ev_ms(fo, reps)
+        # ours first, then the reference, each warmed up and timed on its own
+        l0 = _lib.query("flc_launch_count")
+        o_ms = ev_ms(fo, reps)
+        launches = (_lib.query("flc_launch_count") - l0) // (reps + 1)
+        r_ms = ev_ms(fr, reps)
         out[name] = {"reference_ms": round(r_ms, 3), "ours_ms": round(o_ms, 3),
-                     "speedup": round(r_ms / o_ms, 2)}
+                     "speedup": round(r_ms / o_ms, 2), "ours_launches_per_call": int(launches)}
         print("[ref-gpu]", name, out[name], file=sys.stderr, flush=True)
     return out
 

@@ -100,6 +100,55 @@ __device__ __forceinline__ void dft_small(float2 (&v)[R], float sg) {
         v[0] = make_float2(v[0].x + a.x, v[0].y + a.y);
         v[1] = make_float2(t.x + u.x, t.y + u.y);
         v[2] = make_float2(t.x - u.x, t.y - u.y);
+    } else if constexpr (R == 8) {
+        // 8 = 2 x 4: pairs (n, n+4) by 2-point DFTs, the odd outputs turned by
+        // e^{sg i pi n / 4}, then 4-point DFTs over n; output k1 + 2 k2
+        constexpr float h = 0.7071067811865476f;   // sqrt(1/2)
+        float2 e[4], o[4];
+#pragma unroll
+        for (int n = 0; n < 4; ++n) {
+            e[n] = make_float2(v[n].x + v[n + 4].x, v[n].y + v[n + 4].y);
+            o[n] = make_float2(v[n].x - v[n + 4].x, v[n].y - v[n + 4].y);
+        }
+        o[1] = make_float2(h * (o[1].x - sg * o[1].y), h * (o[1].y + sg * o[1].x));
+        o[2] = rot_i(o[2], sg);
+        o[3] = make_float2(h * (-o[3].x - sg * o[3].y), h * (-o[3].y + sg * o[3].x));
+        dft_small<4>(e, sg);
+        dft_small<4>(o, sg);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            v[2 * k] = e[k];
+            v[2 * k + 1] = o[k];
+        }
+    } else if constexpr (R == 9) {
+        // 9 = 3 x 3: 3-point DFTs over n1 of x[3 n1 + n2], turned by
+        // e^{sg 2 pi i n2 k1 / 9}, then 3-point DFTs over n2; output k1 + 3 k2
+        constexpr float c1 = 0.766044443118978f, s1 = 0.6427876096865393f;    // 2 pi / 9
+        constexpr float c2 = 0.17364817766693041f, s2 = 0.984807753012208f;   // 4 pi / 9
+        constexpr float c4 = -0.9396926207859083f, s4 = 0.3420201433256689f;  // 8 pi / 9
+        float2 y[3][3];   // y[n2][k1]
+#pragma unroll
+        for (int n2 = 0; n2 < 3; ++n2) {
+            float2 t[3] = {v[n2], v[n2 + 3], v[n2 + 6]};
+            dft_small<3>(t, sg);
+#pragma unroll
+            for (int k1 = 0; k1 < 3; ++k1) y[n2][k1] = t[k1];
+        }
+        auto turn = [&](float2 z, float c, float sn) {
+            const float ss = sg * sn;
+            return make_float2(c * z.x - ss * z.y, c * z.y + ss * z.x);
+        };
+        y[1][1] = turn(y[1][1], c1, s1);
+        y[1][2] = turn(y[1][2], c2, s2);
+        y[2][1] = turn(y[2][1], c2, s2);
+        y[2][2] = turn(y[2][2], c4, s4);
+#pragma unroll
+        for (int k1 = 0; k1 < 3; ++k1) {
+            float2 t[3] = {y[0][k1], y[1][k1], y[2][k1]};
+            dft_small<3>(t, sg);
+#pragma unroll
+            for (int k2 = 0; k2 < 3; ++k2) v[k1 + 3 * k2] = t[k2];
+        }
     } else {  // R == 5
         const float c1 = 0.309016994374947424f, c2 = -0.809016994374947424f;  // cos 2pi/5, 4pi/5
         const float s1 = 0.951056516295153572f, s2 = 0.587785252292473129f;   // sin 2pi/5, 4pi/5
@@ -174,6 +223,8 @@ __device__ float2* fft_batch(float2* a, float2* b, const Radices& rad, int nseq,
     for (int st = 0; st < rad.nst; ++st) {
         const int R = rad.r[st];
         if (R == 4) fft_pass<4>(a, b, rad.n, Ns, nseq, ss, es, tw, sg, seq_fast);
+        else if (R == 8) fft_pass<8>(a, b, rad.n, Ns, nseq, ss, es, tw, sg, seq_fast);
+        else if (R == 9) fft_pass<9>(a, b, rad.n, Ns, nseq, ss, es, tw, sg, seq_fast);
         else if (R == 2) fft_pass<2>(a, b, rad.n, Ns, nseq, ss, es, tw, sg, seq_fast);
         else if (R == 3) fft_pass<3>(a, b, rad.n, Ns, nseq, ss, es, tw, sg, seq_fast);
         else fft_pass<5>(a, b, rad.n, Ns, nseq, ss, es, tw, sg, seq_fast);
@@ -621,13 +672,25 @@ int smooth_even(int need) {
     }
 }
 
+// The passes of a length-n transform: the factor 2^e in passes of 8 and 4
+// (fewest passes, radix 4 where the count ties), 3^f in 9s and a 3, then 5s.
+// Every pass is one read and one write of the sequences in shared memory
+// with a barrier, so fewer, larger butterflies shorten the latency-bound
+// transforms (144 = 4 x 4 x 9: three passes instead of four).
 Radices radices(int n) {
     Radices r{};
     r.n = n;
-    int k = n;
-    while (k % 4 == 0 && r.nst < kMaxStages) { r.r[r.nst++] = 4; k /= 4; }
-    for (int f : {2, 3, 5})
-        while (k % f == 0 && r.nst < kMaxStages) { r.r[r.nst++] = f; k /= f; }
+    int k = n, e = 0, f = 0;
+    while (k % 2 == 0) { k /= 2; ++e; }
+    while (k % 3 == 0) { k /= 3; ++f; }
+    while (e > 0 && r.nst < kMaxStages) {
+        const int t = (e >= 3 && e != 4) ? 3 : (e >= 2 ? 2 : 1);
+        r.r[r.nst++] = 1 << t;
+        e -= t;
+    }
+    while (f >= 2 && r.nst < kMaxStages) { r.r[r.nst++] = 9; f -= 2; }
+    if (f == 1 && r.nst < kMaxStages) r.r[r.nst++] = 3;
+    while (k % 5 == 0 && r.nst < kMaxStages) { r.r[r.nst++] = 5; k /= 5; }
     return r;
 }
 

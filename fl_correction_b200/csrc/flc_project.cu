@@ -785,10 +785,11 @@ constexpr int kSegU = 8;      // ... and in a backward segment walk
 // run along w (coalesced); batch j of kFwdU rows is loaded while batch j - 1
 // is computed.  em_a: the angle's R emission values (RC == 1: unused, the
 // caller scales the column sums).
-template <int RC>
+template <int RC, int WC>
 __device__ __forceinline__ void fwd_angle2(const float* __restrict__ at, const float* sC, int img,
                                            int pitch, const float* __restrict__ em_a, int R,
-                                           const Geo& g, int H, int W, int parts, float* sp) {
+                                           const Geo& g, int H, int Wrt, int parts, float* sp) {
+    const int W = WC > 0 ? WC : Wrt;       // a compile-time width makes the row strides immediates
     const int hper = (H + parts - 1) / parts;
     const int nitems = parts * W;
     for (int item = threadIdx.x; item < nitems; item += blockDim.x) {
@@ -802,21 +803,11 @@ __device__ __forceinline__ void fwd_angle2(const float* __restrict__ at, const f
         const float* ap = at + (int64_t)h0 * W + w;
         float acc = 0.f;
         float hf = (float)h0 - g.cy;
-
-        // rows past the part repeat its last row with weight 0
+        // rows past the part have weight 0
         float cur[kFwdU], nxt[kFwdU];
 #pragma unroll
-        for (int k = 0; k < kFwdU; ++k) {
-            cur[k] = __ldg(ap + (int64_t)min(k, n - 1) * W);
-            if (k >= n) cur[k] = 0.f;
-        }
-        for (int j = 0; j < n; j += kFwdU) {
-#pragma unroll
-            for (int k = 0; k < kFwdU; ++k) {
-                const int r = j + kFwdU + k;
-                nxt[k] = __ldg(ap + (int64_t)min(r, n - 1) * W);
-                if (r >= n) nxt[k] = 0.f;
-            }
+        for (int k = 0; k < kFwdU; ++k) cur[k] = k < n ? __ldg(ap + (int64_t)k * W) : 0.f;
+        auto walk = [&]() {
 #pragma unroll
             for (int k = 0; k < kFwdU; ++k) {
                 const Smp s = sample_xy(g, fmaf(g.c, hf, bx), fmaf(g.s, hf, by));
@@ -833,6 +824,22 @@ __device__ __forceinline__ void fwd_angle2(const float* __restrict__ at, const f
             }
 #pragma unroll
             for (int k = 0; k < kFwdU; ++k) cur[k] = nxt[k];
+        };
+        int j = 0;
+        // the next batch lies inside the part: its loads need no bound
+        for (; j + 2 * kFwdU <= n; j += kFwdU) {
+            const float* an = ap + (int64_t)(j + kFwdU) * W;
+#pragma unroll
+            for (int k = 0; k < kFwdU; ++k) nxt[k] = __ldg(an + (int64_t)k * W);
+            walk();
+        }
+        for (; j < n; j += kFwdU) {
+#pragma unroll
+            for (int k = 0; k < kFwdU; ++k) {
+                const int r = j + kFwdU + k;
+                nxt[k] = r < n ? __ldg(ap + (int64_t)r * W) : 0.f;
+            }
+            walk();
         }
         sp[part * W + w] = acc;
     }
@@ -857,13 +864,14 @@ __device__ __forceinline__ void fwd_finish(const float* sp, int parts, int W, fl
 // row pitch == 9 mod 32) and walks its angles (fwd_angle2).  The partial sums
 // are double buffered, so an angle costs one barrier.  I != nullptr: out =
 // I / max(Pf, 1e-6) (the MLEM ratio), else out = Pf.
-template <int RC>
+template <int RC, int WC>
 __global__ void __launch_bounds__(kT2, 3)
 proj_fwd2_kernel(const float* __restrict__ atten, const float* __restrict__ C,
                  const float* __restrict__ em, const float* __restrict__ theta,
                  float* __restrict__ out, const float* __restrict__ I, int A, int B, int Rrt,
-                 int H, int W, int apc, int parts) {
+                 int H, int Wrt, int apc, int parts) {
     extern __shared__ __align__(16) float smem[];
+    const int W = WC > 0 ? WC : Wrt;
     const int R = RC > 0 ? RC : Rrt;
     const int b = blockIdx.y;
     const int a0 = blockIdx.x * apc, a1 = min(A, a0 + apc);
@@ -876,8 +884,8 @@ proj_fwd2_kernel(const float* __restrict__ atten, const float* __restrict__ C,
     for (int a = a0; a < a1; ++a) {
         const Geo g = make_geo(theta[a], H, W);
         float* sp = spart + (a & 1) * parts * W;
-        fwd_angle2<RC>(atten + ((int64_t)a * B + b) * H * W, sC, img, pitch, em + (int64_t)a * R,
-                       R, g, H, W, parts, sp);
+        fwd_angle2<RC, WC>(atten + ((int64_t)a * B + b) * H * W, sC, img, pitch,
+                           em + (int64_t)a * R, R, g, H, W, parts, sp);
         __syncthreads();
         fwd_finish(sp, parts, W, RC == 1 ? __ldg(em + (int64_t)a * R) : 1.f, I, out,
                    (int64_t)a * B + b);
@@ -906,11 +914,12 @@ __device__ __forceinline__ void stage_q(float* sq, const float* __restrict__ rat
 // leaves idle, or into a pass over all threads after each angle -- measured
 // slower: 2.53 and 1.92 ms against 1.56 ms for the backward of 120 angles x
 // 128 slices of 128^2; without any clamped samples it would run 1.22 ms.)
-template <int RC>
+template <int RC, int WC>
 __device__ __forceinline__ void bwd_segment(const float* __restrict__ at, const float* q,
                                             float* sacc, float* srow, float* scol, int img,
-                                            int pitch, int R, const Geo& g, int H, int W, int w,
+                                            int pitch, int R, const Geo& g, int H, int Wrt, int w,
                                             int h0, int h1, Corners& cs) {
+    const int W = WC > 0 ? WC : Wrt;       // a compile-time width makes the row strides immediates
     const float bx = col_bx(g, w), by = col_by(g, w);
     const float q0 = q[w];
     const float* ap = at + (int64_t)h0 * W + w;
@@ -918,8 +927,14 @@ __device__ __forceinline__ void bwd_segment(const float* __restrict__ at, const 
     float hf = (float)h0 - g.cy;
     for (int j = 0; j < n; j += kSegU) {
         float av[kSegU];
+        const float* aj = ap + (int64_t)j * W;
+        if (j + kSegU <= n) {
 #pragma unroll
-        for (int k = 0; k < kSegU; ++k) av[k] = __ldg(ap + (int64_t)min(j + k, n - 1) * W);
+            for (int k = 0; k < kSegU; ++k) av[k] = __ldg(aj + (int64_t)k * W);
+        } else {
+#pragma unroll
+            for (int k = 0; k < kSegU; ++k) av[k] = j + k < n ? __ldg(aj + (int64_t)k * W) : 0.f;
+        }
 #pragma unroll
         for (int k = 0; k < kSegU; ++k) {
             if (j + k >= n) break;
@@ -976,11 +991,12 @@ __device__ __forceinline__ void bwd_segment(const float* __restrict__ at, const 
 // the clamped samples in the frame buffers, which are folded into the image
 // at the end.  q = ratio * em of each angle is staged during the previous
 // angle's last phase (ratio == nullptr: 1).
-template <int RC>
+template <int RC, int WC>
 __device__ void bwd_splat_angles(const float* __restrict__ atten, const float* __restrict__ ratio,
                                  const float* __restrict__ em, const float* __restrict__ theta,
                                  float* sacc, float* sframe, float* sq, int ncopy, int a0, int a1,
-                                 int b, int B, int R, int H, int W, int seg) {
+                                 int b, int B, int R, int H, int Wrt, int seg) {
+    const int W = WC > 0 ? WC : Wrt;
     const int pitch = slice_pitch(W);
     const int img = H * pitch;
     float* srow = sframe + ((threadIdx.x >> 5) % ncopy) * 2 * R * (H + W);
@@ -1006,8 +1022,8 @@ __device__ void bwd_splat_angles(const float* __restrict__ atten, const float* _
             for (int it = threadIdx.x; it < items; it += blockDim.x) {
                 const int k = it / nw, cw = it - k * nw;
                 const int h0 = (ps + 2 * k) * seg;
-                bwd_segment<RC>(at, q, sacc, srow, scol, img, pitch, R, g, H, W, pw + 3 * cw, h0,
-                                min(H, h0 + seg), cs);
+                bwd_segment<RC, WC>(at, q, sacc, srow, scol, img, pitch, R, g, H, W, pw + 3 * cw,
+                                    h0, min(H, h0 + seg), cs);
             }
             // the other q buffer was last read in the previous angle
             if (ph == 5 && a + 1 < a1) stage_q(sq + ((a + 1) & 1) * R * W, ratio, em, a + 1, b, B, R, W);
@@ -1048,24 +1064,25 @@ __device__ __forceinline__ void bwd_epilogue(int mode, float* __restrict__ out,
 // Backward with an epilogue: grid (G, B), cluster (G, 1, 1).  CTA g of slice b
 // splats angles [g*apc, (g+1)*apc) (bwd_splat_angles); the cluster then sums
 // its G images over DSMEM in rank order and applies bwd_epilogue.
-template <int RC>
+template <int RC, int WC>
 __global__ void __launch_bounds__(kT2, 3)
 proj_bwd2_kernel(const float* __restrict__ atten, const float* __restrict__ ratio,
                  const float* __restrict__ em, const float* __restrict__ theta,
                  float* __restrict__ out, const float* __restrict__ Cin,
-                 const float* __restrict__ sens, int A, int B, int Rrt, int H, int W, int apc,
+                 const float* __restrict__ sens, int A, int B, int Rrt, int H, int Wrt, int apc,
                  int seg, int ncopy, float clamp_min, int mode, float beta, float delta) {
     extern __shared__ __align__(16) float smem[];
     cg::cluster_group cluster = cg::this_cluster();
     const int R = RC > 0 ? RC : Rrt;
+    const int W = WC > 0 ? WC : Wrt;
     const int b = blockIdx.y;
     const int a0 = blockIdx.x * apc, a1 = min(A, a0 + apc);
     const int pitch = slice_pitch(W);
     float* sacc = smem;                                     // [R][H][pitch]
     float* sframe = sacc + R * H * pitch;                   // ncopy x [R][2][W + H]
     float* sq = sframe + frame_floats(R, H, W, ncopy);      // [2][R][W]
-    bwd_splat_angles<RC>(atten, ratio, em, theta, sacc, sframe, sq, ncopy, a0, a1, b, B, R, H, W,
-                         seg);
+    bwd_splat_angles<RC, WC>(atten, ratio, em, theta, sacc, sframe, sq, ncopy, a0, a1, b, B, R, H,
+                             W, seg);
     cluster.sync();
     cluster_reduce(cluster, sacc, R, H, W, pitch, [&](int r, int h, int w, float s) {
         bwd_epilogue(mode, out, Cin, sens, clamp_min, beta, delta, r, b, B, H, W, h, w, s);
@@ -1384,7 +1401,7 @@ mlem_queue_kernel(const MlemQueue* __restrict__ queue, int* __restrict__ counter
             for (int a = a0; a < a1; ++a) {
                 const Geo g = make_geo(P.theta[a], H, W);
                 float* sp = sframe + (a & 1) * parts * W;
-                fwd_angle2<RC>(P.atten + ((int64_t)a * P.B + b) * H * W, simg, img, pitch,
+                fwd_angle2<RC, 0>(P.atten + ((int64_t)a * P.B + b) * H * W, simg, img, pitch,
                                P.em + (int64_t)a * R, R, g, H, W, parts, sp);
                 __syncthreads();
                 fwd_finish(sp, parts, W, RC == 1 ? __ldg(P.em + (int64_t)a * R) : 1.f, P.I,
@@ -1392,7 +1409,7 @@ mlem_queue_kernel(const MlemQueue* __restrict__ queue, int* __restrict__ counter
             }
             __syncthreads();   // the image and partials are reused below
         }
-        bwd_splat_angles<RC>(P.atten, mode == 0 ? P.ratio : nullptr, P.em, P.theta, simg, sframe,
+        bwd_splat_angles<RC, 0>(P.atten, mode == 0 ? P.ratio : nullptr, P.em, P.theta, simg, sframe,
                              sq, ncopy, a0, a1, b, P.B, R, H, W, seg);
         cluster.sync();
         cluster_reduce(cluster, simg, R, H, W, pitch, [&](int r, int h, int w, float s) {
@@ -1647,6 +1664,40 @@ int bwd2_copies(int64_t R, int64_t H, int64_t W) {
 }
 
 bool use_lean() { return tune(kTuneProjLegacy) == 0; }
+
+// The lean kernels instantiated for the common slice widths (their row
+// strides and pitch become immediates) and for any width at run time.
+template <int RC>
+const void* fwd2_for_width(int64_t W) {
+    switch (W) {
+        case 64: return (const void*)proj_fwd2_kernel<RC, 64>;
+        case 96: return (const void*)proj_fwd2_kernel<RC, 96>;
+        case 128: return (const void*)proj_fwd2_kernel<RC, 128>;
+        case 160: return (const void*)proj_fwd2_kernel<RC, 160>;
+        case 192: return (const void*)proj_fwd2_kernel<RC, 192>;
+        default: return (const void*)proj_fwd2_kernel<RC, 0>;
+    }
+}
+
+template <int RC>
+const void* bwd2_for_width(int64_t W) {
+    switch (W) {
+        case 64: return (const void*)proj_bwd2_kernel<RC, 64>;
+        case 96: return (const void*)proj_bwd2_kernel<RC, 96>;
+        case 128: return (const void*)proj_bwd2_kernel<RC, 128>;
+        case 160: return (const void*)proj_bwd2_kernel<RC, 160>;
+        case 192: return (const void*)proj_bwd2_kernel<RC, 192>;
+        default: return (const void*)proj_bwd2_kernel<RC, 0>;
+    }
+}
+
+const void* fwd2_kernel_for(int64_t R, int64_t W) {
+    return R == 1 ? fwd2_for_width<1>(W) : fwd2_for_width<0>(W);
+}
+
+const void* bwd2_kernel_for(int64_t R, int64_t W) {
+    return R == 1 ? bwd2_for_width<1>(W) : bwd2_for_width<0>(W);
+}
 bool force_band() { return use_lean() && tune(kTuneProjBand) != 0; }
 
 }  // namespace
@@ -1658,7 +1709,7 @@ int fwd2_launch(const float* atten, const float* C, const float* em, const float
                 cudaStream_t st) {
     const size_t smem = fwd2_smem(R, H, W);
     if (smem > (size_t)max_smem_optin()) return FLC_ERR_UNSUPPORTED;
-    const void* fn = R == 1 ? (const void*)proj_fwd2_kernel<1> : (const void*)proj_fwd2_kernel<0>;
+    const void* fn = fwd2_kernel_for(R, W);
     FLC_TRY_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kT2, smem) != cudaSuccess ||
@@ -1698,7 +1749,7 @@ int bwd2_launch(const float* atten, const float* ratio, const float* em, const f
     if (bwd2_smem(R, H, W, 1) > (size_t)max_smem_optin()) return FLC_ERR_UNSUPPORTED;
     const int ncopy = bwd2_copies(R, H, W);
     const size_t smem = bwd2_smem(R, H, W, ncopy);
-    const void* fn = R == 1 ? (const void*)proj_bwd2_kernel<1> : (const void*)proj_bwd2_kernel<0>;
+    const void* fn = bwd2_kernel_for(R, W);
     const int threads = bwd2_threads(H, W);
     Plan p = plan_cluster(fn, A, B, smem, threads);
     int iA = (int)A, iB = (int)B, iR = (int)R, iH = (int)H, iW = (int)W, apc = p.apc;
@@ -1864,7 +1915,7 @@ int mlem_iter_launch(const float* atten, const float* em, const float* theta, co
 void mlem_iter_prepare(int64_t A, int64_t B, int64_t R, int64_t H, int64_t W) {
     if (use_lean() && !force_band() && bwd2_smem(R, H, W, 1) <= (size_t)max_smem_optin()) {
         const size_t smem = bwd2_smem(R, H, W, bwd2_copies(R, H, W));
-        const void* fn = R == 1 ? (const void*)proj_bwd2_kernel<1> : (const void*)proj_bwd2_kernel<0>;
+        const void* fn = bwd2_kernel_for(R, W);
         (void)plan_cluster(fn, A, B, smem, bwd2_threads(H, W));
         return;
     }

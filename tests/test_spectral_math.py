@@ -31,16 +31,72 @@ def smooth_even(n):
 
 
 def radices(n):
+    """The kernels' passes: 2^e in 8s and 4s (fewest passes, 4 on ties),
+    3^f in 9s and a 3, then 5s."""
     rs = []
-    while n % 4 == 0:
-        rs.append(4)
-        n //= 4
-    for f in (2, 3, 5):
-        while n % f == 0:
-            rs.append(f)
-            n //= f
+    e = f = 0
+    while n % 2 == 0:
+        n //= 2
+        e += 1
+    while n % 3 == 0:
+        n //= 3
+        f += 1
+    while e > 0:
+        t = 3 if (e >= 3 and e != 4) else (2 if e >= 2 else 1)
+        rs.append(1 << t)
+        e -= t
+    while f >= 2:
+        rs.append(9)
+        f -= 2
+    if f == 1:
+        rs.append(3)
+    while n % 5 == 0:
+        rs.append(5)
+        n //= 5
     assert n == 1
     return rs
+
+
+def _dft(v, sg):
+    R = v.shape[-1]
+    return v @ np.exp(sg * 2j * np.pi * np.outer(np.arange(R), np.arange(R)) / R).T
+
+
+def dft8_kernel_form(v, sg):
+    """dft_small<8>: 2-point DFTs of (n, n+4), odd outputs turned by
+    e^{sg i pi n/4}, 4-point DFTs over n; output k1 + 2 k2."""
+    e = v[..., :4] + v[..., 4:]
+    o = (v[..., :4] - v[..., 4:]) * np.exp(sg * 1j * np.pi * np.arange(4) / 4)
+    out = np.empty_like(v)
+    out[..., 0::2] = _dft(e, sg)
+    out[..., 1::2] = _dft(o, sg)
+    return out
+
+
+def dft9_kernel_form(v, sg):
+    """dft_small<9>: 3-point DFTs over n1 of x[3 n1 + n2], turned by
+    e^{sg 2 pi i n2 k1 / 9}, 3-point DFTs over n2; output k1 + 3 k2."""
+    y = np.stack([_dft(v[..., [n2, n2 + 3, n2 + 6]], sg) for n2 in range(3)], -2)  # [n2][k1]
+    y = y * np.exp(sg * 2j * np.pi * np.outer(np.arange(3), np.arange(3)) / 9)
+    out = np.empty_like(v)
+    for k1 in range(3):
+        out[..., k1::3] = _dft(y[..., :, k1], sg)
+    return out
+
+
+@pytest.mark.parametrize("sg", [-1, 1])
+def test_radix8_and_radix9_butterflies(sg):
+    rng = np.random.default_rng(8 + sg)
+    for R, form in ((8, dft8_kernel_form), (9, dft9_kernel_form)):
+        v = rng.random((4, R)) + 1j * rng.random((4, R))
+        assert np.abs(form(v, sg) - _dft(v, sg)).max() < 1e-12
+
+
+def test_pass_counts():
+    assert radices(144) == [4, 4, 9]
+    assert radices(216) == [8, 9, 3]
+    assert radices(288) == [8, 4, 9]
+    assert radices(160) == [8, 4, 5]
 
 
 def stockham(x, sign=-1):
@@ -68,7 +124,7 @@ def stockham(x, sign=-1):
     return a
 
 
-@pytest.mark.parametrize("n", [2, 4, 6, 12, 20, 36, 50, 144, 160])
+@pytest.mark.parametrize("n", [2, 4, 6, 8, 12, 18, 20, 36, 50, 72, 144, 160, 216, 288])
 def test_stockham_recurrence_is_the_dft(n):
     rng = np.random.default_rng(n)
     x = rng.random((3, n)) + 1j * rng.random((3, n))

@@ -653,12 +653,23 @@ __global__ void fft_apply_kernel(const float* __restrict__ res, float* __restric
     __syncthreads();
     const int al = v / L, l = v - al * L;
     float* ob = out + l * out_l_stride + (int64_t)(a_base + al) * out_a_stride;
-    for (int i = threadIdx.y; i < 32; i += blockDim.y) {
-        const int y = y0 + i, x = x0 + threadIdx.x;
+    // the block's rows of the attenuation are loaded together before any is
+    // stored (blockDim.y = 8: four rows per thread), so the read-modify-write
+    // keeps four loads in flight
+    constexpr int kRows = 4;
+    const int x = x0 + threadIdx.x;
+    float prev[kRows];
+#pragma unroll
+    for (int r = 0; r < kRows; ++r) {
+        const int y = y0 + threadIdx.y + r * 8;
+        prev[r] = (mode == 2 && y < Y && x < X)
+                      ? ob[((int64_t)z * Y + (Y - 1 - y)) * X + x] : 1.f;
+    }
+#pragma unroll
+    for (int r = 0; r < kRows; ++r) {
+        const int i = threadIdx.y + r * 8, y = y0 + i;
         if (y >= Y || x >= X) continue;
-        float* o = ob + ((int64_t)z * Y + (Y - 1 - y)) * X + x;
-        const float e = expf(-tile[threadIdx.x][i]);
-        if (mode == 2) *o *= e; else *o = e;
+        ob[((int64_t)z * Y + (Y - 1 - y)) * X + x] = prev[r] * expf(-tile[threadIdx.x][i]);
     }
 }
 

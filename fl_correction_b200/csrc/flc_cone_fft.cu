@@ -69,6 +69,29 @@ constexpr int kRowPairs = 16;
 constexpr int kColK = 16;
 constexpr int kSplitThreads = 512;
 
+// Paired FP32 arithmetic: sm_100 executes an FMA on both FP32 halves of a
+// 64-bit register pair in one instruction (PTX fma.rn.f32x2), each half
+// rounded as the scalar FMA would round it.
+typedef unsigned long long f32x2;
+
+__device__ __forceinline__ f32x2 pk2(float a, float b) {
+    f32x2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ void upk2(f32x2 r, float& a, float& b) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r));
+}
+__device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
+    f32x2 d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+// A complex value in shared memory as a register pair (one 8-byte load).
+__device__ __forceinline__ f32x2 ld2(const float2* p) {
+    return *reinterpret_cast<const f32x2*>(p);
+}
+
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
     return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
 }
@@ -482,7 +505,7 @@ fft_inv_rows_kernel(const float2* __restrict__ S, const float2* __restrict__ Tyg
 // groups of 8 consecutive x, paired first with last so that every warp sums
 // about the same number of depths.  P rows past X and G rows past Mx are
 // zero in shared memory, so the blocks of 8 depths need no edge tests.
-__global__ void __launch_bounds__(kCorrWarps * 32, 4)
+__global__ void __launch_bounds__(kCorrWarps * 32, 3)
 fft_corr_kernel(float2* __restrict__ S, const float2* __restrict__ G, FftGeom g) {
     extern __shared__ __align__(16) float2 sc[];
     const int X = g.X, Mx = g.Mx;
@@ -524,41 +547,55 @@ fft_corr_kernel(float2* __restrict__ S, const float2* __restrict__ G, FftGeom g)
             // multiple of 8 near dmax / 2
             const int dsplit = ((dmax + 15) / 16) * 8;
             const int dlo = half ? dsplit : 0, dhi = half ? dmax : dsplit;
-            float2 acc[8];
+            // acc[t] = sum_e G[d0+e] * P[x0+t+d0+e] in two paired sums:
+            // pr[t] = sum G.x * (P.x, P.y), qi[t] = sum G.y * (P.x, P.y), one
+            // paired FMA each per depth (the complex product is
+            // (pr.x - qi.y, pr.y + qi.x), formed once at the end)
+            f32x2 pr[8], qi[8];
 #pragma unroll
-            for (int t = 0; t < 8; ++t) acc[t] = make_float2(0.f, 0.f);
-            float2 lo[8], hi[8];
+            for (int t = 0; t < 8; ++t) pr[t] = qi[t] = pk2(0.f, 0.f);
+            f32x2 lo[8], hi[8];
 #pragma unroll
-            for (int i = 0; i < 8; ++i) lo[i] = sP[(x0 + dlo + i) * kCorrK + l16];
-#define FLC_CMAC(A, W)                                   \
-    A.x = fmaf(gv.x, W.x, fmaf(-gv.y, W.y, A.x));       \
-    A.y = fmaf(gv.x, W.y, fmaf(gv.y, W.x, A.y));
+            for (int i = 0; i < 8; ++i) lo[i] = ld2(sP + (x0 + dlo + i) * kCorrK + l16);
+#define FLC_CMAC2(W)                                \
+    pr[t] = fma2(gx, W, pr[t]);                     \
+    qi[t] = fma2(gy, W, qi[t]);
             for (int d0 = dlo; d0 < dhi; d0 += 16) {
 #pragma unroll
-                for (int i = 0; i < 8; ++i) hi[i] = sP[(x0 + d0 + 8 + i) * kCorrK + l16];
+                for (int i = 0; i < 8; ++i) hi[i] = ld2(sP + (x0 + d0 + 8 + i) * kCorrK + l16);
 #pragma unroll
                 for (int e = 0; e < 8; ++e) {
                     const float2 gv = sG[(d0 + e) * kCorrK + l16];
+                    const f32x2 gx = pk2(gv.x, gv.x), gy = pk2(gv.y, gv.y);
 #pragma unroll
                     for (int t = 0; t < 8; ++t) {
-                        if (t + e < 8) { FLC_CMAC(acc[t], lo[t + e]) }
-                        else { FLC_CMAC(acc[t], hi[t + e - 8]) }
+                        if (t + e < 8) { FLC_CMAC2(lo[t + e]) }
+                        else { FLC_CMAC2(hi[t + e - 8]) }
                     }
                 }
                 if (d0 + 8 >= dhi) break;
 #pragma unroll
-                for (int i = 0; i < 8; ++i) lo[i] = sP[(x0 + d0 + 16 + i) * kCorrK + l16];
+                for (int i = 0; i < 8; ++i) lo[i] = ld2(sP + (x0 + d0 + 16 + i) * kCorrK + l16);
 #pragma unroll
                 for (int e = 0; e < 8; ++e) {
                     const float2 gv = sG[(d0 + 8 + e) * kCorrK + l16];
+                    const f32x2 gx = pk2(gv.x, gv.x), gy = pk2(gv.y, gv.y);
 #pragma unroll
                     for (int t = 0; t < 8; ++t) {
-                        if (t + e < 8) { FLC_CMAC(acc[t], hi[t + e]) }
-                        else { FLC_CMAC(acc[t], lo[t + e - 8]) }
+                        if (t + e < 8) { FLC_CMAC2(hi[t + e]) }
+                        else { FLC_CMAC2(lo[t + e - 8]) }
                     }
                 }
             }
-#undef FLC_CMAC
+#undef FLC_CMAC2
+            float2 acc[8];
+#pragma unroll
+            for (int t = 0; t < 8; ++t) {
+                float px, py, qx, qy;
+                upk2(pr[t], px, py);
+                upk2(qi[t], qx, qy);
+                acc[t] = make_float2(px - qy, py + qx);
+            }
 #pragma unroll
             for (int t = 0; t < 8; ++t) {
                 acc[t].x += __shfl_xor_sync(0xffffffffu, acc[t].x, 16);

@@ -16,7 +16,10 @@ pytestmark = pytest.mark.gpu
 SPECIAL = [0.0, math.pi / 2, math.pi, -math.pi / 2, math.pi / 4, 3 * math.pi / 4, 1e-7, 2.9]
 
 CASES = [(8, 2, 1, 24, 24), (8, 3, 2, 20, 28), (8, 1, 3, 33, 17), (1, 1, 1, 2, 2),
-         (5, 4, 1, 64, 64), (12, 2, 1, 96, 96), (6, 2, 1, 200, 200)]
+         (5, 4, 1, 64, 64), (12, 2, 1, 96, 96), (6, 2, 1, 200, 200),
+         # an odd slice count (the two-slice forward's last CTA has one slice),
+         # non-square slices, a width without a compile-time instance
+         (7, 5, 1, 48, 40), (6, 3, 1, 50, 70)]
 
 
 @pytest.mark.parametrize("A,B,R,H,W", CASES)
@@ -147,3 +150,4 @@ def test_backward_splat_variants(mode, A, B, R, H, W):
         tune.set_knob("proj.bwd", old)
     assert rel_err(out, O.bwd_emission(atten, ratio, em, th)) < TOL_MAP
     assert rel_err(mout, O.mlem(C0, atten, em, th, I, 3, 0.0, 0.01)) < 1e-4
+

@@ -54,7 +54,7 @@ def parse():
     p.add_argument("--adam-steps", type=int, default=0,
                    help="configurations 2/4: Adam steps timed (default 200 / 3)")
     p.add_argument("--case", default=None, choices=["cone", "cone_direct", "mlem", "fwd", "bwd", "stage",
-                                                    "mlem_multi", "bwd_large"],
+                                                    "mlem_multi", "bwd_large", "grad"],
                    help="run one kernel on a profiling-sized case instead of the benchmark")
     p.add_argument("--case-slices", type=int, default=16,
                    help="slices of 128^2 in the projector / MLEM cases (128: the benchmark's shape)")
@@ -848,7 +848,8 @@ def run_case(args):
     the direct separable kernel); mlem: one fused MLEM
     iteration (plus the sensitivity pass) at 24 angles x 16 slices of 128^2;
     fwd / bwd: the projector at 120 angles x 16 slices of 128^2; bwd_large:
-    the backward at 180 angles x --case-slices slices of 256^2."""
+    the backward at 180 angles x --case-slices slices of 256^2; grad: one
+    gradient (projection + adjoint) of configuration 2."""
     import torch
     from fl_correction_b200 import _lib
     from fl_correction_b200.cuda_lib import atten_cuda as AC
@@ -905,6 +906,21 @@ def run_case(args):
             _lib.call("flc_atten_stage_ws", _lib.ptr(frac), _lib.ptr(th), _lib.ptr(cx),
                       _lib.ptr(cf), _lib.ptr(atten), _lib.ptr(ws), n_ch, N, N, N, A, L, 0, n_a,
                       0, 1, _lib.ptr(ws4), nb, _lib.stream())
+    elif args.case == "grad":
+        # one gradient step of configuration 2 (96^3, 3 elements, 90 angles):
+        # the corrected projection and its adjoint through mu
+        from fl_correction_b200 import phantoms
+        from fl_correction_b200.grad_recon import GradientRecon
+        wl = phantoms.make_workload(2)
+        Ng, Lg = wl.N, len(wl.elements)
+        maskg = generate_detector_mask(wl.mask_angle, wl.mask_angle, Ng)
+        frac = wl.frac()
+        rec = GradientRecon(wl.param, wl.angles, maskg, (Ng, Ng, Ng), fixed_frac=frac[Lg:],
+                            tv_weight=1e-3, lr=1e-2, device=dev)
+        Ig = rec.proj.project(torch.from_numpy(wl.conc).to(dev))
+        Cg = torch.full((Lg, Ng, Ng, Ng), 0.5, device=dev)
+        def once():
+            rec.gradient(Cg, Ig)
     elif args.case == "bwd_large":
         # the row-band backward: 180 angles x --case-slices slices of 256^2
         N, A, B = 256, 180, args.case_slices

@@ -20,10 +20,15 @@
 // Nothing of size A x volume is stored: each chunk of angles is recomputed in
 // the backward pass (so 256^3 x 180-angle problems fit in HBM).
 
+#include <cooperative_groups.h>
+
+#include <algorithm>
+
 #include "flc_common.cuh"
 #include "flc_geom.cuh"
 
 namespace flc {
+namespace cg = cooperative_groups;
 
 int atten_stage_launch(const float* frac, const float* theta, const float* coef_x,
                        const float* coef_f, float* out, float* mu_ref, int n_ch, int S, int H,
@@ -109,15 +114,16 @@ __global__ void xrf_g_kernel(const float* __restrict__ C, const float* __restric
 //   gbar[h] = dinc[h] + gbar[h-1] * f[h],  df[h] = gbar[h-1] * inc[h]
 // (the adjoint of inc[h-1] = f[h] * inc[h]), then
 //   dfr_j = cx_j * dmu_x_j + sum_l cf_lj * dmu_f_l
-// spread back onto the unrotated grid with the rotation's own taps (global
-// atomics into dC, channels j < L).  grid (S, n_a), block = W rounded to 32.
+// stored per sample, D[j][al][s][h][w] (channels j < L), for
+// rot_adjoint_splat_kernel to spread back onto the unrotated grid.
+// grid (S, n_a), block = W rounded to 32.
 __global__ void xrf_stage_adjoint_kernel(const float* __restrict__ frac,
                                          const float* __restrict__ theta,
                                          const float* __restrict__ coef_x,
                                          const float* __restrict__ coef_f,
                                          const float* __restrict__ INC,
                                          const float* __restrict__ dinc,
-                                         const float* __restrict__ dmu_rev, float* __restrict__ dC,
+                                         const float* __restrict__ dmu_rev, float* __restrict__ D,
                                          int n_ch, int S, int H, int W, int L, int a0, int n_a,
                                          int incident_mode) {
     __shared__ float cx[kMaxCh];
@@ -195,9 +201,77 @@ __global__ void xrf_stage_adjoint_kernel(const float* __restrict__ frac,
 #pragma unroll
             for (int l = 0; l < kMaxL; ++l)
                 if (l < L) d = fmaf(cf[l][j], dmuf[l], d);
-            if (d != 0.f) rot_splat_tap(dC + ((int64_t)j * S + s) * HW, H, W, tp, d);
+            D[(((int64_t)j * n_a + al) * S + s) * HW + (int64_t)h * W + w] = d;
         }
     }
+}
+
+// The rotation adjoint without global atomics: D[j][al][s] (the per-sample
+// gradient of the rotated fractions, one angle of the chunk) spread onto the
+// unrotated grid with the rotation's own taps (rot_tap: the points and
+// weights the forward sampled; taps outside the slice are dropped, as the
+// forward's zero padding reads 0 there), summed over the chunk's angles and
+// added to dC[j][s].  grid (G, S, L), cluster (G, 1, 1): CTA g of (s, j)
+// splats angles g, g + G, ... into a shared-memory image of the slice; the
+// cluster adds its images over DSMEM.  The rotation of a square slice is an
+// isometry, so the sample points of columns three apart, and of same-parity
+// segments (>= 2 samples) of one column, are three or more apart and their
+// 2x2 tap boxes are disjoint: six phases per angle ((w mod 3) x segment
+// parity) update the image with plain read-modify-writes.
+constexpr int kRotAdjThreads = 256;
+
+__global__ void __launch_bounds__(kRotAdjThreads)
+rot_adjoint_splat_kernel(const float* __restrict__ D, const float* __restrict__ theta,
+                         float* __restrict__ dC, int S, int H, int W, int a0, int n_a, int seg) {
+    extern __shared__ __align__(16) float simg[];
+    cg::cluster_group cluster = cg::this_cluster();
+    const int G = (int)cluster.num_blocks(), rank = (int)cluster.block_rank();
+    const int s = blockIdx.y, j = blockIdx.z;
+    const int pitch = slice_pitch(W);
+    const int64_t HW = (int64_t)H * W;
+    for (int i = threadIdx.x; i < H * pitch; i += blockDim.x) simg[i] = 0.f;
+    __syncthreads();
+    const int nseg = (H + seg - 1) / seg;
+    for (int al = rank; al < n_a; al += G) {
+        const double th = (double)theta[a0 + al];
+        const RotGeom g = rot_geom((float)cos(th), (float)sin(th), H, W);
+        const float* d = D + (((int64_t)j * n_a + al) * S + s) * HW;
+        for (int ph = 0; ph < 6; ++ph) {
+            const int pw = ph >> 1, ps = ph & 1;
+            const int nw = (W - pw + 2) / 3, nsp = (nseg - ps + 1) / 2;
+            for (int it = threadIdx.x; it < nw * nsp; it += blockDim.x) {
+                const int k = it / nw, cw = it - k * nw;
+                const int w = pw + 3 * cw;
+                const int h0 = (ps + 2 * k) * seg, h1 = min(H, h0 + seg);
+                for (int h = h0; h < h1; ++h) {
+                    const float v = __ldg(d + (int64_t)h * W + w);
+                    if (v == 0.f) continue;
+                    const RotTap t = rot_tap(g, h, w);
+                    const int x0 = t.x0, y0 = t.y0;
+                    const bool xin0 = x0 >= 0 && x0 < W, xin1 = x0 + 1 >= 0 && x0 + 1 < W;
+                    const bool yin0 = y0 >= 0 && y0 < H, yin1 = y0 + 1 >= 0 && y0 + 1 < H;
+                    const float a = v * (1.f - t.ty), b = v * t.ty;
+                    float* p = simg + y0 * pitch + x0;
+                    if (yin0 && xin0) p[0] += a * (1.f - t.tx);
+                    if (yin0 && xin1) p[1] += a * t.tx;
+                    if (yin1 && xin0) p[pitch] += b * (1.f - t.tx);
+                    if (yin1 && xin1) p[pitch + 1] += b * t.tx;
+                }
+            }
+            __syncthreads();
+        }
+    }
+    cluster.sync();
+    const int64_t share = (HW + G - 1) / G;
+    const int64_t i0 = rank * share, i1 = min(HW, i0 + share);
+    float* out = dC + ((int64_t)j * S + s) * HW;
+    for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+        const int h = (int)(i / W), w = (int)(i - (int64_t)h * W);
+        float sum = 0.f;
+        for (int q = 0; q < G; ++q) sum += cluster.map_shared_rank(simg, q)[h * pitch + w];
+        out[i] += sum;
+    }
+    cluster.sync();
 }
 
 size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
@@ -228,6 +302,45 @@ int64_t xrf_chunk(int64_t S, int64_t H, int64_t W, int64_t A, int64_t L, int64_t
     if (chunk > A) chunk = A;
     if (chunk * L > 65535) chunk = 65535 / L;
     return chunk < 1 ? 1 : chunk;
+}
+
+// Rotation adjoint of one angle chunk: cluster size G (angles split over the
+// cluster) chosen so that S x L x G CTAs fill the GPU, at most 8 and at most
+// the chunk's angles.
+int rot_adjoint_launch(const float* D, const float* theta, float* dC, int64_t S, int64_t H,
+                       int64_t W, int64_t L, int a0, int n_a, cudaStream_t st) {
+    const size_t smem = sizeof(float) * (size_t)H * slice_pitch((int)W);
+    if (smem > (size_t)max_smem_optin()) {
+        set_error("xrf adjoint: a %lld x %lld slice does not fit in shared memory", (long long)H,
+                  (long long)W);
+        return FLC_ERR_UNSUPPORTED;
+    }
+    const int per_sm = (int)std::max<size_t>(1, std::min<size_t>(8, (size_t)smem_per_sm() / (smem + 1024)));
+    int G = (int)ceil_div((int64_t)sm_count() * per_sm, S * L);
+    G = std::max(1, std::min(G, std::min(8, n_a)));
+    int seg = 2;
+    const int64_t nw = (W + 2) / 3;
+    while (seg < H && nw * (((H + seg - 1) / seg + 1) / 2) > kRotAdjThreads) ++seg;
+    const void* fn = (const void*)rot_adjoint_splat_kernel;
+    FLC_TRY_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    FLC_TRY_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)G, (unsigned)S, (unsigned)L);
+    cfg.blockDim = dim3(kRotAdjThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = G;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int iS = (int)S, iH = (int)H, iW = (int)W;
+    FLC_TRY_CUDA(cudaLaunchKernelEx(&cfg, rot_adjoint_splat_kernel, D, theta, dC, iS, iH, iW, a0,
+                                    n_a, seg));
+    count_launches(1);
+    return FLC_OK;
 }
 
 int check_xrf_args(int64_t n_ch, int64_t S, int64_t H, int64_t W, int64_t A, int64_t L,
@@ -388,10 +501,13 @@ extern "C" int flc_xrf_project_adjoint(const float* frac, const float* theta, co
         FLC_TRY(cone_launch_ws(b.DRES, uf, vf, b.DMU, (int64_t)n_a * L, S, W, H, Mz, Mx, My, 0,
                                1, 0, 0, 0, x.fft, x.fft_bytes, st));
         const int threads = (int)((W + 31) & ~31);
+        // the per-sample gradient of the rotated fractions into ATT (free
+        // again), then its rotation adjoint into dC
         xrf_stage_adjoint_kernel<<<dim3((unsigned)S, (unsigned)n_a), threads, 0, st>>>(
-            frac, theta, coef_x, coef_f, b.INC, b.DINC, b.DMU, dC, (int)n_ch, (int)S, (int)H,
+            frac, theta, coef_x, coef_f, b.INC, b.DINC, b.DMU, b.ATT, (int)n_ch, (int)S, (int)H,
             (int)W, (int)L, (int)a0, n_a, incident_mode);
         FLC_TRY(check_launch("xrf_stage_adjoint_kernel"));
+        FLC_TRY(rot_adjoint_launch(b.ATT, theta, dC, S, H, W, L, (int)a0, n_a, st));
     }
     return FLC_OK;
 }

@@ -6,6 +6,15 @@
 
 namespace flc {
 
+// Row pitch (floats) of a slice image staged in shared memory: >= W and
+// == 9 (mod 32) (of the odd residues measured, 1, 3 and 9, the fastest for the
+// column-segment splats).
+__host__ __device__ inline int slice_pitch(int W) {
+    int p = W;
+    while ((p & 31) != 9) ++p;
+    return p;
+}
+
 // ---------------------------------------------------------------------------
 // Projector geometry (atten_cuda_kernel.cu:91-142, :271-337): the sample for
 // detector column w at beam step h of angle th is
@@ -146,19 +155,6 @@ __device__ __forceinline__ float rot_sample_scipy(const float* __restrict__ img,
                                                   const RotGeom& g, int h, int w) {
     const RotTap t = rot_tap(g, h, w);
     return t.inside ? rot_sample_tap(img, H, W, t) : 0.f;
-}
-
-// Adjoint of rot_sample_tap: spreads v over the in-image taps (global atomics).
-// d(out)/d(v00) etc. of the lerp form above: (1-tx)(1-ty), tx(1-ty), (1-tx)ty, tx*ty.
-__device__ __forceinline__ void rot_splat_tap(float* img, int H, int W, const RotTap& t, float v) {
-    const int x0 = t.x0, y0 = t.y0;
-    bool xin0 = x0 >= 0 && x0 < W, xin1 = x0 + 1 >= 0 && x0 + 1 < W;
-    bool yin0 = y0 >= 0 && y0 < H, yin1 = y0 + 1 >= 0 && y0 + 1 < H;
-    const float a = v * (1.f - t.ty), b = v * t.ty;
-    if (yin0 && xin0) atomicAdd(img + y0 * W + x0, a * (1.f - t.tx));
-    if (yin0 && xin1) atomicAdd(img + y0 * W + x0 + 1, a * t.tx);
-    if (yin1 && xin0) atomicAdd(img + (y0 + 1) * W + x0, b * (1.f - t.tx));
-    if (yin1 && xin1) atomicAdd(img + (y0 + 1) * W + x0 + 1, b * t.tx);
 }
 
 }  // namespace flc

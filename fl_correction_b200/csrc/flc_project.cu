@@ -46,13 +46,6 @@ constexpr int kMaxCluster = 8;
 constexpr int kMaxR = 8;
 constexpr int kTileRegs = 8;   // float4 per thread prefetched for the next tile
 
-// Row pitch (floats) of a staged slice: >= W and == 9 (mod 32) (of the odd
-// residues measured, 1, 3 and 9, the fastest for the column-segment kernels).
-__host__ __device__ inline int slice_pitch(int W) {
-    int p = W;
-    while ((p & 31) != 9) ++p;
-    return p;
-}
 
 // Partial sums per detector column: enough (w, part) items to fill the CTA.
 __host__ __device__ inline int col_parts(int W, int H) {

@@ -229,6 +229,42 @@ def test_spectral_cone_benchmark_size():
     assert rel_err(outs[0], outs[1]) < 2e-6
 
 
+def test_spectral_cone_full_planes_against_oracle():
+    """128^2 planes, the benchmark's (29, 128, 29) mask (every depth of the
+    128-deep correlation), 6 slices: the spectral form against the FP64
+    oracle (a few seconds of the oracle's threads)."""
+    from fl_correction_b200 import tune
+    rng = np.random.default_rng(13)
+    mask = generate_detector_mask(13.309, 13.309, 128)
+    u, v = factor_mask(mask)
+    Mz, Mx, My = mask.shape
+    n_a, L, S, N, A = 1, 1, 6, 128, 1
+    mu = (rng.random((n_a, L, S, N, N)) * 0.01).astype(np.float32)
+    mu[..., 40:90, 30:70] += 0.02
+    nb = _lib.query("flc_cone_fft_workspace_bytes", n_a * L, S, N, N, Mz, Mx, My)
+    ws = _lib.workspace(nb, "cuda")
+    old = tune.get_knob("cone.variant")
+    try:
+        tune.set_knob("cone.variant", 4)
+        out = torch.ones((L, A, S, N, N), device="cuda")
+        _lib.call("flc_cone_atten_apply_ws", _lib.ptr(T(mu)), _lib.ptr(T(u)), _lib.ptr(T(v)),
+                  _lib.ptr(out), n_a, L, S, N, N, A, 0, Mz, Mx, My, _lib.ptr(ws), nb,
+                  _lib.stream())
+        got = out.cpu().numpy()
+    finally:
+        tune.set_knob("cone.variant", old)
+    O.set_threads(O.max_threads())
+    res = O.cone_ref(mu.reshape(n_a * L, S, N, N), mask)          # cone frame (Z=S, X=W, Y=H)
+    exp = np.exp(-res[0][:, :, ::-1].transpose(0, 2, 1))
+    assert rel_err(got[0, 0], exp) < TOL_MAP
+    # the path sum itself where it is large enough to carry digits (exp(-res) is
+    # within rounding of 1 wherever res is tiny)
+    r_got = -np.log(np.clip(got[0, 0].astype(np.float64), 1e-30, None))
+    r_ref = res[0][:, :, ::-1].transpose(0, 2, 1)
+    big = r_ref > 1e-3 * r_ref.max()
+    assert np.abs(r_got - r_ref)[big].max() <= 1e-4 * r_ref.max()
+
+
 def test_bounded_wait_runs_out_and_reports_timeout():
     """The direct cone's bounded TMA waits: with the test hooks the first
     staged plane's load is never issued and the wait gives up after a few

@@ -243,11 +243,12 @@ def test_spectral_cone_full_planes_against_oracle():
     mu[..., 40:90, 30:70] += 0.02
     nb = _lib.query("flc_cone_fft_workspace_bytes", n_a * L, S, N, N, Mz, Mx, My)
     ws = _lib.workspace(nb, "cuda")
+    x, U, V = T(mu), T(u), T(v)           # held until the kernels have run
     old = tune.get_knob("cone.variant")
     try:
         tune.set_knob("cone.variant", 4)
         out = torch.ones((L, A, S, N, N), device="cuda")
-        _lib.call("flc_cone_atten_apply_ws", _lib.ptr(T(mu)), _lib.ptr(T(u)), _lib.ptr(T(v)),
+        _lib.call("flc_cone_atten_apply_ws", _lib.ptr(x), _lib.ptr(U), _lib.ptr(V),
                   _lib.ptr(out), n_a, L, S, N, N, A, 0, Mz, Mx, My, _lib.ptr(ws), nb,
                   _lib.stream())
         got = out.cpu().numpy()

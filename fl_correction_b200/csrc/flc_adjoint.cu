@@ -222,14 +222,20 @@ constexpr int kRotAdjThreads = 256;
 
 __global__ void __launch_bounds__(kRotAdjThreads)
 rot_adjoint_splat_kernel(const float* __restrict__ D, const float* __restrict__ theta,
-                         float* __restrict__ dC, int S, int H, int W, int a0, int n_a, int seg) {
+                         float* __restrict__ dC, int S, int H, int W, int a0, int n_a, int seg,
+                         int hb) {
     extern __shared__ __align__(16) float simg[];
     cg::cluster_group cluster = cg::this_cluster();
     const int G = (int)cluster.num_blocks(), rank = (int)cluster.block_rank();
-    const int s = blockIdx.y, j = blockIdx.z;
+    // a slice too large for shared memory is split into bands of hb rows: the
+    // CTA of band b applies only the taps that fall on its rows (every tap row
+    // belongs to one band, so the bands' sums are exact)
+    const int nband = (H + hb - 1) / hb;
+    const int s = blockIdx.y / nband, band = blockIdx.y - s * nband, j = blockIdx.z;
+    const int r0 = band * hb, r1 = min(H, r0 + hb);
     const int pitch = slice_pitch(W);
     const int64_t HW = (int64_t)H * W;
-    for (int i = threadIdx.x; i < H * pitch; i += blockDim.x) simg[i] = 0.f;
+    for (int i = threadIdx.x; i < (r1 - r0) * pitch; i += blockDim.x) simg[i] = 0.f;
     __syncthreads();
     const int nseg = (H + seg - 1) / seg;
     for (int al = rank; al < n_a; al += G) {
@@ -243,28 +249,41 @@ rot_adjoint_splat_kernel(const float* __restrict__ D, const float* __restrict__ 
                 const int k = it / nw, cw = it - k * nw;
                 const int w = pw + 3 * cw;
                 const int h0 = (ps + 2 * k) * seg, h1 = min(H, h0 + seg);
+                if (nband > 1) {
+                    // a segment whose sample rows all lie two rows or more
+                    // outside the band has no tap in it
+                    const float ya = rot_tap_y(g, h0, w), yb = rot_tap_y(g, h1 - 1, w);
+                    if (fmaxf(ya, yb) < (float)r0 - 2.f || fminf(ya, yb) > (float)r1 + 1.f)
+                        continue;
+                }
                 for (int h = h0; h < h1; ++h) {
                     const float v = __ldg(d + (int64_t)h * W + w);
                     if (v == 0.f) continue;
                     const RotTap t = rot_tap(g, h, w);
                     const int x0 = t.x0, y0 = t.y0;
                     const bool xin0 = x0 >= 0 && x0 < W, xin1 = x0 + 1 >= 0 && x0 + 1 < W;
-                    const bool yin0 = y0 >= 0 && y0 < H, yin1 = y0 + 1 >= 0 && y0 + 1 < H;
+                    const bool yin0 = y0 >= r0 && y0 < r1, yin1 = y0 + 1 >= r0 && y0 + 1 < r1;
                     const float a = v * (1.f - t.ty), b = v * t.ty;
-                    float* p = simg + y0 * pitch + x0;
-                    if (yin0 && xin0) p[0] += a * (1.f - t.tx);
-                    if (yin0 && xin1) p[1] += a * t.tx;
-                    if (yin1 && xin0) p[pitch] += b * (1.f - t.tx);
-                    if (yin1 && xin1) p[pitch + 1] += b * t.tx;
+                    if (yin0) {
+                        float* p = simg + (y0 - r0) * pitch + x0;
+                        if (xin0) p[0] += a * (1.f - t.tx);
+                        if (xin1) p[1] += a * t.tx;
+                    }
+                    if (yin1) {
+                        float* p = simg + (y0 + 1 - r0) * pitch + x0;
+                        if (xin0) p[0] += b * (1.f - t.tx);
+                        if (xin1) p[1] += b * t.tx;
+                    }
                 }
             }
             __syncthreads();
         }
     }
     cluster.sync();
-    const int64_t share = (HW + G - 1) / G;
-    const int64_t i0 = rank * share, i1 = min(HW, i0 + share);
-    float* out = dC + ((int64_t)j * S + s) * HW;
+    const int64_t nb = (int64_t)(r1 - r0) * W;
+    const int64_t share = (nb + G - 1) / G;
+    const int64_t i0 = rank * share, i1 = min(nb, i0 + share);
+    float* out = dC + ((int64_t)j * S + s) * HW + (int64_t)r0 * W;
     for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
         const int h = (int)(i / W), w = (int)(i - (int64_t)h * W);
         float sum = 0.f;
@@ -309,14 +328,21 @@ int64_t xrf_chunk(int64_t S, int64_t H, int64_t W, int64_t A, int64_t L, int64_t
 // the chunk's angles.
 int rot_adjoint_launch(const float* D, const float* theta, float* dC, int64_t S, int64_t H,
                        int64_t W, int64_t L, int a0, int n_a, cudaStream_t st) {
-    const size_t smem = sizeof(float) * (size_t)H * slice_pitch((int)W);
+    // bands of rows: the whole slice where it fits in shared memory, else the
+    // fewest even bands that do
+    const size_t row_bytes = sizeof(float) * (size_t)slice_pitch((int)W);
+    int64_t nband = 1;
+    while (ceil_div(H, nband) * row_bytes > (size_t)max_smem_optin() && nband < H) ++nband;
+    if (int64_t t = tune(kTuneXrfBand)) nband = std::max(nband, ceil_div(H, std::min(t, H)));
+    const int hb = (int)ceil_div(H, nband);
+    nband = ceil_div(H, hb);
+    const size_t smem = row_bytes * (size_t)hb;
     if (smem > (size_t)max_smem_optin()) {
-        set_error("xrf adjoint: a %lld x %lld slice does not fit in shared memory", (long long)H,
-                  (long long)W);
+        set_error("xrf adjoint: a row of %lld columns does not fit in shared memory", (long long)W);
         return FLC_ERR_UNSUPPORTED;
     }
     const int per_sm = (int)std::max<size_t>(1, std::min<size_t>(8, (size_t)smem_per_sm() / (smem + 1024)));
-    int G = (int)ceil_div((int64_t)sm_count() * per_sm, S * L);
+    int G = (int)ceil_div((int64_t)sm_count() * per_sm, S * nband * L);
     G = std::max(1, std::min(G, std::min(8, n_a)));
     int seg = 2;
     const int64_t nw = (W + 2) / 3;
@@ -325,7 +351,7 @@ int rot_adjoint_launch(const float* D, const float* theta, float* dC, int64_t S,
     FLC_TRY_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     FLC_TRY_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)G, (unsigned)S, (unsigned)L);
+    cfg.gridDim = dim3((unsigned)G, (unsigned)(S * nband), (unsigned)L);
     cfg.blockDim = dim3(kRotAdjThreads);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = st;
@@ -338,7 +364,7 @@ int rot_adjoint_launch(const float* D, const float* theta, float* dC, int64_t S,
     cfg.numAttrs = 1;
     int iS = (int)S, iH = (int)H, iW = (int)W;
     FLC_TRY_CUDA(cudaLaunchKernelEx(&cfg, rot_adjoint_splat_kernel, D, theta, dC, iS, iH, iW, a0,
-                                    n_a, seg));
+                                    n_a, seg, hb));
     count_launches(1);
     return FLC_OK;
 }

@@ -48,7 +48,9 @@ enum TuneKey {
                             // the two lean kernels (for comparison)
     kTuneProjBand = 8,      // 1: the band backward at every slice size (it runs by
                             // itself only where the lean kernel's image does not fit)
-    kTuneCount = 9
+    kTuneXrfBand = 9,       // rows per band of the XRF rotation adjoint (by itself it
+                            // bands only slices that do not fit in shared memory)
+    kTuneCount = 10
 };
 int64_t tune(int key);
 

@@ -128,6 +128,12 @@ __device__ __forceinline__ RotTap rot_tap(const RotGeom& g, int h, int w) {
     return t;
 }
 
+// The row coordinate iy of rot_tap's sample point.
+__device__ __forceinline__ float rot_tap_y(const RotGeom& g, int h, int w) {
+    const float dw = (float)w - g.cx, dh = (float)h - g.cy;
+    return g.s * dw * g.syh + g.c * dh + g.cy;
+}
+
 __device__ __forceinline__ float rot_sample_tap(const float* __restrict__ img, int H, int W,
                                                 const RotTap& t) {
     const int x0 = t.x0, y0 = t.y0;

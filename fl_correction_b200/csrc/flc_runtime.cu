@@ -63,7 +63,8 @@ namespace {
 std::atomic<int64_t> g_tune[kTuneCount];
 const char* const kTuneNames[kTuneCount] = {"proj.cluster", "proj.apc", "cone.variant",
                                             "atten.chunk", "proj.bwd", "cone.test_wait_limit",
-                                            "cone.test_skip_load", "proj.legacy", "proj.band"};
+                                            "cone.test_skip_load", "proj.legacy", "proj.band",
+                                            "xrf.band"};
 }  // namespace
 
 int64_t tune(int key) { return (key >= 0 && key < kTuneCount) ? g_tune[key].load() : 0; }

@@ -73,6 +73,8 @@ FLC_API uint64_t flc_launch_count(void);
  *                   lean forward / backward pair (for comparison)
  *   "proj.band"     1: the row-band backward (no global atomics; it runs by itself
  *                   where a slice image does not fit in shared memory) at every size
+ *   "xrf.band"      rows per band of the XRF rotation adjoint (automatic: the whole
+ *                   slice, or the fewest even bands that fit in shared memory)
  * Test hooks of the direct cone's bounded waits (for failure-path tests):
  *   "cone.test_wait_limit"  polls before a TMA-plane wait gives up (default 2^26)
  *   "cone.test_skip_load"   k > 0: the load of the k-th staged plane of every

@@ -101,7 +101,8 @@ def test_cpu_tensors_fail_loudly():
 def test_tuning_knobs_round_trip():
     lib = _lib.load()
     for name in (b"proj.cluster", b"proj.apc", b"cone.variant", b"atten.chunk", b"proj.bwd",
-                 b"cone.test_wait_limit", b"cone.test_skip_load", b"proj.legacy", b"proj.band"):
+                 b"cone.test_wait_limit", b"cone.test_skip_load", b"proj.legacy", b"proj.band",
+                 b"xrf.band"):
         old = lib.flc_tune_get(name)
         assert old >= 0
         assert lib.flc_tune_set(name, 3) == 0

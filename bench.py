@@ -669,6 +669,19 @@ def run_grad(args, device):
         grad_check["projection_max_rel_err_vs_fp64"] = float((Pf32 - Pf64).abs().max() /
                                                              Pf64.abs().max())
     del Pf64, Pf32
+    # directional derivative along a random unit direction v: <g32, v> against
+    # the FP64 central difference of the loss (two FP64 evaluations, so it runs
+    # at every volume size)
+    with torch.no_grad():
+        gv = torch.Generator(device=device).manual_seed(3)
+        v = torch.randn(Cc.shape, generator=gv, device=device, dtype=torch.float64)
+        v /= v.norm()
+        eps = 1e-3
+        fd = (float(loss64(Cc.double() + eps * v)) - float(loss64(Cc.double() - eps * v))) / (2 * eps)
+        ad = float((g32.double() * v).sum())
+        grad_check["directional_fd"] = {"adjoint": ad, "fp64_central_difference": fd,
+                                        "rel_err": abs(ad - fd) / abs(fd)}
+        del v
     log("FP64 comparison done", grad_check)
     if N <= 128:
         rng = np.random.default_rng(7)

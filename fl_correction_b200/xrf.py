@@ -30,7 +30,7 @@ class XRFProjector:
     angles_deg  (A,) projection angles in degrees.
     mask        cone mask (Mz, Mx, My), rank one per depth plane, odd Mz, My.
     incident    'own' | 'all' | 'none' (as core.atten_maps).
-    chunk       angles per recomputation pass (0: about 1 GB of scratch).
+    chunk       angles per recomputation pass (0: about 8 GiB of scratch, at least one angle).
     """
 
     def __init__(self, param, angles_deg, mask, shape, fixed_frac=None, incident="own",

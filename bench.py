@@ -54,7 +54,8 @@ def parse():
     p.add_argument("--adam-steps", type=int, default=0,
                    help="configurations 2/4: Adam steps timed (default 200 / 3)")
     p.add_argument("--case", default=None, choices=["cone", "cone_direct", "mlem", "fwd", "bwd", "stage",
-                                                    "mlem_multi", "bwd_large", "grad"],
+                                                    "mlem_multi", "bwd_large", "grad",
+                                                    "xrf_adjoint_large"],
                    help="run one kernel on a profiling-sized case instead of the benchmark")
     p.add_argument("--case-slices", type=int, default=16,
                    help="slices of 128^2 in the projector / MLEM cases (128: the benchmark's shape)")
@@ -679,8 +680,11 @@ def run_grad(args, device):
         eps = 1e-3
         fd = (float(loss64(Cc.double() + eps * v)) - float(loss64(Cc.double() - eps * v))) / (2 * eps)
         ad = float((g32.double() * v).sum())
+        # rel_err_over_norms: the difference against |g32| |v| (the dot product
+        # sums terms of both signs, so |fd| can be far below that scale)
         grad_check["directional_fd"] = {"adjoint": ad, "fp64_central_difference": fd,
-                                        "rel_err": abs(ad - fd) / abs(fd)}
+                                        "rel_err": abs(ad - fd) / abs(fd),
+                                        "rel_err_over_norms": abs(ad - fd) / float(g32.double().norm())}
         del v
     log("FP64 comparison done", grad_check)
     if N <= 128:
@@ -862,7 +866,9 @@ def run_case(args):
     iteration (plus the sensitivity pass) at 24 angles x 16 slices of 128^2;
     fwd / bwd: the projector at 120 angles x 16 slices of 128^2; bwd_large:
     the backward at 180 angles x --case-slices slices of 256^2; grad: one
-    gradient (projection + adjoint) of configuration 2."""
+    gradient (projection + adjoint) of configuration 2; xrf_adjoint_large: the
+    corrected-projection adjoint of 4 lines at 4 angles (one chunk) over
+    --case-slices slices of 256^2 (the rotation adjoint in row bands)."""
     import torch
     from fl_correction_b200 import _lib
     from fl_correction_b200.cuda_lib import atten_cuda as AC
@@ -934,6 +940,20 @@ def run_case(args):
         Cg = torch.full((Lg, Ng, Ng, Ng), 0.5, device=dev)
         def once():
             rec.gradient(Cg, Ig)
+    elif args.case == "xrf_adjoint_large":
+        from fl_correction_b200 import phantoms
+        from fl_correction_b200.xrf import XRFProjector
+        wl = phantoms.make_workload(4)
+        Nx, Lx, S = wl.N, len(wl.elements), args.case_slices
+        sub = np.arange(4) * (len(wl.angles) // 4)
+        maskx = generate_detector_mask(wl.mask_angle, wl.mask_angle, Nx)
+        fr = wl.frac()[:, :S].copy()
+        proj = XRFProjector(param_at_angles(wl.param, len(wl.angles), sub), wl.angles[sub], maskx,
+                            (S, Nx, Nx), fixed_frac=fr[Lx:], device=dev)
+        Cx = torch.from_numpy(fr[:Lx]).to(dev).contiguous()
+        gx = torch.rand((Lx, len(sub), S, Nx), device=dev, generator=g)
+        def once():
+            proj.adjoint(Cx, gx)
     elif args.case == "bwd_large":
         # the row-band backward: 180 angles x --case-slices slices of 256^2
         N, A, B = 256, 180, args.case_slices

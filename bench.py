@@ -848,9 +848,10 @@ def run_batch(args, device):
                        "ms_per_step": round(t_pers / args.steps, 2),
                        "speedup_vs_plain_loop": round(t_loop / t_pers, 3),
                        "max_rel_err_vs_plain_loop": err_p,
-                       "form": "one flc_mlem_multi_sizes launch per MLEM iteration over all "
-                               "(volume, element) problems; attenuation rebuilt per volume; "
-                               "the schedule replayed as one CUDA graph"},
+                       "form": "one flc_mlem_multi_sizes call per MLEM iteration over all "
+                               "(volume, element) problems (one queue launch per slice width); "
+                               "attenuation rebuilt per volume; the schedule replayed as one "
+                               "CUDA graph"},
         # a replay runs the kernels the eager loop launches (the graph was
         # captured from the same schedule); the host-side counter does not see
         # graph replays, so the loop's count stands for them

@@ -1331,19 +1331,21 @@ proj_bwd_band_kernel(const float* __restrict__ atten, const float* __restrict__ 
 
 // ---------------------------------------------------------------------------
 // Persistent MLEM over several problems (a problem: one element's -- or one
-// volume's -- C, atten, em, theta, I; all with the same R, H, W).  Work item =
-// (problem, slice); the clusters of G CTAs take items from a device counter
-// (largest angle counts first, as the host orders the problems) until none
-// is left.  Per item, CTA g of the cluster takes the angles [g*apc, ...):
+// volume's -- C, atten, em, theta, I; all with the same R; every problem of
+// one launch with the same slice width W, which WC > 0 fixes at compile
+// time).  Work item = (problem, slice); the clusters of G CTAs take items from
+// a device counter (largest work per item first, as the host orders the
+// problems) until none is left.  Per item, CTA g of the cluster takes the angles [g*apc, ...):
 //   mode 0 (iteration): the forward of its angles with the slice of Cin in
 //     shared memory, the ratio I / max(Pf, 1e-6) written to the problem's
 //     ratio buffer; then the backward of the same angles (the image region is
 //     reused as the accumulator), the cluster reduction and the update into
 //     Cout (bwd_epilogue mode 1);
 //   mode 1 (sensitivity): the backward of ratio = 1, max(P^T 1, 1e-6) into sens.
-// One launch thus covers an MLEM iteration of every problem, so that small
-// problems fill the GPU beside large ones and no launch leaves a tail per
-// problem.
+// One launch per slice width thus covers an MLEM iteration of every problem
+// of that width, so that small problems fill the GPU beside large ones and no
+// launch leaves a tail per problem; the shared memory of a launch is sized for
+// its own width, so small slices keep three CTAs per SM.
 // ---------------------------------------------------------------------------
 constexpr int kMaxProbs = 64;
 
@@ -1366,7 +1368,7 @@ struct MlemQueue {
     int n_prob;
 };
 
-template <int RC>
+template <int RC, int WC>
 __global__ void __launch_bounds__(kT2, 3)
 mlem_queue_kernel(const MlemQueue* __restrict__ queue, int* __restrict__ counter, int Rrt,
                   int img_region, int frame_region, int ncopy, int mode, float beta, float delta) {
@@ -1391,7 +1393,7 @@ mlem_queue_kernel(const MlemQueue* __restrict__ queue, int* __restrict__ counter
         while (queue->start[pi + 1] <= item) ++pi;
         const MlemProb P = queue->p[pi];
         const int b = item - queue->start[pi];
-        const int H = P.H, W = P.W, seg = P.seg, parts = P.parts;
+        const int H = P.H, W = WC > 0 ? WC : P.W, seg = P.seg, parts = P.parts;
         const int pitch = slice_pitch(W);
         const int img = H * pitch;
         const int apc = (P.A + G - 1) / G;
@@ -1402,7 +1404,7 @@ mlem_queue_kernel(const MlemQueue* __restrict__ queue, int* __restrict__ counter
             for (int a = a0; a < a1; ++a) {
                 const Geo g = make_geo(P.theta[a], H, W);
                 float* sp = sframe + (a & 1) * parts * W;
-                fwd_angle2<RC, 0>(P.atten + ((int64_t)a * P.B + b) * H * W, simg, img, pitch,
+                fwd_angle2<RC, WC>(P.atten + ((int64_t)a * P.B + b) * H * W, simg, img, pitch,
                                P.em + (int64_t)a * R, R, g, H, W, parts, sp);
                 __syncthreads();
                 fwd_finish(sp, parts, W, RC == 1 ? __ldg(P.em + (int64_t)a * R) : 1.f, P.I,
@@ -1410,7 +1412,7 @@ mlem_queue_kernel(const MlemQueue* __restrict__ queue, int* __restrict__ counter
             }
             __syncthreads();   // the image and partials are reused below
         }
-        bwd_splat_angles<RC, 0>(P.atten, mode == 0 ? P.ratio : nullptr, P.em, P.theta, simg, sframe,
+        bwd_splat_angles<RC, WC>(P.atten, mode == 0 ? P.ratio : nullptr, P.em, P.theta, simg, sframe,
                              sq, ncopy, a0, a1, b, P.B, R, H, W, seg);
         cluster.sync();
         cluster_reduce(cluster, simg, R, H, W, pitch, [&](int r, int h, int w, float s) {
@@ -2003,9 +2005,27 @@ MultiSmem multi_smem(int64_t P, int64_t R, const int64_t* H, const int64_t* W, i
     return m;
 }
 
+// Groups of the problems by slice width, in order of first appearance:
+// gid[i] = group of problem i; returns the number of groups.
+int width_groups(int64_t P, const int64_t* W, int* gid, int64_t* gw) {
+    int ng = 0;
+    for (int64_t i = 0; i < P; ++i) {
+        int g = 0;
+        while (g < ng && gw[g] != W[i]) ++g;
+        if (g == ng) gw[ng++] = W[i];
+        gid[i] = g;
+    }
+    return ng;
+}
+
+// Workspace: per width group two problem tables and a counter (256 bytes),
+// then per problem the sensitivity, the second C buffer and the ratio.
 size_t multi_layout(int64_t P, const int64_t* A, const int64_t* B, int64_t R, const int64_t* H,
                     const int64_t* W, size_t* prob_off) {
-    size_t off = 2 * al256(sizeof(MlemQueue)) + 256;   // two tables, the counter
+    int gid[kMaxProbs];
+    int64_t gw[kMaxProbs];
+    const int ng = width_groups(P, W, gid, gw);
+    size_t off = (size_t)ng * (2 * al256(sizeof(MlemQueue)) + 256);
     for (int64_t i = 0; i < P; ++i) {
         if (prob_off) prob_off[i] = off;
         const size_t nC = al256(sizeof(float) * (size_t)(R * B[i] * H[i] * W[i]));
@@ -2019,6 +2039,24 @@ int mlem_multi_impl(int64_t P, float* const* C, const float* const* atten, const
                     const int64_t* B, int64_t R, const int64_t* H, const int64_t* W, int64_t n_iter,
                     double beta, double delta, void* workspace, size_t workspace_bytes,
                     void* stream);
+
+// The queue kernel for R references and slice width W (compile-time widths
+// 64, 96, 128, 160, 192; any other width at run time).
+template <int RC>
+const void* queue_kernel_for_r(int64_t W) {
+    switch (W) {
+        case 64: return (const void*)mlem_queue_kernel<RC, 64>;
+        case 96: return (const void*)mlem_queue_kernel<RC, 96>;
+        case 128: return (const void*)mlem_queue_kernel<RC, 128>;
+        case 160: return (const void*)mlem_queue_kernel<RC, 160>;
+        case 192: return (const void*)mlem_queue_kernel<RC, 192>;
+        default: return (const void*)mlem_queue_kernel<RC, 0>;
+    }
+}
+
+const void* queue_kernel_for(int64_t R, int64_t W) {
+    return R == 1 ? queue_kernel_for_r<1>(W) : queue_kernel_for_r<0>(W);
+}
 
 }  // namespace
 }  // namespace flc
@@ -2101,86 +2139,116 @@ int mlem_multi_impl(int64_t P, float* const* C, const float* const* atten, const
     }
     cudaStream_t st = as_stream(stream);
     char* ws = (char*)workspace;
-    MlemQueue* q_even = (MlemQueue*)ws;
-    MlemQueue* q_odd = (MlemQueue*)(ws + al256(sizeof(MlemQueue)));
-    int* counter = (int*)(ws + 2 * al256(sizeof(MlemQueue)));
-    // problems in decreasing work per item (angles x slice area): the long
-    // items are taken first
-    int order[kMaxProbs];
-    for (int i = 0; i < P; ++i) order[i] = i;
-    auto cost = [&](int i) { return A[i] * H[i] * W[i]; };
-    for (int i = 1; i < P; ++i)
-        for (int j = i; j > 0 && cost(order[j]) > cost(order[j - 1]); --j) std::swap(order[j], order[j - 1]);
-    MlemQueue te = {}, to = {};
-    te.n_prob = to.n_prob = (int)P;
-    int64_t amax = 1;
-    for (int k = 0; k < P; ++k) {
-        const int i = order[k];
-        char* base = ws + prob_off[i];
-        const size_t nC = al256(sizeof(float) * (size_t)(R * B[i] * H[i] * W[i]));
-        float* sens = (float*)base;
-        float* alt = (float*)(base + nC);
-        float* ratio = (float*)(base + 2 * nC);
-        const int hh = (int)H[i], ww = (int)W[i];
-        const int sg = seg2_length(hh, ww), pt = fwd2_parts(hh, ww);
-        te.p[k] = MlemProb{atten[i], em[i], theta[i], I[i], sens, C[i], alt, ratio,
-                           (int)A[i], (int)B[i], hh, ww, sg, pt};
-        to.p[k] = MlemProb{atten[i], em[i], theta[i], I[i], sens, alt, C[i], ratio,
-                           (int)A[i], (int)B[i], hh, ww, sg, pt};
-        te.start[k + 1] = to.start[k + 1] = te.start[k] + (int)B[i];
-        amax = A[i] > amax ? A[i] : amax;
-    }
-    mlem_queue_init_kernel<<<1, 32, 0, st>>>(te, q_even);
-    FLC_TRY(check_launch("mlem_queue_init_kernel"));
-    mlem_queue_init_kernel<<<1, 32, 0, st>>>(to, q_odd);
-    FLC_TRY(check_launch("mlem_queue_init_kernel"));
-    // launch shape: frame copies that keep the CTAs per SM, cluster size by
-    // (item work / clusters + the longest item), persistent grid
-    int per_sm = 3;
-    while (per_sm > 1 && multi_smem(P, R, H, W, 1).bytes > smem_budget(per_sm)) --per_sm;
-    int ncopy = kMaxFrameCopies;
-    while (ncopy > 1 && multi_smem(P, R, H, W, ncopy).bytes > smem_budget(per_sm)) ncopy /= 2;
-    const MultiSmem ms = multi_smem(P, R, H, W, ncopy);
-    const void* fn = R == 1 ? (const void*)mlem_queue_kernel<1> : (const void*)mlem_queue_kernel<0>;
-    int bestG = 1, nclu = 1;
-    double best = -1;
-    const int gmax = (int)(amax < kMaxCluster ? amax : kMaxCluster);
-    if (int64_t t = tune(kTuneProjCluster)) {
-        bestG = (int)(t < gmax ? t : gmax);
-        nclu = active_clusters(fn, bestG, ms.bytes, kT2);
-    } else {
-        for (int G = 1; G <= gmax; ++G) {
-            const int n = active_clusters(fn, G, ms.bytes, kT2);
-            if (n < 1) continue;
-            double total = 0, longest = 0;
-            for (int64_t i = 0; i < P; ++i) {
-                const double item = (double)(ceil_div(A[i], G) + 2) * (double)(H[i] * W[i]);
-                total += item * (double)B[i];
-                longest = item > longest ? item : longest;
-            }
-            const double c = total / n + longest;
-            if (best < 0 || c < best) {
-                best = c;
-                bestG = G;
-                nclu = n;
+    int gid[kMaxProbs];
+    int64_t gw[kMaxProbs];
+    const int ng = width_groups(P, W, gid, gw);
+    const size_t tbl = al256(sizeof(MlemQueue));
+    struct GroupLaunch {
+        const void* fn;
+        MlemQueue *q_even, *q_odd;
+        int* counter;
+        int G, nclu, ncopy, img_region, frame_region;
+        size_t smem;
+    };
+    GroupLaunch gl[kMaxProbs];
+    for (int gi = 0; gi < ng; ++gi) {
+        // this width's problems, in decreasing work per item (angles x slice
+        // area): the long items are taken first
+        int64_t n = 0, gA[kMaxProbs], gB[kMaxProbs], gH[kMaxProbs], gW[kMaxProbs];
+        int order[kMaxProbs];
+        for (int64_t i = 0; i < P; ++i)
+            if (gid[i] == gi) order[n++] = (int)i;
+        auto cost = [&](int i) { return A[i] * H[i] * W[i]; };
+        for (int i = 1; i < n; ++i)
+            for (int j = i; j > 0 && cost(order[j]) > cost(order[j - 1]); --j) std::swap(order[j], order[j - 1]);
+        char* gbase = ws + (size_t)gi * (2 * tbl + 256);
+        GroupLaunch& L = gl[gi];
+        L.q_even = (MlemQueue*)gbase;
+        L.q_odd = (MlemQueue*)(gbase + tbl);
+        L.counter = (int*)(gbase + 2 * tbl);
+        MlemQueue te = {}, to = {};
+        te.n_prob = to.n_prob = (int)n;
+        int64_t amax = 1, items = 0;
+        for (int k = 0; k < n; ++k) {
+            const int i = order[k];
+            char* base = ws + prob_off[i];
+            const size_t nC = al256(sizeof(float) * (size_t)(R * B[i] * H[i] * W[i]));
+            float* sens = (float*)base;
+            float* alt = (float*)(base + nC);
+            float* ratio = (float*)(base + 2 * nC);
+            const int hh = (int)H[i], ww = (int)W[i];
+            const int sg = seg2_length(hh, ww), pt = fwd2_parts(hh, ww);
+            te.p[k] = MlemProb{atten[i], em[i], theta[i], I[i], sens, C[i], alt, ratio,
+                               (int)A[i], (int)B[i], hh, ww, sg, pt};
+            to.p[k] = MlemProb{atten[i], em[i], theta[i], I[i], sens, alt, C[i], ratio,
+                               (int)A[i], (int)B[i], hh, ww, sg, pt};
+            te.start[k + 1] = to.start[k + 1] = te.start[k] + (int)B[i];
+            amax = A[i] > amax ? A[i] : amax;
+            items += B[i];
+            gA[k] = A[i], gB[k] = B[i], gH[k] = H[i], gW[k] = W[i];
+        }
+        mlem_queue_init_kernel<<<1, 32, 0, st>>>(te, L.q_even);
+        FLC_TRY(check_launch("mlem_queue_init_kernel"));
+        mlem_queue_init_kernel<<<1, 32, 0, st>>>(to, L.q_odd);
+        FLC_TRY(check_launch("mlem_queue_init_kernel"));
+        // launch shape: frame copies that keep the CTAs per SM, cluster size by
+        // (item work / clusters + the longest item), persistent grid
+        int per_sm = 3;
+        while (per_sm > 1 && multi_smem(n, R, gH, gW, 1).bytes > smem_budget(per_sm)) --per_sm;
+        int ncopy = kMaxFrameCopies;
+        while (ncopy > 1 && multi_smem(n, R, gH, gW, ncopy).bytes > smem_budget(per_sm)) ncopy /= 2;
+        const MultiSmem ms = multi_smem(n, R, gH, gW, ncopy);
+        const void* fn = queue_kernel_for(R, gw[gi]);
+        int bestG = 1, nclu = 1;
+        double best = -1;
+        const int gmax = (int)(amax < kMaxCluster ? amax : kMaxCluster);
+        if (int64_t t = tune(kTuneProjCluster)) {
+            bestG = (int)(t < gmax ? t : gmax);
+            nclu = active_clusters(fn, bestG, ms.bytes, kT2);
+        } else {
+            for (int G = 1; G <= gmax; ++G) {
+                const int nc = active_clusters(fn, G, ms.bytes, kT2);
+                if (nc < 1) continue;
+                double total = 0, longest = 0;
+                for (int64_t k = 0; k < n; ++k) {
+                    const double item = (double)(ceil_div(gA[k], G) + 2) * (double)(gH[k] * gW[k]);
+                    total += item * (double)gB[k];
+                    longest = item > longest ? item : longest;
+                }
+                const double c = total / nc + longest;
+                if (best < 0 || c < best) {
+                    best = c;
+                    bestG = G;
+                    nclu = nc;
+                }
             }
         }
+        if (nclu < 1) {
+            set_error("flc_mlem_multi: the queue kernel cannot be made resident");
+            return FLC_ERR_UNSUPPORTED;
+        }
+        if (nclu > items) nclu = (int)items;
+        L.fn = fn;
+        L.G = bestG;
+        L.nclu = nclu;
+        L.ncopy = ncopy;
+        L.img_region = (int)ms.img;
+        L.frame_region = (int)ms.frame;
+        L.smem = ms.bytes;
     }
-    if (nclu < 1) {
-        set_error("flc_mlem_multi: the queue kernel cannot be made resident");
-        return FLC_ERR_UNSUPPORTED;
-    }
-    if (nclu > items) nclu = (int)items;
-    int iR = (int)R, img_region = (int)ms.img, frame_region = (int)ms.frame;
+    int iR = (int)R;
     float fb = (float)beta, fd = (float)delta;
-    auto launch = [&](const MlemQueue* q, int mode) -> int {
-        FLC_TRY_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), st));
-        void* args[] = {(void*)&q, (void*)&counter, &iR, &img_region, &frame_region, &ncopy,
+    auto launch = [&](const GroupLaunch& L, bool odd, int mode) -> int {
+        FLC_TRY_CUDA(cudaMemsetAsync(L.counter, 0, sizeof(int), st));
+        const MlemQueue* q = odd ? L.q_odd : L.q_even;
+        int img_region = L.img_region, frame_region = L.frame_region, ncopy = L.ncopy;
+        void* args[] = {(void*)&q, (void*)&L.counter, &iR, &img_region, &frame_region, &ncopy,
                         &mode, &fb, &fd};
-        return launch_cluster(fn, dim3((unsigned)(nclu * bestG)), bestG, ms.bytes, st, args, kT2);
+        return launch_cluster(L.fn, dim3((unsigned)(L.nclu * L.G)), L.G, L.smem, st, args, kT2);
     };
-    FLC_TRY(launch(q_even, 1));                       // sensitivities
-    for (int64_t it = 0; it < n_iter; ++it) FLC_TRY(launch((it & 1) ? q_odd : q_even, 0));
+    for (int gi = 0; gi < ng; ++gi) FLC_TRY(launch(gl[gi], false, 1));   // sensitivities
+    for (int64_t it = 0; it < n_iter; ++it)
+        for (int gi = 0; gi < ng; ++gi) FLC_TRY(launch(gl[gi], (it & 1) != 0, 0));
     if (n_iter & 1) {
         for (int64_t i = 0; i < P; ++i) {
             const size_t n = sizeof(float) * (size_t)(R * B[i] * H[i] * W[i]);

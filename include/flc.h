@@ -176,11 +176,12 @@ FLC_API int flc_mlem_static(float* C, const float* atten, const float* em, const
  * (A[i], B[i], W), all device pointers held in host arrays of length P; R,
  * H, W are shared (flc_mlem_multi_sizes: H[i], W[i] per problem).  Each C[i]
  * is updated in place by n_iter iterations of flc_mlem.  One persistent
- * launch per iteration covers every problem: clusters of CTAs take (problem,
- * slice) items from a device counter, the largest work per item (angles x
- * slice area) first, and for each item run the forward of their angles, the
- * backward of the same angles and the update; shared memory is sized for
- * the largest slice, which must fit the lean kernels.  Workspace:
+ * launch per iteration and slice width covers every problem of that width:
+ * clusters of CTAs take (problem, slice) items from a device counter, the
+ * largest work per item (angles x slice area) first, and for each item run
+ * the forward of their angles, the backward of the same angles and the
+ * update; the shared memory of a launch is sized for its width (every width
+ * must fit the lean kernels).  Workspace:
  * flc_mlem_multi[_sizes]_workspace_bytes (256-byte aligned).  Issues no host
  * copies (the problem table travels as a kernel argument).  No counterpart
  * in the reference, which runs mlem_cuda_batch once per element and volume

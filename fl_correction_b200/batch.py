@@ -16,10 +16,11 @@ detector distances -- becomes one job:
 * `run()` replays that one graph.
 
 `run_persistent()` is the other batched form: between attenuation rebuilds,
-the MLEM iterations of every (volume, element) pair run as ONE persistent
-launch per iteration (flc_mlem_multi_sizes: clusters take (problem, slice)
-items of all volumes from a device work queue), optionally replayed as a
-CUDA graph of the whole schedule (`capture_persistent`).
+the MLEM iterations of every (volume, element) pair run as one
+flc_mlem_multi_sizes call per iteration (one persistent launch per slice
+width: clusters take (problem, slice) items of all volumes of that width
+from a device work queue), optionally replayed as a CUDA graph of the whole
+schedule (`capture_persistent`).
 
 `run_loop()` is the plain single-volume path for comparison: the same
 problems one after another, default launch shapes, no graph.

@@ -74,6 +74,12 @@ def peaks():
 # ---------------------------------------------------------------------------
 # algorithmic work counts
 # ---------------------------------------------------------------------------
+def sens_bytes(A, S, H, W, R=1):
+    """Bytes of the sensitivity P^T 1 of one element at the reference API
+    boundary: the attenuation read and the sensitivity written."""
+    return 4 * (A * S * H * W + R * S * H * W)
+
+
 def mlem_bytes_per_iter(A, S, H, W, R=1):
     """Bytes of one MLEM iteration of one element at the reference API
     boundary: forward (atten, C, Pf) + backward (atten, ratio, out) + the
@@ -303,7 +309,13 @@ def run_ours(args, rank, world, device):
     fp32_peak = FP32_PEAK_TFLOPS
     mlem_iters = sum(v for _, _, v in mlem_ev)      # element-iterations timed
     bytes_it = mlem_bytes_per_iter(A, N, N, N)
-    proj_gbs = bytes_it * mlem_iters / (t_mlem * 1e-3) / 1e9 if t_mlem else None
+    # the MLEM windows also hold the sensitivity max(P^T 1, 1e-6) that every
+    # mlem call computes first (atten_cuda.cpp:283-345): one backward of
+    # ratio 1 (attenuation read, sensitivity written) per element and rebuild
+    n_sens = -(-n_iter // k) * L * args.steps
+    bytes_sens = sens_bytes(A, N, N, N)
+    mlem_bytes = bytes_it * mlem_iters + bytes_sens * n_sens
+    proj_gbs = mlem_bytes / (t_mlem * 1e-3) / 1e9 if t_mlem else None
     value = job_rate(world, n_iter * args.steps, ms_max)
     e2e_value = job_rate(world, n_iter * args.steps, e2e_ms)
     cone_share = t_cone / ms if ms else 0.0
@@ -340,7 +352,9 @@ def run_ours(args, rank, world, device):
             "traffic_note": "per element-iteration: ncu dram read + write of the lean forward and backward "
                             "at this shape (the attenuation is read twice)",
             "peak_kind": peak_kind,
-            "algorithmic_unit": "%.4g B per element-iteration (fwd + bwd + update at the reference API boundary)" % bytes_it,
+            "algorithmic_unit": "%.4g B per element-iteration (fwd + bwd + update at the reference API "
+                                "boundary) and %.4g B per sensitivity pass (one per element and "
+                                "rebuild, %d timed)" % (bytes_it, bytes_sens, n_sens),
         },
         "roofline_cone": {
             "kernel": "spectral cone (fft_filter, fft_fwd, fft_corr, fft_inv, fft_apply)",

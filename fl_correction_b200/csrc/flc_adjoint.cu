@@ -206,6 +206,78 @@ __global__ void xrf_stage_adjoint_kernel(const float* __restrict__ frac,
     }
 }
 
+// The same reverse stage for the own-compound incident scan (incident_mode
+// 0), where line l's scan uses only its own compound channel l, so the lines'
+// reverse scans are independent: one thread per (detector column w, line j)
+// walks the beam for line j, samples only channel j's rotated fraction and
+// writes D[j] -- the same operations in the same order as the kernel above.
+// The cone adjoint's output, stored reversed and transposed
+// ([al][l][s][W-1-w][H-1-h]), is staged through shared memory kAdjRows rows
+// at a time, so that its loads are whole sectors.  grid (L, S, n_a): the L
+// lines of one (slice, angle) are adjacent and share those rows through L2.
+// block = W rounded to 32 (up to 1024; wider slices take the kernel above).
+constexpr int kAdjRows = 8;
+
+size_t stage_adjoint_own_smem(int64_t L, int64_t W) {
+    return sizeof(float) * (size_t)L * kAdjRows * (size_t)(W + 1);
+}
+
+constexpr int kAdjOwnMaxThreads = 1024;
+
+__global__ void __launch_bounds__(kAdjOwnMaxThreads)
+xrf_stage_adjoint_own_kernel(const float* __restrict__ frac, const float* __restrict__ theta,
+                             const float* __restrict__ coef_x, const float* __restrict__ coef_f,
+                             const float* __restrict__ INC, const float* __restrict__ dinc,
+                             const float* __restrict__ dmu_rev, float* __restrict__ D, int n_ch,
+                             int S, int H, int W, int L, int a0, int n_a) {
+    extern __shared__ float sdm[];          // [L][kAdjRows][W + 1]
+    const int j = blockIdx.x, s = blockIdx.y, al = blockIdx.z, a = a0 + al, w = threadIdx.x;
+    const int P = W + 1;
+    const float cxj = __ldg(coef_x + (int64_t)a * n_ch + j);
+    float cfj[kMaxL];
+#pragma unroll
+    for (int l = 0; l < kMaxL; ++l)
+        cfj[l] = l < L ? __ldg(coef_f + ((int64_t)a * L + l) * n_ch + j) : 0.f;
+    const double th = (double)theta[a];
+    const RotGeom g = rot_geom((float)cos(th), (float)sin(th), H, W);
+    const int64_t HW = (int64_t)H * W;
+    const float* fj = frac + ((int64_t)j * S + s) * HW;
+    const int64_t o0 = (((int64_t)j * n_a + al) * S + s) * HW;
+    float gbar = 0.f;
+    for (int h0 = 0; h0 < H; h0 += kAdjRows) {
+        const int nr = min(kAdjRows, H - h0);
+        __syncthreads();   // the previous rows have been read
+        // dmu of rows h0 .. h0+nr-1: for each (line, column) nr consecutive
+        // floats of the transposed layout
+        for (int t = threadIdx.x; t < L * W * nr; t += blockDim.x) {
+            const int lx = t / nr, r = t - lx * nr;
+            const int l = lx / W, x = lx - l * W;
+            sdm[(l * kAdjRows + r) * P + (W - 1 - x)] =
+                __ldg(dmu_rev + ((((int64_t)al * L + l) * S + s) * W + x) * H + (H - 1 - h0 - r));
+        }
+        __syncthreads();
+        if (w >= W) continue;
+        // (issuing all eight rows' loads before the recursion needs 128
+        // registers and measured slower: 7.8 against 5.3 ms per 4-angle call
+        // at 256 slices of 256^2)
+        for (int r = 0; r < nr; ++r) {
+            const int h = h0 + r;
+            const RotTap tp = rot_tap(g, h, w);
+            const float fr = rot_sample_tap(fj, H, W, tp);
+            const int64_t o = o0 + (int64_t)h * W + w;
+            const float f = 1.f - fr * cxj;
+            const float di = dinc[o];
+            const float df = h > 0 ? gbar * INC[o] : 0.f;
+            gbar = h > 0 ? fmaf(gbar, f, di) : di;
+            float d = cxj * -df;
+#pragma unroll
+            for (int l = 0; l < kMaxL; ++l)
+                if (l < L) d = fmaf(cfj[l], sdm[(l * kAdjRows + r) * P + w], d);
+            D[o] = d;
+        }
+    }
+}
+
 // The rotation adjoint without global atomics: D[j][al][s] (the per-sample
 // gradient of the rotated fractions, one angle of the chunk) spread onto the
 // unrotated grid with the rotation's own taps (rot_tap: the points and
@@ -553,10 +625,24 @@ extern "C" int flc_xrf_project_adjoint(const float* frac, const float* theta, co
         const int threads = (int)((W + 31) & ~31);
         // the per-sample gradient of the rotated fractions into ATT (free
         // again), then its rotation adjoint into dC
-        xrf_stage_adjoint_kernel<<<dim3((unsigned)S, (unsigned)n_a), threads, 0, st>>>(
-            frac, theta, coef_x, coef_f, b.INC, b.DINC, b.DMU, b.ATT, (int)n_ch, (int)S, (int)H,
-            (int)W, (int)L, (int)a0, n_a, incident_mode);
-        FLC_TRY(check_launch("xrf_stage_adjoint_kernel"));
+        const size_t own_smem = stage_adjoint_own_smem(L, W);
+        if (incident_mode == 0 && threads <= kAdjOwnMaxThreads &&
+            own_smem <= (size_t)max_smem_optin()) {
+            if (own_smem > 48 * 1024)
+                FLC_TRY_CUDA(cudaFuncSetAttribute(xrf_stage_adjoint_own_kernel,
+                                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                  (int)own_smem));
+            xrf_stage_adjoint_own_kernel<<<dim3((unsigned)L, (unsigned)S, (unsigned)n_a), threads,
+                                           own_smem, st>>>(
+                frac, theta, coef_x, coef_f, b.INC, b.DINC, b.DMU, b.ATT, (int)n_ch, (int)S,
+                (int)H, (int)W, (int)L, (int)a0, n_a);
+            FLC_TRY(check_launch("xrf_stage_adjoint_own_kernel"));
+        } else {
+            xrf_stage_adjoint_kernel<<<dim3((unsigned)S, (unsigned)n_a), threads, 0, st>>>(
+                frac, theta, coef_x, coef_f, b.INC, b.DINC, b.DMU, b.ATT, (int)n_ch, (int)S,
+                (int)H, (int)W, (int)L, (int)a0, n_a, incident_mode);
+            FLC_TRY(check_launch("xrf_stage_adjoint_kernel"));
+        }
         FLC_TRY(rot_adjoint_launch(b.ATT, theta, dC, S, H, W, L, (int)a0, n_a, st));
     }
     return FLC_OK;

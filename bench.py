@@ -340,8 +340,8 @@ def run_ours(args, rank, world, device):
         "corrected_proj_gbs": round(proj_gbs, 1) if proj_gbs else None,
         # the same metric without the amortised attenuation rebuilds: MLEM
         # iterations (all elements, their sensitivity passes included) per
-        # second of the MLEM windows alone
-        "mlem_iters_per_s_without_rebuilds": round(n_iter * args.steps / (t_mlem * 1e-3), 3)
+        # second of rank 0's MLEM windows alone, times the replicas
+        "mlem_iters_per_s_without_rebuilds": round(world * n_iter * args.steps / (t_mlem * 1e-3), 3)
                                              if t_mlem else None,
         "corrected_proj_pct_hbm": round(100 * proj_gbs / hbm, 1) if proj_gbs else None,
         "time_share": {"cone (spectral, 5 kernels per launch)": round(cone_share, 3),

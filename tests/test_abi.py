@@ -127,3 +127,27 @@ def test_xrf_argument_checks():
                                1 << 30, None) == 1                      # H != W
     assert lib.flc_xrf_project_adjoint(p, p, p, p, p, p, p, p, p, None, p, 3, 4, 16, 16, 10, 2,
                                        3, 16, 3, 0, 0, p, 1 << 30, None) == 1
+
+
+def test_multi_workspace_holds_tables_per_slice_width():
+    # per slice width two problem tables and a counter, then the problems'
+    # buffers: two problems of different widths need one more width group's
+    # tables than the same two problems at one width with the same buffer bytes
+    import ctypes
+    lib = _lib.load()
+    arr = lambda *v: (ctypes.c_int64 * len(v))(*v)
+    A, B, R = arr(8, 8), arr(4, 4), 1
+    # widths 32 + 48 (one group each) against 40 + 40 (one group): the same
+    # image bytes per problem pair (32 + 48 = 2 x 40 columns at one height)
+    two = lib.flc_mlem_multi_sizes_workspace_bytes(2, A, B, R, arr(40, 40), arr(32, 48))
+    one = lib.flc_mlem_multi_sizes_workspace_bytes(2, A, B, R, arr(40, 40), arr(40, 40))
+    assert two > one
+    three = lib.flc_mlem_multi_sizes_workspace_bytes(3, arr(8, 8, 8), arr(4, 4, 4), R,
+                                                     arr(40, 40, 40), arr(32, 48, 32))
+    # the third problem shares the first one's width: no new tables, only its
+    # sensitivity and second C buffer (4 x 40 x 32 floats each) and its ratio
+    # (8 x 4 x 32 floats)
+    assert three - two == 2 * 4 * 40 * 32 * 4 + 8 * 4 * 32 * 4
+    # a width group's tables hold at least 64 problem entries each
+    assert two - one >= 2 * 64 * 8 * 8
+    assert lib.flc_mlem_multi_sizes_workspace_bytes(0, A, B, R, arr(40, 40), arr(40, 40)) == 0

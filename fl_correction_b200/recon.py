@@ -10,6 +10,8 @@ by one native call (rotation, mu assembly, incident scan, cone path sum), and
 the MLEM iterations in between are native cluster launches.  Nothing is
 copied to the host until the caller asks for the result.
 """
+import ctypes
+
 import numpy as np
 import torch
 
@@ -45,11 +47,15 @@ class CorrectedMLEM:
 
     def __init__(self, param, angles_deg, mask, shape, fixed_frac=None, incident="own",
                  beta=0.0, delta=0.01, device="cuda", chunk=0, bound_frac=True,
-                 feedback="bounded", cal_frac_args=None, multi=False):
+                 feedback="bounded", cal_frac_args=None, multi=False, concurrent=True):
         self.device = torch.device(device)
         # multi: the MLEM iterations of all elements in one persistent launch
         # each (flc_mlem_multi) instead of one flc_mlem call per element
         self.multi = multi
+        # concurrent: the elements' flc_mlem calls (independent chains of
+        # launches) on one stream each, joined back into the caller's stream,
+        # so that one element's kernels fill the SMs another's leave idle
+        self.concurrent = bool(concurrent)
         self._ws_multi = None
         self.bound_frac = bound_frac
         if feedback not in ("bounded", "cal_frac"):
@@ -90,6 +96,12 @@ class CorrectedMLEM:
         self.ws_atten = _lib.workspace(ws, dev)
         self.ws_mlem_bytes = _lib.query("flc_mlem_workspace_bytes", A, S, 1, H, W)
         self.ws_mlem = _lib.workspace(self.ws_mlem_bytes, dev)
+        self._elem = None
+        if self.concurrent and self.L > 1:
+            # one stream and one MLEM workspace per element
+            self._elem = [(torch.cuda.Stream(device=dev),
+                           self.ws_mlem if l == 0 else _lib.workspace(self.ws_mlem_bytes, dev))
+                          for l in range(self.L)]
 
     # -- building blocks -------------------------------------------------
     def recompute_attenuation(self, C, cone_events=None):
@@ -120,7 +132,8 @@ class CorrectedMLEM:
     def mlem(self, C, I, n_iter, use_graph=0, mlem_events=None):
         """n_iter MLEM iterations per element with the current attenuation; C
         (L, S, H, W) is updated in place.  mlem_events: optional list receiving
-        (start, end) CUDA events around each element's iterations."""
+        (start, end) CUDA events around each element's iterations (around all
+        elements' when they run concurrently)."""
         S, H, W = self.shape
         if self.multi and use_graph == 0:
             if mlem_events is not None:
@@ -133,6 +146,24 @@ class CorrectedMLEM:
             if mlem_events is not None:
                 e1.record()
                 mlem_events.append((e0, e1, int(n_iter) * self.L))
+            return C
+        if self._elem is not None and use_graph == 0:
+            with torch.cuda.device(self.device):
+                main = torch.cuda.current_stream(self.device)
+                if mlem_events is not None:
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(main)
+                for l, (st, ws) in enumerate(self._elem):
+                    st.wait_stream(main)
+                    _lib.call("flc_mlem", _lib.ptr(C[l]), _lib.ptr(self.atten[l]),
+                              _lib.ptr(self.em[l]), _lib.ptr(self.theta), _lib.ptr(I[l]),
+                              int(n_iter), self.beta, self.delta, self.A, S, 1, H, W,
+                              _lib.ptr(ws), self.ws_mlem_bytes, 0, ctypes.c_void_p(st.cuda_stream))
+                for st, _ in self._elem:
+                    main.wait_stream(st)
+                if mlem_events is not None:
+                    e1.record(main)
+                    mlem_events.append((e0, e1, int(n_iter) * self.L))
             return C
         with torch.cuda.device(self.device):
             for l in range(self.L):

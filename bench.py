@@ -497,8 +497,11 @@ def reference_gpu_leg(device, N=128, A=120, n_vol=30):
     ratio = torch.rand((A, N, N), device=device, generator=g)
     I = AC.forward_emission_batch(atten, C, em, th) * 1.05
 
-    def ev_ms(fn, reps):
-        fn()
+    def ev_ms(fn, reps, warm=1):
+        # warm-up calls first: a GPU left idle (the host-side legs before this
+        # one) runs its first kernels at low clocks
+        for _ in range(warm):
+            fn()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
@@ -525,9 +528,12 @@ def reference_gpu_leg(device, N=128, A=120, n_vol=30):
     out = {}
     for name, (fr, fo, reps) in cases.items():
         # ours first, then the reference, each warmed up and timed on its own
+        # (ours: three warm-up calls and at least five timed; the reference's
+        # slowest call takes about a second, so it keeps one warm-up call)
         l0 = _lib.query("flc_launch_count")
-        o_ms = ev_ms(fo, reps)
-        launches = (_lib.query("flc_launch_count") - l0) // (reps + 1)
+        o_reps = max(reps, 5)
+        o_ms = ev_ms(fo, o_reps, warm=3)
+        launches = (_lib.query("flc_launch_count") - l0) // (o_reps + 3)
         r_ms = ev_ms(fr, reps)
         out[name] = {"reference_ms": round(r_ms, 3), "ours_ms": round(o_ms, 3),
                      "speedup": round(r_ms / o_ms, 2), "ours_launches_per_call": int(launches)}

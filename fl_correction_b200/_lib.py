@@ -60,6 +60,8 @@ SIGNATURES = {
     "flc_cone_atten_apply": (_int, [_vp, _vp, _vp, _vp, _i64, _i64, _i64, _i64, _i64, _i64, _i64,
                                     _i64, _i64, _i64, _vp]),
     "flc_cone_fft_workspace_bytes": (_sz, [_i64] * 7),
+    "flc_cone_atten_workspace_bytes": (_sz, [_i64] * 7),
+    "flc_cone_atten_separable_ws": (_int, [_vp, _vp, _vp, _vp] + [_i64] * 7 + [_int, _vp, _sz, _vp]),
     "flc_atten_stage_workspace_bytes": (_sz, [_i64] * 4),
     "flc_atten_stage_ws": (_int, [_vp] * 6 + [_i64] * 8 + [_int, _int, _vp, _sz, _vp]),
     "flc_cone_atten_apply_ws": (_int, [_vp, _vp, _vp, _vp] + [_i64] * 10 + [_vp, _sz, _vp]),

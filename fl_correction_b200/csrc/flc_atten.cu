@@ -766,6 +766,31 @@ extern "C" int flc_cone_atten_separable(const float* mu, const float* u, const f
                            as_stream(stream));
 }
 
+extern "C" size_t flc_cone_atten_workspace_bytes(int64_t K, int64_t Z, int64_t X, int64_t Y,
+                                                 int64_t Mz, int64_t Mx, int64_t My) {
+    if (K < 1 || Z < 1 || X < 1 || Y < 1 || Mz < 1 || Mx < 1 || My < 1) return 0;
+    return cone_fft_ws_bytes(K, Z, X, Y, Mz, Mx, My, 0);
+}
+
+extern "C" int flc_cone_atten_separable_ws(const float* mu, const float* u, const float* v,
+                                           float* out, int64_t K, int64_t Z, int64_t X,
+                                           int64_t Y, int64_t Mz, int64_t Mx, int64_t My,
+                                           int mode, void* workspace, size_t workspace_bytes,
+                                           void* stream) {
+    clear_error();
+    FLC_REQUIRE(mu && u && v && out, "flc_cone_atten_separable_ws: null pointer argument");
+    FLC_REQUIRE(K >= 1 && Z >= 1 && X >= 1 && Y >= 1 && Mz >= 1 && Mx >= 1 && My >= 1,
+                "flc_cone_atten_separable_ws: sizes must be positive");
+    FLC_REQUIRE(mode == 0 || mode == 1, "flc_cone_atten_separable_ws: mode must be 0 or 1");
+    FLC_REQUIRE(K <= 65535, "flc_cone_atten_separable_ws: K must be <= 65535");
+    if (workspace && ((uintptr_t)workspace & 255) != 0) {
+        set_error("flc_cone_atten_separable_ws: workspace must be 256-byte aligned");
+        return FLC_ERR_ALIGNMENT;
+    }
+    return cone_launch_ws(mu, u, v, out, K, Z, X, Y, Mz, Mx, My, mode, 1, 0, 0, 0, workspace,
+                          workspace ? workspace_bytes : 0, as_stream(stream));
+}
+
 extern "C" int flc_cone_atten(const float* mu, const float* mask, float* out, int64_t K,
                               int64_t Z, int64_t X, int64_t Y, int64_t Mz, int64_t Mx, int64_t My,
                               int flags, void* stream) {

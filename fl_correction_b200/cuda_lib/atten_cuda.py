@@ -18,8 +18,35 @@ def _c(t):
     return t if t.is_contiguous() else t.contiguous()
 
 
+# per device: (copy of the last mask, its factors u, v or None when it is not
+# rank one per depth plane)
+_MASK_FACTORS = {}
+
+
+def _mask_factors(mask):
+    """The rank-one factors of each depth plane of a float32 device mask,
+    computed on the host once per distinct mask (a caller that passes the
+    same mask every angle, as the reference's torch_xrf_atten_3D does, pays
+    one device comparison per call), or None if some plane is not rank one."""
+    from ..detector_mask import factor_mask
+    key = (mask.device.index, tuple(mask.shape))
+    hit = _MASK_FACTORS.get(key)
+    if hit is not None and torch.equal(hit[0], mask):
+        return hit[1]
+    fac = factor_mask(mask.detach().cpu().numpy())
+    uv = None if fac is None else tuple(torch.from_numpy(f).to(mask.device).contiguous()
+                                        for f in fac)
+    _MASK_FACTORS[key] = (mask.detach().clone(), uv)
+    return uv
+
+
 def cal_atten_cuda(mu, mask):
-    """Cone-mask path sum (atten_cuda.cpp:12-28): mu (K,Z,X,Y), mask (Mz,Mx,My) -> (K,Z,X,Y)."""
+    """Cone-mask path sum (atten_cuda.cpp:12-28): mu (K,Z,X,Y), mask (Mz,Mx,My) -> (K,Z,X,Y).
+
+    A mask that is rank one per depth plane (every mask generate_detector_mask
+    builds) runs the separable forms with its factors cached and the spectral
+    form's scratch taken from torch's allocator; any other mask, or a shape
+    the separable kernels do not take, runs flc_cone_atten."""
     _lib.require_cuda("cal_atten_cuda", mu, mask)
     if mu.dim() != 4 or mask.dim() != 3:
         raise RuntimeError("cal_atten_cuda: mu must be (K,Z,X,Y) and mask (Mz,Mx,My)")
@@ -28,6 +55,18 @@ def cal_atten_cuda(mu, mask):
     K, Z, X, Y = mu.shape
     Mz, Mx, My = mask.shape
     with torch.cuda.device(mu.device):
+        uv = _mask_factors(mask) if mask.dtype == torch.float32 and K <= 65535 else None
+        if uv is not None:
+            nb = int(_lib.query("flc_cone_atten_workspace_bytes", K, Z, X, Y, Mz, Mx, My))
+            ws = _lib.workspace(nb, mu.device) if nb else None
+            try:
+                _lib.call("flc_cone_atten_separable_ws", _lib.ptr(mu), _lib.ptr(uv[0]),
+                          _lib.ptr(uv[1]), _lib.ptr(out), K, Z, X, Y, Mz, Mx, My, 0,
+                          _lib.ptr(ws), nb, _lib.stream())
+                return out
+            except _lib.FlcError as e:
+                if e.status != "FLC_ERR_UNSUPPORTED":
+                    raise
         _lib.call("flc_cone_atten", _lib.ptr(mu), _lib.ptr(mask), _lib.ptr(out), K, Z, X, Y,
                   Mz, Mx, My, 0, _lib.stream())
     return out

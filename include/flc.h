@@ -115,6 +115,21 @@ FLC_API int flc_cone_atten_separable(const float* mu, const float* u, const floa
                              int64_t K, int64_t Z, int64_t X, int64_t Y,
                              int64_t Mz, int64_t Mx, int64_t My, int mode, void* stream);
 
+/* flc_cone_atten_separable with caller scratch for the spectral form (the
+ * form flc_cone_atten picks, without its per-call mask read-back,
+ * factorisation and scratch allocation): `workspace` (256-byte aligned) of
+ * flc_cone_atten_workspace_bytes(K, Z, X, Y, Mz, Mx, My) bytes; where that is
+ * 0 (the padded planes do not fit) or workspace is NULL, the direct separable
+ * kernel runs.  mode 0 writes the sum, 1 exp(-sum).  Same results as
+ * flc_cone_atten to FP32 rounding.  Counterpart: cal_atten_cuda
+ * (atten_cuda.cpp:12-28) with the mask factored once by the caller. */
+FLC_API size_t flc_cone_atten_workspace_bytes(int64_t K, int64_t Z, int64_t X, int64_t Y,
+                                              int64_t Mz, int64_t Mx, int64_t My);
+FLC_API int flc_cone_atten_separable_ws(const float* mu, const float* u, const float* v,
+                                        float* out, int64_t K, int64_t Z, int64_t X, int64_t Y,
+                                        int64_t Mz, int64_t Mx, int64_t My, int mode,
+                                        void* workspace, size_t workspace_bytes, void* stream);
+
 /* ---------------------------------------------------------------------
  * Attenuated emission projector.
  * forward: Pf[a,b,w] = sum_h atten[a,b,h,w] * sum_r em[a,r] * bilerp(C[r,b], row(a,h,w), col(a,h,w))

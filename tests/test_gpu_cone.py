@@ -298,3 +298,29 @@ def test_bounded_wait_runs_out_and_reports_timeout():
     run()                                           # the same call works again
     assert lib.flc_device_status(1) == 0
     assert rel_err(out.cpu().numpy(), O.cone_ref(mu, mask.astype(np.float32))) < TOL_MAP
+
+
+def test_cached_mask_factors_follow_the_mask():
+    # cal_atten_cuda factors a mask once and reuses the factors while the same
+    # mask comes back: the cached path against flc_cone_atten (which reads and
+    # factors the mask on every call), then after the mask changes in place,
+    # then with a mask that is not rank one (the general gather)
+    rng = np.random.default_rng(12)
+    mu = T((rng.random((3, 20, 24, 20)) * 0.05).astype(np.float32))
+    mask = T(generate_detector_mask(13.309, 13.309, 24).astype(np.float32))
+
+    def direct(m):
+        out = torch.empty_like(mu)
+        _lib.call("flc_cone_atten", _lib.ptr(mu), _lib.ptr(m), _lib.ptr(out), *mu.shape,
+                  *m.shape, 0, _lib.stream())
+        return out
+
+    for _ in range(2):
+        got = AC.cal_atten_cuda(mu, mask)
+        assert rel_err(got.cpu().numpy(), direct(mask).cpu().numpy()) < 1e-6
+    mask.mul_(0.5)
+    got = AC.cal_atten_cuda(mu, mask)
+    assert rel_err(got.cpu().numpy(), O.cone_ref(mu.cpu().numpy(), mask.cpu().numpy())) < TOL_MAP
+    mask[0, 3, 1] += 0.7        # no longer rank one in that depth plane
+    got = AC.cal_atten_cuda(mu, mask)
+    assert rel_err(got.cpu().numpy(), O.cone_ref(mu.cpu().numpy(), mask.cpu().numpy())) < TOL_MAP

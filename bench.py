@@ -402,7 +402,7 @@ def load_reference_extension():
 
 
 def parity_leg(wl, mask, solver, I, device):
-    """Errors of this build's corrected MLEM against independent compositions
+    """Errors of this library's corrected MLEM against independent compositions
     (tests/compose.py), on inputs identical to the benchmark's:
 
     * first block of the benchmark (128^3, 3 elements, 120 angles; the
@@ -477,7 +477,7 @@ def parity_leg(wl, mask, solver, I, device):
 
 def reference_gpu_leg(device, N=128, A=120, n_vol=30):
     """CUDA-event times of the reference's own kernels (FL/cuda_lib compiled
-    from its sources for sm_100a) beside this build's drop-ins, through the
+    from its sources for sm_100a) beside this library's drop-ins, through the
     same Python API, at the benchmark's shapes: the cone path sum of one
     30-volume attenuation chunk, the batched forward and backward projector
     (120 angles x 128 slices of 128^2, one reference) and 5 MLEM iterations."""

@@ -45,7 +45,7 @@ def compose_cs_incident_xray_with_reference(ref_3D, ref_cs, ref_comp):
     FL.core.cal_frac(ref_3D, scale_range=[], enable_scale=False)
     (FL/core.py:159-205) without its Otsu-threshold mask: the reference masks
     with skimage's threshold_multiotsu and falls back to no mask when the
-    threshold fails, which is the case this build reproduces.  FP64 on the
+    threshold fails, which is the case this library reproduces.  FP64 on the
     device of ref_3D (numpy input: cuda)."""
     n_ref = int(ref_cs["n_ref"])
     if len(ref_3D) != n_ref:

@@ -36,7 +36,7 @@ extern "C" {
 typedef enum {
     FLC_OK = 0,
     FLC_ERR_INVALID_ARG = 1,  /* null pointer, non-positive or inconsistent size */
-    FLC_ERR_UNSUPPORTED = 2,  /* valid request outside what this build supports */
+    FLC_ERR_UNSUPPORTED = 2,  /* valid request outside what this library supports */
     FLC_ERR_ALIGNMENT = 3,    /* pointer not aligned as the entry point requires */
     FLC_ERR_WORKSPACE = 4,    /* caller-provided workspace too small */
     FLC_ERR_CUDA = 5,         /* CUDA runtime / launch error */
